@@ -1,0 +1,370 @@
+#!/usr/bin/env python
+"""Depth-step throughput of the BFPn pencil-beam solver on B200.
+
+Metric: phase-space updates/s -- cells of both species advanced one full
+Strang depth step per second.  Workload (the single-beam configuration of the
+benchmark plan): water, 230 MeV beam, sigma_E 2.3 MeV (1 %), sigma_yz 0.5 cm,
+8 x 8 cm lateral domain, Ny = Nz = 20, Nmu = Nom = 20, Ng = 500, 40 cm depth
+(Nx = 1000, 1000 steps); 88.2 M cells per array, both species.  Inputs are the
+reference's water tables (tests/golden/tables/water).  Mixed precision by
+default (float state; double energy recursion and IDD), --precision fp64 for
+the parity mode.
+
+One "step" = one depth step of the whole beam (both species) with the state
+resident in HBM.  The four state arrays (1.4 GB in mixed precision) exceed the
+126 MB L2, so no flush is needed between timed steps.
+
+Multi-GPU: independent replicas (one beam per GPU, no collective on the data
+path); the timed region is bracketed by barriers and the time is the max over
+ranks.
+
+--impl reference times the CPU oracle (FP64 restatement of the reference's
+eq15 path, all host threads) on the same workload, one depth step per step.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+WORKLOAD = dict(nx=1000, t_final=40.0, ny=20, nz=20, nmu=20, nom=20, ng=500, ly=8.0, lz=8.0, beam_energy=230.0,
+                sigma_e=2.3, sigma_yz=0.5, material_name="water")
+WORKLOAD_NAME = "water 230 MeV pencil beam, 20x20 yz / 20x20 angles / 500 groups, 40 cm (1000 depth steps)"
+TABLES = os.path.join(ROOT, "tests", "golden", "tables", "water")
+METRIC = "phase-space updates/s"
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return p, "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.out, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.out.flush()
+        self.out.seek(0)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.out.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        os.unlink(self.out.name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", init_method="env://", world_size=world, rank=rank,
+                                timeout=__import__("datetime").timedelta(seconds=300))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world, local):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda:%d" % local)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def kernel_bytes(cls, cells, elem, n_groups, nyz, NA):
+    """Algorithmic bytes (hbm) or flops (tensor) of one launch of a kernel class."""
+    if cls == "energy":
+        return "hbm", 4.5 * cells * elem  # F, f read + write; the secondary's two launches also read the source
+    if cls == "transport":
+        return "hbm", 2.0 * cells * elem
+    if cls == "angle":
+        return "hbm", 2.0 * cells * elem
+    if cls == "source_energy":
+        return "hbm", 3.0 * cells * elem  # A1, A2 read, S written
+    if cls == "source_angular":
+        return "tensor", 2.0 * 2.0 * nyz * NA * NA * n_groups  # two operands
+    return "hbm", 0.0
+
+
+def run_ours(args):
+    import torch
+    from bfpn_gpu_b200 import Context, capi, make_config, read_tables
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    cfg = make_config(**WORKLOAD)
+    prec = capi.PREC_MIXED if args.precision == "mixed" else capi.PREC_FP64
+    elem = 4 if prec == capi.PREC_MIXED else 8
+    mu, sig = read_tables(TABLES, cfg.ng)
+    ctx = Context(cfg.grid(), cfg.phys(), prec, device=local)
+    ctx.load_tables(mu, sig)
+    ctx.init_beam()
+    ctx.step(1 + max(args.warmup, 3), fetch=False)  # first step (no secondary) + warm-up (graph capture)
+    cells = ctx.cells
+    updates_per_step = 2 * cells
+
+    sampler = ClockSampler(local)
+    torch.cuda.synchronize()
+    barrier(world)
+    sampler.start()
+    ms = ctx.timed_steps(args.steps)
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = sampler.stop()
+    ms = max_over_ranks(ms, world, local)
+    sec = ms / 1e3
+    value = world * updates_per_step * args.steps / sec
+    kps = ctx.kernels_per_step()
+
+    # per-kernel device times, eager launches bracketed by CUDA events
+    ctx.set_profiling(True)
+    ctx.kernel_profile(reset=True)
+    prof_steps = 2
+    ctx.step(prof_steps, fetch=False)
+    prof = ctx.kernel_profile()
+    ctx.set_profiling(False)
+    nyz = (cfg.ny + 1) * (cfg.nz + 1)
+    NA = cfg.nmu * cfg.nom
+    n_groups = ctx.source_groups()
+    pk, pk_kind = peaks()
+    per_kernel = {}
+    for cls, (tot, n) in prof.items():
+        if n == 0:
+            continue
+        bound, work = kernel_bytes(cls, cells, elem, n_groups, nyz, NA)
+        avg = tot / n
+        entry = {"launches_per_step": n / prof_steps, "ms_per_launch": avg, "share": tot / sum(v[0] for v in prof.values())}
+        if work > 0:
+            if bound == "hbm":
+                entry["achieved_GBps"] = work / (avg / 1e3) / 1e9
+            else:
+                entry["achieved_TFLOPs"] = work / (avg / 1e3) / 1e12
+        per_kernel[cls] = entry
+    dom = max(prof.items(), key=lambda kv: kv[1][0])[0]
+    bound, work = kernel_bytes(dom, cells, elem, n_groups, nyz, NA)
+    avg_s = prof[dom][0] / prof[dom][1] / 1e3
+    if bound == "hbm":
+        achieved = work / avg_s / 1e9
+        peak = pk["hbm_gbs"]
+        roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": None, "peak_source": pk_kind}
+    else:
+        achieved = work / avg_s / 1e12
+        peak = pk.get("bf16_tflops_sustained", pk["bf16_tflops"])
+        roof = {"kernel": dom, "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak, "traffic": None, "peak_source": pk_kind}
+    ctx.close()
+
+    out = {"metric": METRIC, "value": value, "unit": "updates/s", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32 state / f64 recursion" if prec == capi.PREC_MIXED else "f64",
+           "data": "reference water tables; synthetic initial beam (Gaussian y/z/E, near-delta angle)",
+           "config": {"workload": WORKLOAD_NAME, "precision": args.precision, "cells_per_array": cells,
+                      "species": 2, "l2": "state arrays 4 x %.2f GB > L2; no flush" % (cells * elem / 1e9),
+                      "parallelism": "replicas x%d" % world},
+           "gpu_launches": kps * args.steps, "kernels_per_step": kps, "roofline": roof, "per_kernel": per_kernel}
+    if clocks:
+        out["clocks"] = clocks
+
+    if rank == 0 and not args.no_e2e:
+        out["e2e"] = e2e_job(cfg, prec, local, mu, sig)
+    if rank == 0 and world == 1 and not args.no_accuracy and prec == capi.PREC_MIXED:
+        out["accuracy"] = accuracy(cfg, local, mu, sig, args.accuracy_steps)
+    if rank == 0 and world == 1 and not args.no_cpu:
+        out["cpu_baseline"] = cpu_baseline(cfg, mu, sig, args.cpu_steps)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+def e2e_job(cfg, prec, device, mu_host, sig_host):
+    """The whole beam solve through the public C ABI: host tables in, IDD out."""
+    from bfpn_gpu_b200 import Context, capi, read_tables
+
+    steps = cfg.max_steps()
+    t0 = time.perf_counter()
+    mu, sig = read_tables(TABLES, cfg.ng)
+    ctx = Context(cfg.grid(), cfg.phys(), prec, device=device)
+    ctx.load_tables(mu, sig)
+    ctx.init_beam()
+    idd, proxy = ctx.step(steps)
+    t1 = time.perf_counter()
+    cells = ctx.cells
+    elem = 4 if prec == capi.PREC_MIXED else 8
+    NA = cfg.nmu * cfg.nom
+    nyz = (cfg.ny + 1) * (cfg.nz + 1)
+    h2d = (cfg.ng * NA * NA * elem + 2 * cfg.ng * cfg.ng * 8 + nyz * NA * 8 + 2 * cfg.ng * NA * elem
+           + cfg.ng * 40 * 8)
+    ctx.close()
+    updates = cells * (2 * steps - 1)  # the first step advances the primary only
+    return {"value": updates / (t1 - t0), "unit": "updates/s", "h2d_bytes_per_step": h2d / steps,
+            "d2h_bytes_per_step": 16, "steps": steps, "seconds": t1 - t0,
+            "what": "create + load tables + initial beam + %d depth steps + IDD/proxy history to host" % steps}
+
+
+def accuracy(cfg, device, mu, sig, nsteps):
+    """IDD of the mixed-precision run against the FP64 run, same inputs."""
+    from bfpn_gpu_b200 import Context, capi
+
+    res = {}
+    idds = {}
+    for prec in (capi.PREC_FP64, capi.PREC_MIXED):
+        ctx = Context(cfg.grid(), cfg.phys(), prec, device=device)
+        ctx.load_tables(mu, sig)
+        ctx.init_beam()
+        idds[prec], _ = ctx.step(nsteps)
+        ctx.close()
+    a, b = idds[capi.PREC_MIXED], idds[capi.PREC_FP64]
+    peak = np.abs(b).max()
+    big = b > 0.01 * peak
+    res["steps"] = nsteps
+    res["idd_max_rel_err_above_1pct_peak"] = float((np.abs(a - b)[big] / b[big]).max())
+    res["idd_max_err_rel_to_peak"] = float(np.abs(a - b).max() / peak)
+    dx = cfg.dt()
+    res["bragg_peak_cm_fp64"] = float((np.argmax(b) + 1) * dx)
+    res["bragg_peak_shift_mm"] = float(abs(np.argmax(a) - np.argmax(b)) * dx * 10)
+    return res
+
+
+def cpu_baseline(cfg, mu, sig, nsteps):
+    """The oracle (FP64 restatement of the reference's path) on the host cores:
+    a bounded sample of the same workload -- depth steps after the first."""
+    from oracle import oracle as O
+
+    threads = O.max_threads()
+    o = O.Oracle(cfg.grid(), cfg.phys(), mu, sig)
+    o.step(1)  # first step: primary only
+    t0 = time.perf_counter()
+    o.step(nsteps)
+    sec = time.perf_counter() - t0
+    o.close()
+    return {"value": 2 * o.cells * nsteps / sec, "unit": "updates/s", "cores": threads, "kind": "port",
+            "sample": "%d depth step(s) (both species, FP64) of the same workload after the first" % nsteps,
+            "seconds": sec}
+
+
+def run_reference(args):
+    """CPU reference arm: the oracle port on all host threads, rank 0 only."""
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return
+    from bfpn_gpu_b200 import make_config, read_tables
+    from oracle import oracle as O
+
+    cfg = make_config(**WORKLOAD)
+    mu, sig = read_tables(TABLES, cfg.ng)
+    threads = O.max_threads()
+    o = O.Oracle(cfg.grid(), cfg.phys(), mu, sig)
+    o.step(1)  # first step (primary only)
+    warm = min(args.warmup, 1)
+    if warm:
+        o.step(warm)
+    budget = args.reference_budget_s
+    done = 0
+    t0 = time.perf_counter()
+    while done < args.steps:
+        o.step(1)
+        done += 1
+        if time.perf_counter() - t0 > budget:
+            break
+    sec = time.perf_counter() - t0
+    value = 2 * o.cells * done / sec
+    o.close()
+    sample = "%d depth step(s) of the workload, FP64, %d threads (time-bounded at %.0f s)" % (done, threads, budget)
+    out = {"metric": METRIC, "value": value, "unit": "updates/s", "n_gpus": world, "steps": done,
+           "warmup": warm, "ms_per_step": sec * 1e3 / done, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "reference water tables; synthetic initial beam",
+           "config": {"workload": WORKLOAD_NAME, "precision": "fp64"}, "impl": "reference",
+           "cpu_baseline": {"value": value, "unit": "updates/s", "cores": threads, "kind": "port", "sample": sample},
+           "e2e": {"value": value, "unit": "updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--accuracy-steps", type=int, default=1000)
+    ap.add_argument("--cpu-steps", type=int, default=1)
+    ap.add_argument("--reference-budget-s", type=float, default=120.0)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

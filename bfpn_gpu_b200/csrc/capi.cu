@@ -1,0 +1,1172 @@
+// C-ABI implementation: one beam's solver context (replaces BFPnSolver,
+// bfpm_solver.cuh:97-253, for the in-memory eq15 path).
+//
+// The context owns all device memory, allocated up front.  A depth step is
+// enqueued as a fixed sequence of kernels on the context stream and captured
+// once into a CUDA graph; the IDD of each step is reduced on the device into a
+// history array, so a run of steps needs no host synchronisation.
+
+#include "../../include/bfpn_capi.h"
+#include "common.cuh"
+#include "tables.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <type_traits>
+#include <string>
+#include <vector>
+
+using namespace bfpn;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+}  // namespace
+
+struct bfpn_ctx {
+    bfpn_grid g{};
+    bfpn_phys p{};
+    int prec = BFPN_PREC_FP64;
+    int device = 0;
+    size_t elem = 8;
+    Deltas d{};
+    int Ng = 0, Ny = 0, Nz = 0, Nmu = 0, Nom = 0, nyz = 0, NA = 0;
+    long long per_e = 0, cells = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+    std::vector<DevBuf> allocs;
+    void* st[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    void* tmp = nullptr;       // out-of-place transport target (tiled planes only)
+    void* src = nullptr;       // secondary source
+    void* A1 = nullptr;        // angular contractions of the primary
+    void* A2 = nullptr;
+    double* ecoef_half = nullptr;   // energy constants for dt/2
+    double* ecoef_op = nullptr;     // energy constants for a per-operator dt
+    double ecoef_op_dt = -1.0;
+    double* dose_coef = nullptr;
+    void* omega = nullptr;
+    void* fac_step = nullptr;       // angle factor for the full step dt
+    void* fac_op = nullptr;         // angle factor for a per-operator dt
+    double fac_op_dt = -1.0;
+    void* sine_u = nullptr;
+    void* sine_v = nullptr;
+    void* ker_v = nullptr;
+    double* e1 = nullptr;
+    double* e2 = nullptr;
+    int* groups = nullptr;
+    int n_groups = 0;
+    int* tile_lo = nullptr;
+    int* tile_hi = nullptr;
+    int tile_e = 16;
+    double* beam_yza = nullptr;
+    double* beam_e = nullptr;
+    double* partials = nullptr;     // [2][energy_grid][2]
+    int n_part = 0;
+    double* hist_idd = nullptr;
+    double* hist_proxy = nullptr;
+    int hist_cap = 0;
+    int* counter = nullptr;
+    int* zero_counter = nullptr;    // scratch counter for one-off IDD reductions
+    double* scalar_out = nullptr;   // [2] one-off IDD / proxy
+    double* moments = nullptr;      // [Ng][2]
+
+    BeamTables tables;
+    std::vector<double> raw_sigma;  // sigma_c as given, before the optional calibration
+    bool tables_loaded = false;
+    bool beam_ready = false;
+    int steps_done = 0;
+    bool secondary_zero = true;
+
+    // transport launch shape
+    int tr_ac = 16, tr_ty = 1, tr_tz = 1;
+    bool tr_inplace = true;
+    int ang_slices = 4;
+    int energy_block = 128;
+
+    cudaGraphExec_t graph_exec = nullptr;
+    int graph_key = -1;
+    bool use_graphs = true;
+    bool profiling = false;
+    struct Pending {
+        int cls;
+        cudaEvent_t a, b;
+    };
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<Pending> pending;
+    double prof_ms[BFPN_KERNEL_CLASSES] = {};
+    int prof_n[BFPN_KERNEL_CLASSES] = {};
+    long long launches = 0;        // launches issued by host enqueue code
+    int kernels_per_step = 0;
+
+    std::string err;
+};
+
+namespace {
+
+bfpn_status fail(bfpn_ctx* c, bfpn_status s, const std::string& msg) {
+    if (c) c->err = msg;
+    else g_create_error = msg;
+    return s;
+}
+
+#define CUDA_TRY(ctx, expr)                                                                      \
+    do {                                                                                         \
+        cudaError_t _e = (expr);                                                                 \
+        if (_e != cudaSuccess)                                                                   \
+            return fail(ctx, _e == cudaErrorMemoryAllocation ? BFPN_OOM : BFPN_CUDA_ERROR,       \
+                        std::string(#expr) + ": " + cudaGetErrorString(_e));                     \
+    } while (0)
+
+bool valid_grid(const bfpn_grid& g, std::string& why) {
+    if (g.Nx <= 0 || g.Ny <= 0 || g.Nz <= 0 || g.Ng < 2 || g.Nmu <= 0 || g.Nom <= 0) {
+        why = "grid sizes must be positive (Ng >= 2)";
+        return false;
+    }
+    if (!(g.Lx > 0) || !(g.Ly > 0) || !(g.Lz > 0) || !(g.Lu > 0) || !(g.Lv > 0) || !(g.Lg > 0)) {
+        why = "domain widths must be positive";
+        return false;
+    }
+    if (g.Nmu * g.Nom > 4096) {
+        why = "Nmu*Nom above 4096 is not supported";
+        return false;
+    }
+    const long long cells = static_cast<long long>(g.Ny + 1) * (g.Nz + 1) * g.Nmu * g.Nom * g.Ng;
+    if (cells <= 0 || cells > (1LL << 40)) {
+        why = "phase space too large";
+        return false;
+    }
+    return true;
+}
+
+struct Layout {
+    long long cells, per_e;
+    size_t elem;
+    int part_blocks;
+    int hist_cap;
+};
+
+Layout layout_of(const bfpn_grid& g, int prec, int energy_block) {
+    Layout L;
+    L.per_e = static_cast<long long>(g.Ny + 1) * (g.Nz + 1) * g.Nmu * g.Nom;
+    L.cells = L.per_e * g.Ng;
+    L.elem = prec == BFPN_PREC_FP64 ? sizeof(double) : sizeof(float);
+    L.part_blocks = std::max(energy_grid(L.per_e, energy_block), idd_partials_grid(L.per_e));
+    L.hist_cap = std::max(2 * g.Nx + 16, 4096);
+    return L;
+}
+
+uint64_t footprint(const bfpn_grid& g, int prec) {
+    const Layout L = layout_of(g, prec, 128);
+    const uint64_t arr = static_cast<uint64_t>(L.cells) * L.elem;
+    const uint64_t NA = static_cast<uint64_t>(g.Nmu) * g.Nom;
+    uint64_t b = 0;
+    b += 4 * arr;   // F, f, F1, f1
+    b += arr;       // transport target
+    b += arr;       // source
+    b += 2 * arr;   // angular contractions
+    b += static_cast<uint64_t>(g.Ng) * NA * NA * L.elem;           // ker_v
+    b += 2 * static_cast<uint64_t>(g.Ng) * g.Ng * sizeof(double);  // e1, e2
+    b += 2 * static_cast<uint64_t>(g.Ng) * NA * L.elem;            // angle factors
+    b += static_cast<uint64_t>(L.per_e) * sizeof(double);          // beam factor
+    b += 4 * static_cast<uint64_t>(L.part_blocks) * sizeof(double);
+    b += 2 * static_cast<uint64_t>(L.hist_cap) * sizeof(double);
+    b += 64ull * g.Ng * sizeof(double) + (1u << 20);               // small tables
+    return b;
+}
+
+template <typename T>
+T* as(void* p) {
+    return static_cast<T*>(p);
+}
+
+// Wraps one kernel launch: counts it and, with profiling on, brackets it with
+// CUDA events on the context stream (resolved by collect_profile).
+template <typename F>
+cudaError_t prof(bfpn_ctx* c, int cls, F&& launch) {
+    c->launches++;
+    if (!c->profiling) return launch();
+    cudaEvent_t ev[2];
+    for (auto& e : ev) {
+        if (c->ev_pool.empty()) {
+            cudaError_t r = cudaEventCreate(&e);
+            if (r != cudaSuccess) return r;
+        } else {
+            e = c->ev_pool.back();
+            c->ev_pool.pop_back();
+        }
+    }
+    cudaError_t r = cudaEventRecord(ev[0], c->stream);
+    if (r != cudaSuccess) return r;
+    r = launch();
+    if (r != cudaSuccess) return r;
+    r = cudaEventRecord(ev[1], c->stream);
+    c->pending.push_back({cls, ev[0], ev[1]});
+    return r;
+}
+
+// Adds the elapsed times of finished profiled launches to the totals.
+cudaError_t collect_profile(bfpn_ctx* c) {
+    if (c->pending.empty()) return cudaSuccess;
+    cudaError_t r = cudaStreamSynchronize(c->stream);
+    if (r != cudaSuccess) return r;
+    for (auto& p : c->pending) {
+        float ms = 0.f;
+        r = cudaEventElapsedTime(&ms, p.a, p.b);
+        if (r != cudaSuccess) return r;
+        c->prof_ms[p.cls] += ms;
+        c->prof_n[p.cls] += 1;
+        c->ev_pool.push_back(p.a);
+        c->ev_pool.push_back(p.b);
+    }
+    c->pending.clear();
+    return cudaSuccess;
+}
+
+bfpn_status dalloc(bfpn_ctx* c, void** out, size_t bytes) {
+    void* p = nullptr;
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        char msg[256];
+        std::snprintf(msg, sizeof msg, "device allocation of %.3f GiB failed: %s", bytes / 1073741824.0,
+                      cudaGetErrorString(e));
+        return fail(c, BFPN_OOM, msg);
+    }
+    c->allocs.push_back({p, bytes});
+    *out = p;
+    return BFPN_OK;
+}
+
+void free_all(bfpn_ctx* c) {
+    for (auto& p : c->pending) {
+        cudaEventDestroy(p.a);
+        cudaEventDestroy(p.b);
+    }
+    c->pending.clear();
+    for (auto e : c->ev_pool) cudaEventDestroy(e);
+    c->ev_pool.clear();
+    if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+    c->graph_exec = nullptr;
+    for (auto& b : c->allocs) cudaFree(b.p);
+    c->allocs.clear();
+}
+
+// Transport launch shape: a whole (Ny+1) x (Nz+1) plane per block when it
+// fits (updates in place); otherwise square tiles written to ctx->tmp.
+void choose_transport(bfpn_ctx* c) {
+    const size_t sz = c->elem;
+    const int Ny1 = c->Ny + 1, Nz1 = c->Nz + 1;
+    const size_t budget = 100 * 1024;
+    for (int ac : {32, 16, 8, 4}) {
+        if (ac * sz > 128) continue;
+        if (ac * sz < 32 && c->NA >= 8) break;
+        if (2ull * Ny1 * Nz1 * ac * sz <= budget) {
+            c->tr_ac = ac;
+            c->tr_ty = Ny1;
+            c->tr_tz = Nz1;
+            c->tr_inplace = true;
+            return;
+        }
+    }
+    const int ac = static_cast<int>(64 / sz);
+    int t = 8;
+    for (int cand = 64; cand >= 8; cand -= 4) {
+        const size_t s = static_cast<size_t>((cand + 8) * (cand + 8) + (cand + 4) * (cand + 4)) * ac * sz;
+        if (s <= budget) {
+            t = cand;
+            break;
+        }
+    }
+    c->tr_ac = ac;
+    c->tr_ty = std::min(t, Ny1);
+    c->tr_tz = std::min(t, Nz1);
+    c->tr_inplace = (c->tr_ty >= Ny1 && c->tr_tz >= Nz1);
+}
+
+template <typename T>
+bfpn_status upload_as(bfpn_ctx* c, void* dst, const double* host, size_t n) {
+    if (sizeof(T) == sizeof(double)) {
+        CUDA_TRY(c, cudaMemcpyAsync(dst, host, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        return BFPN_OK;
+    }
+    std::vector<T> tmp(host, host + n);
+    CUDA_TRY(c, cudaMemcpyAsync(dst, tmp.data(), n * sizeof(T), cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return BFPN_OK;
+}
+
+bfpn_status upload_state_table(bfpn_ctx* c, void* dst, const std::vector<double>& h) {
+    return c->prec == BFPN_PREC_FP64 ? upload_as<double>(c, dst, h.data(), h.size())
+                                     : upload_as<float>(c, dst, h.data(), h.size());
+}
+
+bfpn_status upload_f64(bfpn_ctx* c, void* dst, const void* host, size_t bytes) {
+    CUDA_TRY(c, cudaMemcpyAsync(dst, host, bytes, cudaMemcpyHostToDevice, c->stream));
+    return BFPN_OK;
+}
+
+// ---- operator enqueues (typed) ---------------------------------------------
+
+template <typename T>
+cudaError_t enq_energy(bfpn_ctx* c, int species, const double* coef, bool with_source, double* partials) {
+    EnergyArgs<T> a;
+    a.F = as<T>(c->st[species][0]);
+    a.f = as<T>(c->st[species][1]);
+    a.src = with_source ? as<const T>(c->src) : nullptr;
+    a.coef = coef;
+    a.Ng = c->Ng;
+    a.lanes = c->per_e;
+    if (c->p.flags & BFPN_FLAG_LEGACY_ENERGY) a.mode = EMODE_LEGACY;
+    else if (c->p.flags & BFPN_FLAG_EQ15_STRAGGLING) a.mode = EMODE_EQ15_STRAG;
+    else a.mode = EMODE_EQ15;
+    a.partials = partials;
+    a.dose_coef = c->dose_coef;
+    a.NA = c->NA;
+    a.Ny = c->Ny;
+    a.Nz = c->Nz;
+    a.trapezoidal = (c->p.flags & BFPN_FLAG_TRAPEZOIDAL_YZ) ? 1 : 0;
+    return prof(c, BFPN_KERNEL_ENERGY, [&] { return launch_energy<T>(a, c->energy_block, c->stream); });
+}
+
+template <typename T>
+cudaError_t enq_transport(bfpn_ctx* c, const void* in, void* out, double dt, bool preserve_sign) {
+    TransportArgs<T> a;
+    a.in = as<const T>(const_cast<void*>(in));
+    a.out = as<T>(out);
+    a.omega = as<const T>(c->omega);
+    a.Ny = c->Ny;
+    a.Nz = c->Nz;
+    a.NA = c->NA;
+    a.Ng = c->Ng;
+    a.dt = static_cast<T>(dt);
+    a.dy = static_cast<T>(c->d.dy);
+    a.dz = static_cast<T>(c->d.dz);
+    a.tile_y = c->tr_ty;
+    a.tile_z = c->tr_tz;
+    a.preserve_sign = preserve_sign ? 1 : 0;
+    return prof(c, BFPN_KERNEL_TRANSPORT, [&] { return launch_transport<T>(a, c->tr_ac, c->stream); });
+}
+
+template <typename T>
+cudaError_t enq_angle(bfpn_ctx* c, void* X, const void* fac) {
+    AngleArgs<T> a;
+    a.F = as<T>(X);
+    a.fac = as<const T>(const_cast<void*>(fac));
+    a.sine_u = as<const T>(c->sine_u);
+    a.sine_v = as<const T>(c->sine_v);
+    a.Nom = c->Nom;
+    a.Nmu = c->Nmu;
+    a.nyz = c->nyz;
+    a.Ng = c->Ng;
+    a.slices_per_block = c->ang_slices;
+    return prof(c, BFPN_KERNEL_ANGLE, [&] { return launch_angle<T>(a, c->stream); });
+}
+
+template <typename T>
+cudaError_t enq_source(bfpn_ctx* c) {
+    SourceArgs<T> a;
+    a.P1 = as<const T>(c->st[0][0]);
+    a.P2 = as<const T>(c->st[0][1]);
+    a.ker_v = as<const T>(c->ker_v);
+    a.groups = c->groups;
+    a.n_groups = c->n_groups;
+    a.A1 = as<T>(c->A1);
+    a.A2 = as<T>(c->A2);
+    a.S = as<T>(c->src);
+    a.e1 = c->e1;
+    a.e2 = c->e2;
+    a.tile_lo = c->tile_lo;
+    a.tile_hi = c->tile_hi;
+    a.Ng = c->Ng;
+    a.nyz = c->nyz;
+    a.NA = c->NA;
+    a.dg = c->d.dg;
+    cudaError_t e = prof(c, BFPN_KERNEL_SOURCE_ANGULAR, [&] { return launch_source_angular<T>(a, c->stream); });
+    if (e != cudaSuccess) return e;
+    return prof(c, BFPN_KERNEL_SOURCE_ENERGY, [&] { return launch_source_energy<T>(a, c->tile_e, c->stream); });
+}
+
+// transport half-step, angle full step, transport half-step on one array
+// (the per-array part of stepPrimary/stepSecondary; the operations on F and
+// f are independent, so each array runs its own T-A-T sequence).
+template <typename T>
+cudaError_t enq_tat(bfpn_ctx* c, int species, int coef, bool do_tr, bool do_an, bool preserve) {
+    void* X = c->st[species][coef];
+    const double h = 0.5 * c->d.dt;
+    cudaError_t e = cudaSuccess;
+    if (do_tr) {
+        void* Y = c->tr_inplace ? X : c->tmp;
+        e = enq_transport<T>(c, X, Y, h, preserve);
+        if (e != cudaSuccess) return e;
+        if (do_an) {
+            e = enq_angle<T>(c, Y, c->fac_step);
+            if (e != cudaSuccess) return e;
+        }
+        return enq_transport<T>(c, Y, X, h, preserve);
+    }
+    if (do_an) e = enq_angle<T>(c, X, c->fac_step);
+    return e;
+}
+
+// One depth step: the loop body of BFPnSolver::solve (bfpm_solver.cu:2201-2232).
+template <typename T>
+cudaError_t enq_step(bfpn_ctx* c, bool first, bool secondary_zero) {
+    const unsigned fl = c->p.flags;
+    const bool energy_only = fl & BFPN_FLAG_ENERGY_ONLY;
+    const bool do_tr = !(fl & BFPN_FLAG_NO_TRANSPORT), do_an = !(fl & BFPN_FLAG_NO_ANGLE);
+    double* partP = c->partials;
+    double* partS = c->partials + 2 * c->n_part;
+    cudaError_t e;
+    // stepPrimary (3238-3311) / stepPrimaryEnergyOnly (3313-3333)
+    if ((e = enq_energy<T>(c, 0, c->ecoef_half, false, nullptr)) != cudaSuccess) return e;
+    if (!energy_only) {
+        const bool clip_F = !(fl & BFPN_FLAG_NO_SPATIAL_CLIPPING);
+        if ((e = enq_tat<T>(c, 0, 0, do_tr, do_an, !clip_F)) != cudaSuccess) return e;
+        if ((e = enq_tat<T>(c, 0, 1, do_tr, do_an, true)) != cudaSuccess) return e;
+    }
+    if ((e = enq_energy<T>(c, 0, c->ecoef_half, false, partP)) != cudaSuccess) return e;
+    const int nP = energy_grid(c->per_e, c->energy_block);
+    int nS = 0;
+    const bool secondary = !energy_only && !(fl & BFPN_FLAG_PRIMARY_ONLY) && !first;
+    if (secondary) {
+        // stepSecondary (3335-3394): the source depends only on the primary,
+        // which this half does not change, so both of the reference's
+        // evaluations are the same tensor; it is built once.  Transport of
+        // the secondary always clips F1 (3355-3356) and always runs.
+        if ((e = enq_source<T>(c)) != cudaSuccess) return e;
+        if ((e = enq_energy<T>(c, 1, c->ecoef_half, true, nullptr)) != cudaSuccess) return e;
+        if ((e = enq_tat<T>(c, 1, 0, true, true, false)) != cudaSuccess) return e;
+        if ((e = enq_tat<T>(c, 1, 1, true, true, true)) != cudaSuccess) return e;
+        if ((e = enq_energy<T>(c, 1, c->ecoef_half, true, partS)) != cudaSuccess) return e;
+        nS = nP;
+    } else if (!secondary_zero) {
+        nS = idd_partials_grid(c->per_e);
+        e = prof(c, BFPN_KERNEL_IDD, [&] {
+            return launch_idd_partials<T>(as<const T>(c->st[1][0]), as<const T>(c->st[1][1]), c->dose_coef, c->Ng,
+                                          c->per_e, c->NA, c->Ny, c->Nz, (fl & BFPN_FLAG_TRAPEZOIDAL_YZ) ? 1 : 0, 0,
+                                          partS, nS, c->stream);
+        });
+        if (e != cudaSuccess) return e;
+    }
+    const double w = c->d.du * c->d.dv * c->d.dy * c->d.dz;
+    return prof(c, BFPN_KERNEL_IDD, [&] {
+        return launch_finalize_idd(partP, nP, partS, nS, w, c->d.dg, c->hist_idd, c->hist_proxy, c->counter,
+                                   c->hist_cap, 1, c->stream);
+    });
+}
+
+cudaError_t enq_step_any(bfpn_ctx* c, bool first, bool secondary_zero) {
+    return c->prec == BFPN_PREC_FP64 ? enq_step<double>(c, first, secondary_zero)
+                                     : enq_step<float>(c, first, secondary_zero);
+}
+
+bfpn_status ensure_history(bfpn_ctx* c, int needed) {
+    if (needed <= c->hist_cap) return BFPN_OK;
+    int cap = c->hist_cap;
+    while (cap < needed) cap *= 2;
+    void *ni = nullptr, *np = nullptr;
+    bfpn_status s;
+    if ((s = dalloc(c, &ni, cap * sizeof(double))) != BFPN_OK) return s;
+    if ((s = dalloc(c, &np, cap * sizeof(double))) != BFPN_OK) return s;
+    CUDA_TRY(c, cudaMemcpyAsync(ni, c->hist_idd, c->hist_cap * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(np, c->hist_proxy, c->hist_cap * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    c->hist_idd = static_cast<double*>(ni);
+    c->hist_proxy = static_cast<double*>(np);
+    c->hist_cap = cap;
+    if (c->graph_exec) {
+        cudaGraphExecDestroy(c->graph_exec);
+        c->graph_exec = nullptr;
+        c->graph_key = -1;
+    }
+    return BFPN_OK;
+}
+
+bfpn_status run_steps(bfpn_ctx* c, int nsteps) {
+    if (!c->tables_loaded) return fail(c, BFPN_NOT_READY, "tables not loaded (bfpn_load_tables)");
+    if (!c->beam_ready) return fail(c, BFPN_NOT_READY, "beam not initialised (bfpn_init_beam)");
+    if (nsteps < 0) return fail(c, BFPN_INVALID_ARG, "nsteps < 0");
+    bfpn_status s = ensure_history(c, c->steps_done + nsteps);
+    if (s != BFPN_OK) return s;
+    for (int i = 0; i < nsteps; ++i) {
+        const bool first = c->steps_done == 0;
+        const bool secondary_stepping =
+            !first && !(c->p.flags & (BFPN_FLAG_ENERGY_ONLY | BFPN_FLAG_PRIMARY_ONLY));
+        if (first || !c->use_graphs) {
+            const long long before = c->launches;
+            CUDA_TRY(c, enq_step_any(c, first, c->secondary_zero));
+            if (!first) c->kernels_per_step = static_cast<int>(c->launches - before);
+        } else {
+            const int key = c->secondary_zero ? 1 : 0;
+            if (!c->graph_exec || c->graph_key != key) {
+                if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+                c->graph_exec = nullptr;
+                cudaGraph_t graph = nullptr;
+                CUDA_TRY(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+                const long long before = c->launches;
+                cudaError_t ce = enq_step_any(c, false, c->secondary_zero);
+                c->kernels_per_step = static_cast<int>(c->launches - before);
+                cudaError_t ee = cudaStreamEndCapture(c->stream, &graph);
+                if (ce != cudaSuccess || ee != cudaSuccess) {
+                    if (graph) cudaGraphDestroy(graph);
+                    cudaGetLastError();
+                    return fail(c, BFPN_CUDA_ERROR,
+                                std::string("step capture failed: ") +
+                                    cudaGetErrorString(ce != cudaSuccess ? ce : ee));
+                }
+                ce = cudaGraphInstantiate(&c->graph_exec, graph, 0);
+                cudaGraphDestroy(graph);
+                if (ce != cudaSuccess) return fail(c, BFPN_CUDA_ERROR, std::string("graph instantiate: ") + cudaGetErrorString(ce));
+                c->graph_key = key;
+            }
+            CUDA_TRY(c, cudaGraphLaunch(c->graph_exec, c->stream));
+        }
+        if (secondary_stepping) c->secondary_zero = false;
+        c->steps_done++;
+    }
+    return BFPN_OK;
+}
+
+template <typename T>
+bfpn_status download_as(bfpn_ctx* c, const void* dev, double* host, size_t n) {
+    if (sizeof(T) == sizeof(double)) {
+        CUDA_TRY(c, cudaMemcpyAsync(host, dev, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+        return BFPN_OK;
+    }
+    std::vector<T> tmp(n);
+    CUDA_TRY(c, cudaMemcpyAsync(tmp.data(), dev, n * sizeof(T), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    for (size_t i = 0; i < n; ++i) host[i] = static_cast<double>(tmp[i]);
+    return BFPN_OK;
+}
+
+
+const std::vector<double>* table_of(const BeamTables& T, int which, std::vector<double>& tmp) {
+    switch (which) {
+        case BFPN_TABLE_S_S: return &T.S_s;
+        case BFPN_TABLE_T_C: return &T.T_c;
+        case BFPN_TABLE_SIG_TRG: return &T.sig_trg;
+        case BFPN_TABLE_SIGMA_C: return &T.sigma;
+        case BFPN_TABLE_EN: return &T.en;
+        case BFPN_TABLE_OMEND: return &T.omega;
+        case BFPN_TABLE_KER_E1: return &T.ker_e1;
+        case BFPN_TABLE_KER_E2: return &T.ker_e2;
+        case BFPN_TABLE_KER_V: return &T.ker_v;
+        case BFPN_TABLE_BAND:
+            tmp.resize(2 * static_cast<size_t>(T.Ng));
+            for (int i = 0; i < T.Ng; ++i) {
+                tmp[2 * i] = T.band_begin[i];
+                tmp[2 * i + 1] = T.band_end[i];
+            }
+            return &tmp;
+        case BFPN_TABLE_BEAM_YZA: return &T.beam_yza;
+        case BFPN_TABLE_BEAM_E: return &T.beam_e;
+        default: return nullptr;
+    }
+}
+
+bfpn_status set_device(bfpn_ctx* c) {
+    CUDA_TRY(c, cudaSetDevice(c->device));
+    return BFPN_OK;
+}
+
+}  // namespace
+
+// ============================================================================
+// C ABI
+// ============================================================================
+extern "C" {
+
+const char* bfpn_version(void) { return "bfpn-b200 0.1.0 (sm_100a)"; }
+
+const char* bfpn_status_string(bfpn_status s) {
+    switch (s) {
+        case BFPN_OK: return "ok";
+        case BFPN_INVALID_ARG: return "invalid argument";
+        case BFPN_OOM: return "out of device memory";
+        case BFPN_CUDA_ERROR: return "CUDA error";
+        case BFPN_TIMEOUT: return "timeout";
+        case BFPN_IO_ERROR: return "I/O error";
+        case BFPN_NOT_READY: return "not ready";
+        case BFPN_NO_DEVICE: return "no CUDA device";
+    }
+    return "unknown status";
+}
+
+const char* bfpn_last_error(const bfpn_ctx* ctx) { return ctx ? ctx->err.c_str() : g_create_error.c_str(); }
+
+bfpn_status bfpn_read_tables(const char* data_path, int32_t Ng, double* mu, int32_t* mu_rows, double* sigma_c,
+                             int32_t* sigma_rows) {
+    if (!data_path || !mu || !mu_rows || !sigma_c || !sigma_rows || Ng <= 0)
+        return fail(nullptr, BFPN_INVALID_ARG, "null argument or Ng <= 0");
+    std::vector<double> m, s;
+    int mr = 0, sr = 0;
+    std::string path, err;
+    if (!read_table_files(data_path, Ng, m, mr, s, sr, path, err)) return fail(nullptr, BFPN_IO_ERROR, err);
+    std::memcpy(mu, m.data(), m.size() * sizeof(double));
+    std::memcpy(sigma_c, s.data(), s.size() * sizeof(double));
+    *mu_rows = mr;
+    *sigma_rows = sr;
+    return BFPN_OK;
+}
+
+bfpn_status bfpn_host_table(const bfpn_grid* grid, const bfpn_phys* phys, const double* mu, int32_t mu_rows,
+                            const double* sigma_c, int32_t sigma_rows, int32_t which, double* out, uint64_t n,
+                            uint64_t* n_out) {
+    if (!grid || !phys || !sigma_c || !n_out || (!out && n > 0) || (!mu && mu_rows > 0))
+        return fail(nullptr, BFPN_INVALID_ARG, "null argument");
+    std::string why;
+    if (!valid_grid(*grid, why)) return fail(nullptr, BFPN_INVALID_ARG, why);
+    BeamTables T;
+    if (!build_tables(*grid, *phys, mu, mu_rows, sigma_c, sigma_rows, T, why)) return fail(nullptr, BFPN_INVALID_ARG, why);
+    std::vector<double> tmp;
+    const std::vector<double>* src = table_of(T, which, tmp);
+    if (!src) return fail(nullptr, BFPN_INVALID_ARG, "unknown table id");
+    *n_out = src->size();
+    if (src->size() > n) return fail(nullptr, BFPN_INVALID_ARG, "output buffer too small for the table");
+    std::memcpy(out, src->data(), src->size() * sizeof(double));
+    return BFPN_OK;
+}
+
+bfpn_status bfpn_footprint_bytes(const bfpn_grid* grid, const bfpn_phys* phys, int precision, uint64_t* bytes) {
+    (void)phys;
+    if (!grid || !bytes) return fail(nullptr, BFPN_INVALID_ARG, "null argument");
+    std::string why;
+    if (!valid_grid(*grid, why)) return fail(nullptr, BFPN_INVALID_ARG, why);
+    if (precision != BFPN_PREC_FP64 && precision != BFPN_PREC_MIXED)
+        return fail(nullptr, BFPN_INVALID_ARG, "unknown precision");
+    *bytes = footprint(*grid, precision);
+    return BFPN_OK;
+}
+
+bfpn_status bfpn_create(const bfpn_grid* grid, const bfpn_phys* phys, int precision, int device, bfpn_ctx** out) {
+    if (!grid || !phys || !out) return fail(nullptr, BFPN_INVALID_ARG, "null argument");
+    *out = nullptr;
+    std::string why;
+    if (!valid_grid(*grid, why)) return fail(nullptr, BFPN_INVALID_ARG, why);
+    if (precision != BFPN_PREC_FP64 && precision != BFPN_PREC_MIXED)
+        return fail(nullptr, BFPN_INVALID_ARG, "unknown precision");
+    if (!(phys->density > 0) || !(phys->energy_density > 0) || !(phys->sig_E > 0))
+        return fail(nullptr, BFPN_INVALID_ARG, "density and sigma_E must be positive");
+    if (phys->flags & BFPN_FLAG_LITE_MEMORY)
+        return fail(nullptr, BFPN_INVALID_ARG, "lite-memory mode is not provided by this solver");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(nullptr, BFPN_NO_DEVICE, "no CUDA device available");
+    }
+    if (device < 0 || device >= ndev) return fail(nullptr, BFPN_INVALID_ARG, "device ordinal out of range");
+
+    auto* c = new bfpn_ctx();
+    c->g = *grid;
+    c->p = *phys;
+    c->prec = precision;
+    c->device = device;
+    c->elem = precision == BFPN_PREC_FP64 ? sizeof(double) : sizeof(float);
+    c->d = compute_deltas(*grid);
+    c->Ng = grid->Ng;
+    c->Ny = grid->Ny;
+    c->Nz = grid->Nz;
+    c->Nmu = grid->Nmu;
+    c->Nom = grid->Nom;
+    c->nyz = (grid->Ny + 1) * (grid->Nz + 1);
+    c->NA = grid->Nmu * grid->Nom;
+    c->per_e = static_cast<long long>(c->nyz) * c->NA;
+    c->cells = c->per_e * c->Ng;
+    auto bail = [&](bfpn_status s) {
+        g_create_error = c->err;
+        free_all(c);
+        if (c->stream) cudaStreamDestroy(c->stream);
+        if (c->ev0) cudaEventDestroy(c->ev0);
+        if (c->ev1) cudaEventDestroy(c->ev1);
+        delete c;
+        return s;
+    };
+    if (set_device(c) != BFPN_OK) return bail(BFPN_CUDA_ERROR);
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
+        c->err = "stream/event creation failed";
+        return bail(BFPN_CUDA_ERROR);
+    }
+    {
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
+            const uint64_t need = footprint(*grid, precision);
+            if (need > free_b) {
+                char msg[256];
+                std::snprintf(msg, sizeof msg,
+                              "grid needs about %.2f GiB of device memory but only %.2f GiB is free", need / 1073741824.0,
+                              free_b / 1073741824.0);
+                c->err = msg;
+                return bail(BFPN_OOM);
+            }
+        }
+    }
+    choose_transport(c);
+    {
+        const size_t per_slice = 2 * static_cast<size_t>(c->NA) * c->elem;
+        c->ang_slices = static_cast<int>(std::max<size_t>(1, std::min<size_t>(32, (48 * 1024) / per_slice)));
+    }
+    const size_t arr = static_cast<size_t>(c->cells) * c->elem;
+    const Layout L = layout_of(*grid, precision, c->energy_block);
+    c->n_part = L.part_blocks;
+    c->hist_cap = L.hist_cap;
+    bfpn_status s;
+    void* v = nullptr;
+#define ALLOC(dst, bytes)                                      \
+    if ((s = dalloc(c, &v, (bytes))) != BFPN_OK) return bail(s); \
+    dst = static_cast<std::remove_reference_t<decltype(dst)>>(v);
+    for (int sp = 0; sp < 2; ++sp)
+        for (int cf = 0; cf < 2; ++cf) { ALLOC(c->st[sp][cf], arr); }
+    if (!c->tr_inplace) { ALLOC(c->tmp, arr); }
+    const bool need_secondary = !(phys->flags & (BFPN_FLAG_PRIMARY_ONLY | BFPN_FLAG_ENERGY_ONLY));
+    if (need_secondary) {
+        ALLOC(c->src, arr);
+        ALLOC(c->A1, arr);
+        ALLOC(c->A2, arr);
+    } else {
+        ALLOC(c->src, c->elem);
+    }
+    ALLOC(c->ecoef_half, static_cast<size_t>(c->Ng) * kEnergyCoef * sizeof(double));
+    ALLOC(c->ecoef_op, static_cast<size_t>(c->Ng) * kEnergyCoef * sizeof(double));
+    ALLOC(c->dose_coef, 2 * static_cast<size_t>(c->Ng) * sizeof(double));
+    ALLOC(c->omega, 2 * static_cast<size_t>(c->NA) * c->elem);
+    ALLOC(c->fac_step, static_cast<size_t>(c->Ng) * c->NA * c->elem);
+    ALLOC(c->fac_op, static_cast<size_t>(c->Ng) * c->NA * c->elem);
+    ALLOC(c->sine_u, static_cast<size_t>(c->Nom) * c->Nom * c->elem);
+    ALLOC(c->sine_v, static_cast<size_t>(c->Nmu) * c->Nmu * c->elem);
+    if (need_secondary) {
+        ALLOC(c->ker_v, static_cast<size_t>(c->Ng) * c->NA * c->NA * c->elem);
+    }
+    ALLOC(c->e1, static_cast<size_t>(c->Ng) * c->Ng * sizeof(double));
+    ALLOC(c->e2, static_cast<size_t>(c->Ng) * c->Ng * sizeof(double));
+    ALLOC(c->groups, static_cast<size_t>(c->Ng) * sizeof(int));
+    ALLOC(c->tile_lo, static_cast<size_t>(c->Ng) * sizeof(int));
+    ALLOC(c->tile_hi, static_cast<size_t>(c->Ng) * sizeof(int));
+    ALLOC(c->beam_yza, static_cast<size_t>(c->per_e) * sizeof(double));
+    ALLOC(c->beam_e, static_cast<size_t>(c->Ng) * sizeof(double));
+    ALLOC(c->partials, 4 * static_cast<size_t>(c->n_part) * sizeof(double));
+    ALLOC(c->hist_idd, static_cast<size_t>(c->hist_cap) * sizeof(double));
+    ALLOC(c->hist_proxy, static_cast<size_t>(c->hist_cap) * sizeof(double));
+    ALLOC(c->counter, sizeof(int));
+    ALLOC(c->zero_counter, sizeof(int));
+    ALLOC(c->scalar_out, 2 * sizeof(double));
+    ALLOC(c->moments, 2 * static_cast<size_t>(c->Ng) * sizeof(double));
+#undef ALLOC
+    if (need_secondary) {
+        if (cudaMemsetAsync(c->A1, 0, arr, c->stream) != cudaSuccess ||
+            cudaMemsetAsync(c->A2, 0, arr, c->stream) != cudaSuccess ||
+            cudaMemsetAsync(c->src, 0, arr, c->stream) != cudaSuccess) {
+            c->err = "memset failed";
+            return bail(BFPN_CUDA_ERROR);
+        }
+    }
+    if (cudaMemsetAsync(c->counter, 0, sizeof(int), c->stream) != cudaSuccess ||
+        cudaMemsetAsync(c->zero_counter, 0, sizeof(int), c->stream) != cudaSuccess ||
+        cudaStreamSynchronize(c->stream) != cudaSuccess) {
+        c->err = "memset failed";
+        return bail(BFPN_CUDA_ERROR);
+    }
+    *out = c;
+    return BFPN_OK;
+}
+
+bfpn_status bfpn_destroy(bfpn_ctx* ctx) {
+    if (!ctx) return BFPN_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    free_all(ctx);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    delete ctx;
+    return BFPN_OK;
+}
+
+bfpn_status bfpn_load_tables(bfpn_ctx* c, const double* mu, int32_t mu_rows, const double* sigma_c,
+                             int32_t sigma_rows) {
+    if (!c) return BFPN_INVALID_ARG;
+    if ((!mu && mu_rows > 0) || !sigma_c) return fail(c, BFPN_INVALID_ARG, "null table pointer");
+    bfpn_status s = set_device(c);
+    if (s != BFPN_OK) return s;
+    std::string err;
+    BeamTables t;
+    if (!build_tables(c->g, c->p, mu, mu_rows, sigma_c, sigma_rows, t, err)) return fail(c, BFPN_INVALID_ARG, err);
+    c->tables = std::move(t);
+    c->raw_sigma.assign(sigma_c, sigma_c + std::min<int>(sigma_rows, c->Ng));
+    BeamTables& T = c->tables;
+    const auto ecoef = energy_coefficients(T, c->p, 0.5 * c->d.dt);
+    if ((s = upload_f64(c, c->ecoef_half, ecoef.data(), ecoef.size() * sizeof(double))) != BFPN_OK) return s;
+    const auto dose = dose_coefficients(T, c->p);
+    if ((s = upload_f64(c, c->dose_coef, dose.data(), dose.size() * sizeof(double))) != BFPN_OK) return s;
+    if ((s = upload_state_table(c, c->omega, T.omega)) != BFPN_OK) return s;
+    if ((s = upload_state_table(c, c->fac_step, angle_factor(T, c->p, c->d.dt))) != BFPN_OK) return s;
+    if ((s = upload_state_table(c, c->sine_u, T.sine_u)) != BFPN_OK) return s;
+    if ((s = upload_state_table(c, c->sine_v, T.sine_v)) != BFPN_OK) return s;
+    if (c->ker_v && (s = upload_state_table(c, c->ker_v, T.ker_v)) != BFPN_OK) return s;
+    if ((s = upload_f64(c, c->e1, T.ker_e1.data(), T.ker_e1.size() * sizeof(double))) != BFPN_OK) return s;
+    if ((s = upload_f64(c, c->e2, T.ker_e2.data(), T.ker_e2.size() * sizeof(double))) != BFPN_OK) return s;
+    // source groups that some output band uses and that carry a kernel
+    std::vector<char> used(c->Ng, 0);
+    for (int e = 0; e < c->Ng; ++e)
+        for (int sg = T.band_begin[e]; sg < T.band_end[e]; ++sg) used[sg] = 1;
+    std::vector<int> groups;
+    for (int sg = 0; sg < c->Ng - 1; ++sg)
+        if (used[sg] && T.mu[sg * 3] != 0.0 && T.mu[sg * 3 + 1] != 0.0) groups.push_back(sg);
+    c->n_groups = static_cast<int>(groups.size());
+    if (!groups.empty() && (s = upload_f64(c, c->groups, groups.data(), groups.size() * sizeof(int))) != BFPN_OK)
+        return s;
+    const int tiles = (c->Ng + c->tile_e - 1) / c->tile_e;
+    std::vector<int> lo(tiles, 0), hi(tiles, 0);
+    for (int tI = 0; tI < tiles; ++tI) {
+        int l = c->Ng, h = 0;
+        for (int e = tI * c->tile_e; e < std::min(c->Ng, (tI + 1) * c->tile_e); ++e)
+            if (T.band_end[e] > T.band_begin[e]) {
+                l = std::min(l, T.band_begin[e]);
+                h = std::max(h, T.band_end[e]);
+            }
+        if (l < h) {
+            lo[tI] = l;
+            hi[tI] = h;
+        }
+    }
+    if ((s = upload_f64(c, c->tile_lo, lo.data(), lo.size() * sizeof(int))) != BFPN_OK) return s;
+    if ((s = upload_f64(c, c->tile_hi, hi.data(), hi.size() * sizeof(int))) != BFPN_OK) return s;
+    if ((s = upload_f64(c, c->beam_yza, T.beam_yza.data(), T.beam_yza.size() * sizeof(double))) != BFPN_OK) return s;
+    if ((s = upload_f64(c, c->beam_e, T.beam_e.data(), T.beam_e.size() * sizeof(double))) != BFPN_OK) return s;
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    c->tables_loaded = true;
+    c->ecoef_op_dt = -1.0;
+    c->fac_op_dt = -1.0;
+    return BFPN_OK;
+}
+
+bfpn_status bfpn_init_beam(bfpn_ctx* c) {
+    if (!c) return BFPN_INVALID_ARG;
+    if (!c->tables_loaded) return fail(c, BFPN_NOT_READY, "tables not loaded (bfpn_load_tables)");
+    bfpn_status s = set_device(c);
+    if (s != BFPN_OK) return s;
+    const size_t arr = static_cast<size_t>(c->cells) * c->elem;
+    if (c->prec == BFPN_PREC_FP64) {
+        CUDA_TRY(c, launch_init_beam<double>(as<double>(c->st[0][0]), c->beam_yza, c->beam_e, c->per_e, c->Ng, c->stream));
+    } else {
+        CUDA_TRY(c, launch_init_beam<float>(as<float>(c->st[0][0]), c->beam_yza, c->beam_e, c->per_e, c->Ng, c->stream));
+    }
+    CUDA_TRY(c, cudaMemsetAsync(c->st[0][1], 0, arr, c->stream));
+    CUDA_TRY(c, cudaMemsetAsync(c->st[1][0], 0, arr, c->stream));
+    CUDA_TRY(c, cudaMemsetAsync(c->st[1][1], 0, arr, c->stream));
+    CUDA_TRY(c, cudaMemsetAsync(c->counter, 0, sizeof(int), c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    c->beam_ready = true;
+    c->steps_done = 0;
+    c->secondary_zero = true;
+    return BFPN_OK;
+}
+
+bfpn_status bfpn_step_async(bfpn_ctx* c, int32_t nsteps) {
+    if (!c) return BFPN_INVALID_ARG;
+    bfpn_status s = set_device(c);
+    if (s != BFPN_OK) return s;
+    return run_steps(c, nsteps);
+}
+
+bfpn_status bfpn_sync(bfpn_ctx* c) {
+    if (!c) return BFPN_INVALID_ARG;
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    CUDA_TRY(c, collect_profile(c));
+    return BFPN_OK;
+}
+
+bfpn_status bfpn_history_download(bfpn_ctx* c, int32_t first, int32_t count, double* idd_out, double* proxy_out) {
+    if (!c) return BFPN_INVALID_ARG;
+    if (first < 0 || count < 0 || first + count > c->steps_done)
+        return fail(c, BFPN_INVALID_ARG, "history range outside the steps done");
+    if (count == 0) return BFPN_OK;
+    if (idd_out)
+        CUDA_TRY(c, cudaMemcpyAsync(idd_out, c->hist_idd + first, count * sizeof(double), cudaMemcpyDeviceToHost,
+                                    c->stream));
+    if (proxy_out)
+        CUDA_TRY(c, cudaMemcpyAsync(proxy_out, c->hist_proxy + first, count * sizeof(double), cudaMemcpyDeviceToHost,
+                                    c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return BFPN_OK;
+}
+
+bfpn_status bfpn_step(bfpn_ctx* c, int32_t nsteps, double* idd_out, double* proxy_out) {
+    if (!c) return BFPN_INVALID_ARG;
+    const int first = c->steps_done;
+    bfpn_status s = bfpn_step_async(c, nsteps);
+    if (s != BFPN_OK) return s;
+    if (idd_out || proxy_out) {
+        s = bfpn_history_download(c, first, nsteps, idd_out, proxy_out);
+        if (s != BFPN_OK) return s;
+    }
+    return bfpn_sync(c);
+}
+
+int32_t bfpn_steps_done(const bfpn_ctx* c) { return c ? c->steps_done : -1; }
+
+uint64_t bfpn_cells(const bfpn_ctx* c) { return c ? static_cast<uint64_t>(c->cells) : 0; }
+
+void* bfpn_stream(bfpn_ctx* c) { return c ? static_cast<void*>(c->stream) : nullptr; }
+
+bfpn_status bfpn_energy_eq15(bfpn_ctx* c, int32_t species, double dt, int32_t with_source) {
+    if (!c) return BFPN_INVALID_ARG;
+    if (!c->tables_loaded) return fail(c, BFPN_NOT_READY, "tables not loaded");
+    if (species < 0 || species > 1 || !(dt > 0)) return fail(c, BFPN_INVALID_ARG, "bad species or dt");
+    if (with_source && (species != 1 || !c->A1))
+        return fail(c, BFPN_INVALID_ARG, "the source applies to the secondary species of a context that has one");
+    bfpn_status s = set_device(c);
+    if (s != BFPN_OK) return s;
+    if (dt != c->ecoef_op_dt) {
+        const auto k = energy_coefficients(c->tables, c->p, dt);
+        if ((s = upload_f64(c, c->ecoef_op, k.data(), k.size() * sizeof(double))) != BFPN_OK) return s;
+        c->ecoef_op_dt = dt;
+    }
+    if (c->prec == BFPN_PREC_FP64) CUDA_TRY(c, enq_energy<double>(c, species, c->ecoef_op, with_source != 0, nullptr));
+    else CUDA_TRY(c, enq_energy<float>(c, species, c->ecoef_op, with_source != 0, nullptr));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return BFPN_OK;
+}
+
+bfpn_status bfpn_transport_eq18(bfpn_ctx* c, int32_t species, int32_t coef, double dt, int32_t preserve_sign) {
+    if (!c) return BFPN_INVALID_ARG;
+    if (!c->tables_loaded) return fail(c, BFPN_NOT_READY, "tables not loaded");
+    if (species < 0 || species > 1 || coef < 0 || coef > 1 || !(dt > 0))
+        return fail(c, BFPN_INVALID_ARG, "bad species, coef or dt");
+    bfpn_status s = set_device(c);
+    if (s != BFPN_OK) return s;
+    void* X = c->st[species][coef];
+    void* Y = c->tr_inplace ? X : c->tmp;
+    if (c->prec == BFPN_PREC_FP64) CUDA_TRY(c, enq_transport<double>(c, X, Y, dt, preserve_sign != 0));
+    else CUDA_TRY(c, enq_transport<float>(c, X, Y, dt, preserve_sign != 0));
+    if (Y != X)
+        CUDA_TRY(c, cudaMemcpyAsync(X, Y, static_cast<size_t>(c->cells) * c->elem, cudaMemcpyDeviceToDevice, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return BFPN_OK;
+}
+
+bfpn_status bfpn_angle_eq19(bfpn_ctx* c, int32_t species, int32_t coef, double dt) {
+    if (!c) return BFPN_INVALID_ARG;
+    if (!c->tables_loaded) return fail(c, BFPN_NOT_READY, "tables not loaded");
+    if (species < 0 || species > 1 || coef < 0 || coef > 1 || !(dt > 0))
+        return fail(c, BFPN_INVALID_ARG, "bad species, coef or dt");
+    bfpn_status s = set_device(c);
+    if (s != BFPN_OK) return s;
+    if (dt != c->fac_op_dt) {
+        if ((s = upload_state_table(c, c->fac_op, angle_factor(c->tables, c->p, dt))) != BFPN_OK) return s;
+        c->fac_op_dt = dt;
+    }
+    if (c->prec == BFPN_PREC_FP64) CUDA_TRY(c, enq_angle<double>(c, c->st[species][coef], c->fac_op));
+    else CUDA_TRY(c, enq_angle<float>(c, c->st[species][coef], c->fac_op));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return BFPN_OK;
+}
+
+bfpn_status bfpn_secondary_source(bfpn_ctx* c) {
+    if (!c) return BFPN_INVALID_ARG;
+    if (!c->tables_loaded) return fail(c, BFPN_NOT_READY, "tables not loaded");
+    if (!c->A1) return fail(c, BFPN_INVALID_ARG, "context has no secondary species (primary-only or energy-only)");
+    bfpn_status s = set_device(c);
+    if (s != BFPN_OK) return s;
+    if (c->prec == BFPN_PREC_FP64) CUDA_TRY(c, enq_source<double>(c));
+    else CUDA_TRY(c, enq_source<float>(c));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return BFPN_OK;
+}
+
+bfpn_status bfpn_idd(bfpn_ctx* c, double* idd, double* proxy) {
+    if (!c) return BFPN_INVALID_ARG;
+    if (!c->tables_loaded) return fail(c, BFPN_NOT_READY, "tables not loaded");
+    bfpn_status s = set_device(c);
+    if (s != BFPN_OK) return s;
+    const int n = idd_partials_grid(c->per_e);
+    const int trap = (c->p.flags & BFPN_FLAG_TRAPEZOIDAL_YZ) ? 1 : 0;
+    double* pP = c->partials;
+    double* pS = c->partials + 2 * c->n_part;
+    if (c->prec == BFPN_PREC_FP64) {
+        CUDA_TRY(c, launch_idd_partials<double>(as<double>(c->st[0][0]), as<double>(c->st[0][1]), c->dose_coef, c->Ng,
+                                                c->per_e, c->NA, c->Ny, c->Nz, trap, 1, pP, n, c->stream));
+        CUDA_TRY(c, launch_idd_partials<double>(as<double>(c->st[1][0]), as<double>(c->st[1][1]), c->dose_coef, c->Ng,
+                                                c->per_e, c->NA, c->Ny, c->Nz, trap, 0, pS, n, c->stream));
+    } else {
+        CUDA_TRY(c, launch_idd_partials<float>(as<float>(c->st[0][0]), as<float>(c->st[0][1]), c->dose_coef, c->Ng,
+                                               c->per_e, c->NA, c->Ny, c->Nz, trap, 1, pP, n, c->stream));
+        CUDA_TRY(c, launch_idd_partials<float>(as<float>(c->st[1][0]), as<float>(c->st[1][1]), c->dose_coef, c->Ng,
+                                               c->per_e, c->NA, c->Ny, c->Nz, trap, 0, pS, n, c->stream));
+    }
+    const double w = c->d.du * c->d.dv * c->d.dy * c->d.dz;
+    CUDA_TRY(c, launch_finalize_idd(pP, n, pS, n, w, c->d.dg, c->scalar_out, c->scalar_out + 1, c->zero_counter, 1, 0,
+                                    c->stream));
+    double h[2] = {0, 0};
+    CUDA_TRY(c, cudaMemcpyAsync(h, c->scalar_out, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    if (idd) *idd = h[0];
+    if (proxy) *proxy = h[1];
+    return BFPN_OK;
+}
+
+bfpn_status bfpn_state_upload(bfpn_ctx* c, int32_t species, int32_t coef, const double* host) {
+    if (!c || !host) return BFPN_INVALID_ARG;
+    if (species < 0 || species > 1 || coef < 0 || coef > 1) return fail(c, BFPN_INVALID_ARG, "bad species or coef");
+    bfpn_status s = set_device(c);
+    if (s != BFPN_OK) return s;
+    s = c->prec == BFPN_PREC_FP64 ? upload_as<double>(c, c->st[species][coef], host, c->cells)
+                                  : upload_as<float>(c, c->st[species][coef], host, c->cells);
+    if (s != BFPN_OK) return s;
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    if (species == 1) c->secondary_zero = false;
+    c->beam_ready = true;
+    return BFPN_OK;
+}
+
+bfpn_status bfpn_state_download(bfpn_ctx* c, int32_t species, int32_t coef, double* host) {
+    if (!c || !host) return BFPN_INVALID_ARG;
+    if (species < 0 || species > 1 || coef < 0 || coef > 1) return fail(c, BFPN_INVALID_ARG, "bad species or coef");
+    bfpn_status s = set_device(c);
+    if (s != BFPN_OK) return s;
+    return c->prec == BFPN_PREC_FP64 ? download_as<double>(c, c->st[species][coef], host, c->cells)
+                                     : download_as<float>(c, c->st[species][coef], host, c->cells);
+}
+
+bfpn_status bfpn_source_download(bfpn_ctx* c, double* host) {
+    if (!c || !host) return BFPN_INVALID_ARG;
+    if (!c->A1) return fail(c, BFPN_INVALID_ARG, "context has no secondary species");
+    bfpn_status s = set_device(c);
+    if (s != BFPN_OK) return s;
+    return c->prec == BFPN_PREC_FP64 ? download_as<double>(c, c->src, host, c->cells)
+                                     : download_as<float>(c, c->src, host, c->cells);
+}
+
+bfpn_status bfpn_table_download(bfpn_ctx* c, int32_t which, double* host, uint64_t n) {
+    if (!c || !host) return BFPN_INVALID_ARG;
+    if (!c->tables_loaded) return fail(c, BFPN_NOT_READY, "tables not loaded");
+    std::vector<double> tmp;
+    const std::vector<double>* src = table_of(c->tables, which, tmp);
+    if (!src) return fail(c, BFPN_INVALID_ARG, "unknown table id");
+    if (src->size() > n) return fail(c, BFPN_INVALID_ARG, "host buffer too small for the table");
+    std::memcpy(host, src->data(), src->size() * sizeof(double));
+    return BFPN_OK;
+}
+
+bfpn_status bfpn_set_profiling(bfpn_ctx* c, int32_t on) {
+    if (!c) return BFPN_INVALID_ARG;
+    CUDA_TRY(c, collect_profile(c));
+    c->profiling = on != 0;
+    c->use_graphs = !c->profiling;
+    return BFPN_OK;
+}
+
+bfpn_status bfpn_kernel_profile(bfpn_ctx* c, double* ms_out, int32_t* launches_out, int32_t n) {
+    if (!c) return BFPN_INVALID_ARG;
+    CUDA_TRY(c, collect_profile(c));
+    for (int i = 0; i < std::min<int>(n, BFPN_KERNEL_CLASSES); ++i) {
+        if (ms_out) ms_out[i] = c->prof_ms[i];
+        if (launches_out) launches_out[i] = c->prof_n[i];
+    }
+    return BFPN_OK;
+}
+
+bfpn_status bfpn_kernel_profile_reset(bfpn_ctx* c) {
+    if (!c) return BFPN_INVALID_ARG;
+    CUDA_TRY(c, collect_profile(c));
+    for (int i = 0; i < BFPN_KERNEL_CLASSES; ++i) {
+        c->prof_ms[i] = 0.0;
+        c->prof_n[i] = 0;
+    }
+    return BFPN_OK;
+}
+
+int32_t bfpn_kernels_per_step(bfpn_ctx* c) { return c ? c->kernels_per_step : -1; }
+
+int32_t bfpn_source_groups(bfpn_ctx* c) { return c ? c->n_groups : -1; }
+
+bfpn_status bfpn_timed_steps(bfpn_ctx* c, int32_t nsteps, double* elapsed_ms) {
+    if (!c || !elapsed_ms) return BFPN_INVALID_ARG;
+    bfpn_status s = set_device(c);
+    if (s != BFPN_OK) return s;
+    CUDA_TRY(c, cudaEventRecord(c->ev0, c->stream));
+    s = run_steps(c, nsteps);
+    if (s != BFPN_OK) return s;
+    CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
+    CUDA_TRY(c, cudaEventSynchronize(c->ev1));
+    float ms = 0.f;
+    CUDA_TRY(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    *elapsed_ms = ms;
+    CUDA_TRY(c, collect_profile(c));
+    return BFPN_OK;
+}
+
+bfpn_status bfpn_setup_summary(bfpn_ctx* c, bfpn_setup_info* out) {
+    if (!c || !out) return BFPN_INVALID_ARG;
+    if (!c->tables_loaded) return fail(c, BFPN_NOT_READY, "tables not loaded");
+    const BeamTables& T = c->tables;
+    out->mu_rows = T.mu_rows;
+    // bfpm_solver.cu:1494-1500
+    const int bg = std::max(0, std::min(static_cast<int>((c->p.beam_energy - 1.0) / c->d.dg), c->Ng - 1));
+    out->beam_group = bg;
+    out->beam_group_energy = (bg + 0.5) * c->d.dg + 1.0;
+    out->sigma_fitted = c->raw_sigma.empty() ? 0.0 : c->raw_sigma[bg];
+    out->sigma_used = T.sigma[bg];
+    out->omega_center_y = T.omega_center_y;
+    out->omega_center_z = T.omega_center_z;
+    out->spatial_mass = T.spatial_mass;
+    out->angular_mass = T.angular_mass;
+    out->energy_mass = T.energy_mass;
+    out->initial_scale = T.initial_scale;
+    return BFPN_OK;
+}
+
+bfpn_status bfpn_energy_moments(bfpn_ctx* c, double* out) {
+    if (!c || !out) return BFPN_INVALID_ARG;
+    bfpn_status s = set_device(c);
+    if (s != BFPN_OK) return s;
+    const double w = c->d.du * c->d.dv * c->d.dy * c->d.dz;
+    if (c->prec == BFPN_PREC_FP64)
+        CUDA_TRY(c, launch_energy_moments<double>(as<double>(c->st[0][0]), as<double>(c->st[0][1]), as<double>(c->st[1][0]),
+                                                  as<double>(c->st[1][1]), c->Ng, c->per_e, w, c->moments, c->stream));
+    else
+        CUDA_TRY(c, launch_energy_moments<float>(as<float>(c->st[0][0]), as<float>(c->st[0][1]), as<float>(c->st[1][0]),
+                                                 as<float>(c->st[1][1]), c->Ng, c->per_e, w, c->moments, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(out, c->moments, 2 * static_cast<size_t>(c->Ng) * sizeof(double),
+                                cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return BFPN_OK;
+}
+
+int32_t bfpn_device_count(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+int32_t bfpn_device_info(int32_t device, char* buf, int32_t buf_len) {
+    cudaDeviceProp prop;
+    if (!buf || buf_len <= 0 || cudaGetDeviceProperties(&prop, device) != cudaSuccess) {
+        cudaGetLastError();
+        return -1;
+    }
+    int n = std::snprintf(buf, buf_len,
+                          "Device %d: %s\n  Compute Capability: %d.%d\n  Total Memory: %zu MB\n"
+                          "  Multiprocessors: %d\n  Max Threads/Block: %d\n",
+                          device, prop.name, prop.major, prop.minor, prop.totalGlobalMem / (1024 * 1024),
+                          prop.multiProcessorCount, prop.maxThreadsPerBlock);
+    return n < buf_len ? n : buf_len - 1;
+}
+
+}  // extern "C"

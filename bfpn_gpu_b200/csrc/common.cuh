@@ -1,0 +1,132 @@
+// Shared definitions of the B200 BFPn depth-step kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace bfpn {
+
+// include/config.hpp:38-41 of the reference.
+constexpr double kEpsilon = 1e-10;
+
+// Number of double coefficients per energy group in the energy-sweep table
+// (see tables.cpp: build_energy_coefficients).
+constexpr int kEnergyCoef = 20;
+enum EnergyCoef {
+    EC_INV_F = 0,      // 1 / max(1/dt + a_lo/2 + sig/2, eps)
+    EC_A = 1,          // 1.5 a_hi * inv_F
+    EC_F_FROM_F = 2,   // 0.5 a_lo * inv_F
+    EC_F_FROM_HI = 3,  // 0.5 a_hi * inv_F
+    EC_C_UP = 4,       // 0.5 a_hi          (common term: up)
+    EC_C_CUR = 5,      // -0.5 a_lo         (common term: cur)
+    EC_C_F = 6,        // 1/dt - 0.5 sig    (common term: F_g)
+    EC_R_F = 7,        // coefficient of f_g in rhs1e + rhs2e
+    EC_R_UP = 8,       // 1.5 a_hi
+    EC_R_CUR = 9,      // 1.5 a_lo
+    EC_R_FG = 10,      // -1.5 (a_lo + a_hi)
+    EC_R_HI = 11,      // 1.5 a_hi - 0.5 A a_hi
+    EC_INV_COE = 12,   // 1 / max(coe, eps)
+    EC_S_HI = 13,      // straggling: 0.5 rho T_hi / dg2
+    EC_S_LO = 14,      // straggling: 0.5 rho T_lo / dg2
+    EC_S_G = 15,       // straggling: rho T_g / dg2
+    EC_L_IDT = 16,     // legacy: 1/dt
+    EC_L_HI = 17,      // legacy: rho S_hi / dg
+    EC_L_INV_DEN = 18, // legacy: 1 / max(denominator, eps)
+    EC_L_LAP = 19      // legacy straggling: 0.5 dt T_g / dg2 (0 when off)
+};
+
+enum EnergyMode { EMODE_EQ15 = 0, EMODE_EQ15_STRAG = 1, EMODE_LEGACY = 2 };
+
+// Arguments of one energy half-step over one species.
+template <typename T>
+struct EnergyArgs {
+    T* F;                  // psi^1, in place
+    T* f;                  // psi^2, in place
+    const T* src;          // catastrophic source of psi^1, or nullptr
+    const double* coef;    // [Ng][kEnergyCoef]
+    int Ng;
+    long long lanes;       // nyz * NA
+    int mode;              // EnergyMode
+    // fused IDD (nullptr partials = off)
+    double* partials;      // [gridDim.x][2]: dose part, psi^2 part
+    const double* dose_coef;  // [Ng][2]: weight of psi^1 and psi^2
+    int NA, Ny, Nz;
+    int trapezoidal;
+};
+
+// Arguments of one transport half-step (Eq. 18) over one array.
+template <typename T>
+struct TransportArgs {
+    const T* in;
+    T* out;                // == in only when one tile covers a whole plane
+    const T* omega;        // [NA][2]: omega_y, omega_z
+    int Ny, Nz, NA, Ng;
+    T dt, dy, dz;
+    int tile_y, tile_z;    // output tile (positions)
+    int preserve_sign;
+};
+
+// Arguments of one angular-diffusion step (Eq. 19) over one array.
+template <typename T>
+struct AngleArgs {
+    T* F;                  // in place
+    const T* fac;          // [Ng][NA] CN ratio * 4/((Nom+1)(Nmu+1))
+    const T* sine_u;       // [Nom][Nom]
+    const T* sine_v;       // [Nmu][Nmu]
+    int Nom, Nmu, nyz, Ng;
+    int slices_per_block;
+};
+
+// Arguments of the factorised catastrophic source.
+template <typename T>
+struct SourceArgs {
+    const T* P1;           // primary psi^1
+    const T* P2;           // primary psi^2
+    const T* ker_v;        // [Ng][NA][NA]  (src, in, out)
+    const int* groups;     // source groups with a non-zero angular kernel that some output uses
+    int n_groups;
+    T* A1;                 // [Ng][nyz][NA] angular contraction of max(P1, 0)
+    T* A2;                 // [Ng][nyz][NA] angular contraction of P2
+    T* S;                  // [Ng][nyz][NA] output source
+    const double* e1;      // [Ng][Ng] ker_e1, row = output group
+    const double* e2;      // [Ng][Ng] ker_e2
+    const int* tile_lo;    // per output-group tile: first source group of the union band
+    const int* tile_hi;    // per output-group tile: one past the last
+    int Ng, nyz, NA;
+    double dg;
+};
+
+// Launchers (kernels_*.cu).  All return the launch status.
+template <typename T> cudaError_t launch_energy(const EnergyArgs<T>& a, int block, cudaStream_t s);
+template <typename T> cudaError_t launch_transport(const TransportArgs<T>& a, int ang_chunk, cudaStream_t s);
+template <typename T> cudaError_t launch_angle(const AngleArgs<T>& a, cudaStream_t s);
+template <typename T> cudaError_t launch_source_angular(const SourceArgs<T>& a, cudaStream_t s);
+template <typename T> cudaError_t launch_source_energy(const SourceArgs<T>& a, int tile_e, cudaStream_t s);
+template <typename T> cudaError_t launch_init_beam(T* F, const double* yza, const double* e, long long per_e,
+                                                   int Ng, cudaStream_t s);
+
+// Sum of partials [n][2] (plus column 0 of partials2 [n2][2]) into
+// hist_idd[*counter] and hist_proxy[*counter], scaled by idd_scale (column 0)
+// and proxy_scale (column 1 of partials only); increments the counter when
+// advance != 0.  n and n2 may be 0.
+cudaError_t launch_finalize_idd(const double* partials, int n, const double* partials2, int n2,
+                                double idd_scale, double proxy_scale, double* hist_idd,
+                                double* hist_proxy, int* counter, int capacity, int advance,
+                                cudaStream_t s);
+// Stand-alone IDD partials of one species (F, f) when it was not fused into
+// an energy pass.  partials: [grid][2].
+template <typename T>
+cudaError_t launch_idd_partials(const T* F, const T* f, const double* dose_coef, int Ng, long long lanes,
+                                int NA, int Ny, int Nz, int trapezoidal, int with_proxy, double* partials,
+                                int grid, cudaStream_t s);
+// Per-group moments (Eq. 25 diagnostics): out[2*ek] += sum psi^1, out[2*ek+1] += sum psi^2.
+template <typename T>
+cudaError_t launch_energy_moments(const T* F, const T* f, const T* F1, const T* f1, int Ng, long long per_e,
+                                  double weight, double* out, cudaStream_t s);
+template <typename Tin, typename Tout>
+cudaError_t launch_convert(const Tin* in, Tout* out, long long n, cudaStream_t s);
+
+int energy_grid(long long lanes, int block);
+int idd_partials_grid(long long lanes);
+
+}  // namespace bfpn

@@ -1,0 +1,274 @@
+/*
+ * bfpn_capi.h -- C ABI of the B200 BFPn pencil-beam depth-step solver.
+ *
+ * Plain C types only: pointers, sizes, doubles and ints.  No CUDA or torch
+ * types appear in the signatures, so any FFI (ctypes, cgo, JNI) can bind it.
+ *
+ * Phase-space layout (HBM, one array per species x DG coefficient):
+ *     index = (ek * nyz + pos) * NA + ang
+ *     pos   = iz * (Ny + 1) + iy          nyz = (Ny + 1) * (Nz + 1)
+ *     ang   = iv * Nom + iu               NA  = Nmu * Nom
+ * which is the index order of the reference (bfpm_solver.cu:1996,
+ * spatial_transport.cu:46-47).  species 0 = primary, 1 = secondary;
+ * coef 0 = psi^1 (F), coef 1 = psi^2 (f).
+ *
+ * Every function returns a bfpn_status; on failure bfpn_last_error(ctx)
+ * gives a message.  Nothing here calls exit().
+ */
+#ifndef BFPN_CAPI_H
+#define BFPN_CAPI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum bfpn_status {
+    BFPN_OK = 0,
+    BFPN_INVALID_ARG = 1,
+    BFPN_OOM = 2,
+    BFPN_CUDA_ERROR = 3,
+    BFPN_TIMEOUT = 4,
+    BFPN_IO_ERROR = 5,
+    BFPN_NOT_READY = 6,
+    BFPN_NO_DEVICE = 7
+} bfpn_status;
+
+/* Grid sizes and domain widths.  Mirrors GridParams (bfpm_solver.cuh:21-27);
+ * the deltas are derived as in GridParams::computeDeltas
+ * (bfpm_solver.cu:1116-1127): dt=Lx/Nx, dy=Ly/Ny, dz=Lz/Nz, dg=Lg/Ng,
+ * du=Lu/(Nom+1), dv=Lv/(Nmu+1). */
+typedef struct bfpn_grid {
+    int32_t Nx, Ny, Nz, Ng, Nmu, Nom;
+    double Lx, Ly, Lz, Lu, Lv, Lg;
+} bfpn_grid;
+
+/* Material presets (main.cu:123-138); selects the Bethe composition used
+ * by the stopping-power ratio (bfpm_solver.cu:184-196). */
+enum {
+    BFPN_MATERIAL_NONE = 0, /* no --material given: water composition */
+    BFPN_MATERIAL_WATER = 1,
+    BFPN_MATERIAL_BONE = 2,
+    BFPN_MATERIAL_AIR = 3
+};
+
+/* Physics / mode switches (PhysicsParams, bfpm_solver.cuh:30-62). */
+enum {
+    BFPN_FLAG_PRIMARY_ONLY = 1u << 0,
+    BFPN_FLAG_LEGACY_ENERGY = 1u << 1,
+    BFPN_FLAG_EQ15_STRAGGLING = 1u << 2,
+    BFPN_FLAG_SAVE_ENERGY_MOMENTS = 1u << 3,
+    BFPN_FLAG_ENERGY_ONLY = 1u << 4,
+    BFPN_FLAG_NO_TRANSPORT = 1u << 5,
+    BFPN_FLAG_NO_ANGLE = 1u << 6,
+    BFPN_FLAG_NO_SPATIAL_CLIPPING = 1u << 7,
+    BFPN_FLAG_DISCRETE_ANGLE_DELTA = 1u << 8,
+    BFPN_FLAG_NORMALIZE_INITIAL_MASS = 1u << 9,
+    BFPN_FLAG_TRAPEZOIDAL_YZ = 1u << 10,
+    BFPN_FLAG_DOSE_CATASTROPHIC_LOSS = 1u << 11,
+    BFPN_FLAG_CALIBRATE_CROSS_SECTIONS = 1u << 12,
+    BFPN_FLAG_LITE_MEMORY = 1u << 13
+};
+
+typedef struct bfpn_phys {
+    double sig_E;          /* initial energy Gaussian sigma, MeV */
+    double a_1;            /* 1 / (2 sigma_yz^2) */
+    double a_2;            /* 1 / (2 sigma_angle^2) */
+    double C_c;            /* carried for interface parity; unused on the path */
+    double beam_energy;    /* E0, MeV */
+    double density;        /* g/cm^3; used by transport-angle factor and dose */
+    double energy_density; /* density used inside the energy sweep */
+    int32_t material;      /* BFPN_MATERIAL_* */
+    uint32_t flags;        /* BFPN_FLAG_* */
+} bfpn_phys;
+
+/* Arithmetic of the device state.
+ * FP64:  every operator in double (parity mode, 1e-10 relative to the oracle).
+ * MIXED: float state; the energy DG/CN recursion, the source energy
+ *        contraction accumulators and the IDD accumulation stay double. */
+enum { BFPN_PREC_FP64 = 0, BFPN_PREC_MIXED = 1 };
+
+/* Set-up tables that bfpn_table_download can return (sizes in doubles). */
+enum {
+    BFPN_TABLE_S_S = 0,      /* Ng+1 stopping power at the DG nodes */
+    BFPN_TABLE_T_C = 1,      /* Ng straggling */
+    BFPN_TABLE_SIG_TRG = 2,  /* Ng transport cross-section */
+    BFPN_TABLE_SIGMA_C = 3,  /* Ng catastrophic cross-section as used */
+    BFPN_TABLE_EN = 4,       /* Ng+1 energy nodes */
+    BFPN_TABLE_OMEND = 5,    /* 2*NA directions (omega_y, omega_z) */
+    BFPN_TABLE_KER_E1 = 6,   /* Ng*Ng */
+    BFPN_TABLE_KER_E2 = 7,   /* Ng*Ng */
+    BFPN_TABLE_KER_V = 8,    /* Ng*NA*NA, [src][in][out] */
+    BFPN_TABLE_BAND = 9,     /* 2*Ng: begin, end source groups per output */
+    BFPN_TABLE_BEAM_YZA = 10,/* nyz*NA transverse-angular beam factor */
+    BFPN_TABLE_BEAM_E = 11   /* Ng energy beam factor */
+};
+
+typedef struct bfpn_ctx bfpn_ctx;
+
+/* ---- version / errors ------------------------------------------------ */
+const char* bfpn_version(void);
+const char* bfpn_status_string(bfpn_status s);
+/* Message of the last failure on ctx (or of the last failed bfpn_create when
+ * ctx is NULL).  Valid until the next call on the same context. */
+const char* bfpn_last_error(const bfpn_ctx* ctx);
+
+/* ---- solver context: replaces BFPnSolver (bfpm_solver.cuh:97-253) ----- */
+
+/* File part of BFPnSolver::initialize (bfpm_solver.cu:1435-1480): reads the
+ * first Ng rows of <data_path>/data_cross.txt (data_b.txt / data_a.txt for a
+ * bone / air directory) into mu (Ng*3, zero-filled) and of cross_total.txt
+ * into sigma_c (Ng).  Returns BFPN_IO_ERROR when a file cannot be opened;
+ * the row counts let the caller apply the reference's checks (done again by
+ * bfpn_load_tables). */
+bfpn_status bfpn_read_tables(const char* data_path, int32_t Ng, double* mu, int32_t* mu_rows,
+                             double* sigma_c, int32_t* sigma_rows);
+
+
+/* One set-up table (BFPN_TABLE_*) built on the host from the same inputs
+ * bfpn_load_tables takes, without a context or a GPU.  *n_out receives the
+ * table length; n = capacity of out in doubles. */
+bfpn_status bfpn_host_table(const bfpn_grid* grid, const bfpn_phys* phys, const double* mu, int32_t mu_rows,
+                            const double* sigma_c, int32_t sigma_rows, int32_t which, double* out, uint64_t n,
+                            uint64_t* n_out);
+
+/* Device bytes a context of this shape needs (state, source, work buffers,
+ * tables).  Replaces the reference's preflightMemory estimate
+ * (bfpm_solver.cu:1321-1433).  Pure host arithmetic; no GPU needed. */
+bfpn_status bfpn_footprint_bytes(const bfpn_grid* grid, const bfpn_phys* phys,
+                                 int precision, uint64_t* bytes);
+
+/* BFPnSolver::BFPnSolver (bfpm_solver.cu:1171-1207) + allocateMemory.
+ * device: CUDA ordinal.  Allocates all device memory up front. */
+bfpn_status bfpn_create(const bfpn_grid* grid, const bfpn_phys* phys,
+                        int precision, int device, bfpn_ctx** out);
+bfpn_status bfpn_destroy(bfpn_ctx* ctx);
+
+/* Table part of BFPnSolver::initialize (bfpm_solver.cu:1435-1568):
+ * mu is mu_rows x 3 (mu1, mu2, mu3), sigma_c has sigma_rows values, both
+ * as read from data_cross.txt / cross_total.txt.  Rows beyond mu_rows are
+ * zero (the reference accepts Ng-1 rows); sigma_rows must equal Ng.
+ * Builds S_s, T_c, sig_trg, ker_e1/e2, band limits, ker_v, directions and
+ * the DST factors, and uploads them. */
+bfpn_status bfpn_load_tables(bfpn_ctx* ctx, const double* mu, int32_t mu_rows,
+                             const double* sigma_c, int32_t sigma_rows);
+
+/* BFPnSolver::initializeDistribution, full mode (bfpm_solver.cu:1815-2026):
+ * Gaussian y/z, near-delta angle, Gaussian energy; F = f1*f2, f = F1 = f1 = 0.
+ * Also resets the step counter. */
+bfpn_status bfpn_init_beam(bfpn_ctx* ctx);
+
+/* nsteps depth steps of BFPnSolver::solve (bfpm_solver.cu:2166-2267):
+ * stepPrimary, stepSecondary (skipped on the context's first step), IDD and
+ * dose proxy.  idd_out / proxy_out (host, nsteps doubles each) may be NULL.
+ * The steps run as one CUDA graph replay per step with no host sync inside;
+ * the call returns after the last step completed. */
+bfpn_status bfpn_step(bfpn_ctx* ctx, int32_t nsteps, double* idd_out, double* proxy_out);
+
+/* Enqueue nsteps without waiting and without copying results back; results
+ * stay in the device history (bfpn_history_download). */
+bfpn_status bfpn_step_async(bfpn_ctx* ctx, int32_t nsteps);
+bfpn_status bfpn_sync(bfpn_ctx* ctx);
+/* Copy IDD / proxy history entries [first, first+count) to the host. */
+bfpn_status bfpn_history_download(bfpn_ctx* ctx, int32_t first, int32_t count,
+                                  double* idd_out, double* proxy_out);
+int32_t bfpn_steps_done(const bfpn_ctx* ctx);
+
+/* ---- per-operator entry points (the sub-solver calls of stepPrimary /
+ *      stepSecondary, bfpm_solver.cu:3238-3394) -------------------------- */
+
+/* EnergyDepositionSolver::solve (energy_solver.cu:444-506), in place on
+ * (F, f) of `species`, half-step dt.  with_source=1 adds the secondary
+ * source computed by bfpn_secondary_source (species 1 only), as
+ * solveSecondaryFromPrimary does (energy_solver.cu:508-573). */
+bfpn_status bfpn_energy_eq15(bfpn_ctx* ctx, int32_t species, double dt, int32_t with_source);
+
+/* SpatialTransportSolver::solveEq18 (spatial_transport.cu:202-262) on one
+ * array; preserve_sign=1 disables the max(.,0) clipping. */
+bfpn_status bfpn_transport_eq18(bfpn_ctx* ctx, int32_t species, int32_t coef,
+                                double dt, int32_t preserve_sign);
+
+/* AngleDiffusionSolver::solveEq19 (angle_diffusion.cu:420-483) on one array
+ * with step dt (the full depth step in the reference's use). */
+bfpn_status bfpn_angle_eq19(bfpn_ctx* ctx, int32_t species, int32_t coef, double dt);
+
+/* secondarySourceFromPrimaryKernel (energy_solver.cu:287-333): source of the
+ * secondary species from the current primary state, into the context's
+ * source buffer. */
+bfpn_status bfpn_secondary_source(bfpn_ctx* ctx);
+
+/* computeIntegratedDepthDose + computeScalarDoseProxy
+ * (bfpm_solver.cu:3473-3502, 3418-3444) of the current state. */
+bfpn_status bfpn_idd(bfpn_ctx* ctx, double* idd, double* proxy);
+
+/* State transfer of one array (cells doubles, converted to the device
+ * precision on upload). */
+bfpn_status bfpn_state_upload(bfpn_ctx* ctx, int32_t species, int32_t coef, const double* host);
+bfpn_status bfpn_state_download(bfpn_ctx* ctx, int32_t species, int32_t coef, double* host);
+bfpn_status bfpn_source_download(bfpn_ctx* ctx, double* host);
+uint64_t bfpn_cells(const bfpn_ctx* ctx);
+
+/* One set-up table (BFPN_TABLE_*); n = capacity of host in doubles. */
+bfpn_status bfpn_table_download(bfpn_ctx* ctx, int32_t which, double* host, uint64_t n);
+
+/* Kernel classes of the per-kernel profile. */
+enum {
+    BFPN_KERNEL_ENERGY = 0,         /* energy sweep (with fused IDD partials) */
+    BFPN_KERNEL_TRANSPORT = 1,      /* MUSCL predictor-corrector */
+    BFPN_KERNEL_ANGLE = 2,          /* DST-I angular diffusion */
+    BFPN_KERNEL_SOURCE_ANGULAR = 3, /* source: angular contraction */
+    BFPN_KERNEL_SOURCE_ENERGY = 4,  /* source: banded energy contraction */
+    BFPN_KERNEL_IDD = 5,            /* IDD partials / final sum */
+    BFPN_KERNEL_CLASSES = 6
+};
+
+/* With profiling on, steps run eagerly (no graph) and every launch is
+ * bracketed by CUDA events on the context stream; bfpn_kernel_profile
+ * returns, per kernel class, the summed device time (ms) and the launch count
+ * since the last reset.  n = entries the arrays hold (BFPN_KERNEL_CLASSES). */
+bfpn_status bfpn_set_profiling(bfpn_ctx* ctx, int32_t on);
+bfpn_status bfpn_kernel_profile(bfpn_ctx* ctx, double* ms_out, int32_t* launches_out, int32_t n);
+bfpn_status bfpn_kernel_profile_reset(bfpn_ctx* ctx);
+/* Kernel launches one regular depth step issues (after the first step). */
+int32_t bfpn_kernels_per_step(bfpn_ctx* ctx);
+/* Source groups whose angular contraction the secondary source computes. */
+int32_t bfpn_source_groups(bfpn_ctx* ctx);
+
+/* bfpn_step_async(nsteps) bracketed by CUDA events on the context stream;
+ * waits and returns the device time of the steps in *elapsed_ms. */
+bfpn_status bfpn_timed_steps(bfpn_ctx* ctx, int32_t nsteps, double* elapsed_ms);
+
+/* Set-up quantities the reference prints during initialize
+ * (bfpm_solver.cu:1476-1500, 1536-1540, 1878-1880). */
+typedef struct bfpn_setup_info {
+    int32_t mu_rows;          /* explicit scattering rows read */
+    int32_t beam_group;       /* group of the beam energy */
+    double beam_group_energy; /* its midpoint, MeV */
+    double sigma_fitted;      /* sigma_c of that group before calibration */
+    double sigma_used;        /* after the optional legacy calibration */
+    double omega_center_y, omega_center_z;
+    double spatial_mass, angular_mass, energy_mass, initial_scale;
+} bfpn_setup_info;
+bfpn_status bfpn_setup_summary(bfpn_ctx* ctx, bfpn_setup_info* out);
+
+/* Per-group integrals of psi^1 and psi^2 (primary + secondary) over y, z, u,
+ * v of the current state (energyMomentKernel, bfpm_solver.cu:311-360), the
+ * Eq. 25 diagnostic: out[2*g] = psi^1 integral, out[2*g+1] = psi^2 integral. */
+bfpn_status bfpn_energy_moments(bfpn_ctx* ctx, double* out);
+
+/* ---- devices (printGPUInfo, main.cu:25-42) ---------------------------- */
+int32_t bfpn_device_count(void);
+/* One line per device property in the reference's format; returns the number
+ * of bytes written (excluding the terminating zero), or -1. */
+int32_t bfpn_device_info(int32_t device, char* buf, int32_t buf_len);
+/* Raw stream handle (cudaStream_t) of the context, for callers that order
+ * their own work against it. */
+void* bfpn_stream(bfpn_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BFPN_CAPI_H */

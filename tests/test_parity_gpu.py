@@ -1,0 +1,223 @@
+"""CUDA path against the oracle, through the C ABI (lib/libbfpn_b200.so).
+
+FP64 mode: every operator and whole depth steps agree with the CPU FP64
+restatement to 1e-10 relative (operators 1e-11), on seeded states, and the full
+1000-step water 230 MeV runs reproduce the reference's own golden IDD files.
+Mixed mode (float state, double energy recursion): IDD within 1e-3 of the
+peak against FP64.
+"""
+import numpy as np
+import pytest
+
+from conftest import golden_config, load_golden, material_tables, rel_err, table_dir
+from bfpn_gpu_b200 import Context, capi, make_config, read_tables
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+OP_TOL = 1e-11
+STEP_TOL = 1e-10
+
+
+def small_cfg(**kw):
+    base = dict(nx=160, ny=6, nz=5, nmu=4, nom=5, ng=40, ly=2.0, lz=1.5, lu=1.0, lv=1.2, lg=59.0, beam_energy=40.0,
+                sigma_e=2.0, sigma_yz=0.4, material_name="water", t_final=4.0)
+    base.update(kw)
+    return make_config(**base)
+
+
+def build(cfg, tables="synthetic500", precision=capi.PREC_FP64):
+    mu, sig = read_tables(table_dir(tables), cfg.ng)
+    ctx = Context(cfg.grid(), cfg.phys(), precision)
+    ctx.load_tables(mu, sig)
+    ctx.init_beam()
+    ora = O.Oracle(cfg.grid(), cfg.phys(), mu, sig)
+    return ctx, ora
+
+
+def seeded_states(ctx, seed):
+    rng = np.random.default_rng(seed)
+    Ng, nyz, NA = ctx.shape
+    beam = ctx.table(capi.TABLE_BEAM_YZA, nyz * NA).reshape(nyz, NA)
+    e = np.exp(-0.5 * ((np.arange(Ng) - 0.7 * Ng) / (0.1 * Ng)) ** 2)
+    F = (e[:, None, None] * (beam / max(beam.max(), 1e-300))[None] + 1e-3 * rng.random((Ng, nyz, NA))).ravel()
+    f = 1e-3 * rng.standard_normal(Ng * nyz * NA)
+    F1 = 1e-2 * rng.random(Ng * nyz * NA)
+    f1 = 1e-3 * rng.standard_normal(Ng * nyz * NA)
+    return F, f, F1, f1
+
+
+def set_both(ctx, ora, states):
+    for k, arr in enumerate(states):
+        ctx.set_state(k // 2, k % 2, arr)
+        ora.set_state(k // 2, k % 2, arr)
+
+
+def assert_states(ctx, ora, tol, which=((0, 0), (0, 1), (1, 0), (1, 1))):
+    for sp, cf in which:
+        r = rel_err(ctx.get_state(sp, cf), ora.get_state(sp, cf))
+        assert r < tol, ("species", sp, "coef", cf, r)
+
+
+@pytest.mark.parametrize("flags", [{}, {"legacy_energy": True}, {"eq15_straggling": True},
+                                   {"legacy_energy": True, "eq15_straggling": True}])
+def test_energy_operator(flags):
+    cfg = small_cfg(**flags)
+    ctx, ora = build(cfg)
+    set_both(ctx, ora, seeded_states(ctx, 1))
+    h = 0.5 * cfg.dt()
+    ctx.energy(0, h)
+    ora.energy(0, h)
+    assert_states(ctx, ora, OP_TOL, ((0, 0), (0, 1)))
+
+
+def test_secondary_source_and_sourced_energy():
+    cfg = small_cfg()
+    ctx, ora = build(cfg)
+    set_both(ctx, ora, seeded_states(ctx, 2))
+    ctx.secondary_source()
+    s_gpu = ctx.source()
+    s_ora = ora.source()
+    assert np.abs(s_ora).max() > 0
+    assert rel_err(s_gpu, s_ora) < OP_TOL
+    ora.use_direct_source(True)  # the reference's own summation order
+    assert rel_err(s_gpu, ora.source()) < OP_TOL
+    h = 0.5 * cfg.dt()
+    ctx.energy(1, h, with_source=True)
+    ora.energy(1, h, with_source=True)
+    assert_states(ctx, ora, OP_TOL, ((1, 0), (1, 1)))
+
+
+@pytest.mark.parametrize("preserve", [False, True])
+@pytest.mark.parametrize("shape", [dict(), dict(ny=40, nz=33, nmu=2, nom=3, ng=3)])
+def test_transport_operator(preserve, shape):
+    cfg = small_cfg(**shape)
+    ctx, ora = build(cfg)
+    set_both(ctx, ora, seeded_states(ctx, 3))
+    for sp, cf in ((0, 0), (0, 1)):
+        ctx.transport(sp, cf, 0.5 * cfg.dt(), preserve)
+        ora.transport(sp, cf, 0.5 * cfg.dt(), preserve)
+    assert_states(ctx, ora, OP_TOL, ((0, 0), (0, 1)))
+
+
+def test_angle_operator():
+    cfg = small_cfg(nmu=7, nom=6)
+    ctx, ora = build(cfg)
+    set_both(ctx, ora, seeded_states(ctx, 4))
+    for sp, cf in ((0, 0), (1, 1)):
+        ctx.angle(sp, cf, cfg.dt())
+        ora.angle(sp, cf, cfg.dt())
+    assert_states(ctx, ora, OP_TOL)
+
+
+def test_idd_operator():
+    cfg = small_cfg(trapezoidal_yz=True)
+    ctx, ora = build(cfg)
+    set_both(ctx, ora, seeded_states(ctx, 5))
+    a, b = ctx.idd()
+    c, d = ora.idd()
+    assert abs(a - c) <= 1e-12 * abs(c)
+    assert abs(b - d) <= 1e-12 * abs(d)
+
+
+@pytest.mark.parametrize("flags", [
+    {},
+    {"trapezoidal_yz": True, "discrete_angle_delta": True, "normalize_initial_mass": True},
+    {"no_spatial_clipping": True},
+    {"primary_only": True},
+    {"energy_only": True},
+    {"no_transport": True},
+    {"no_angle": True},
+    {"legacy_energy": True},
+    {"eq15_straggling": True},
+    {"legacy_cross": True},
+    {"material_name": "bone", "density": 1.85, "energy_density": 1.85},
+])
+def test_depth_steps_fp64(flags):
+    flags = dict(flags)
+    legacy_cross = flags.pop("legacy_cross", False)
+    cfg = small_cfg(**flags)
+    if legacy_cross:
+        cfg.calibrate_cross_sections = True
+    ctx, ora = build(cfg)
+    n = 12
+    idd_g, prox_g = ctx.step(n)
+    idd_o, prox_o = ora.step(n)
+    assert np.abs(idd_o).max() > 0
+    assert rel_err(idd_g, idd_o) < STEP_TOL
+    assert rel_err(prox_g, prox_o) < STEP_TOL
+    assert_states(ctx, ora, STEP_TOL)
+
+
+def test_depth_steps_tiled_transport():
+    cfg = small_cfg(ny=40, nz=36, nmu=3, nom=2, ng=12, lg=20.0, beam_energy=15.0, ly=4.0, lz=4.0)
+    ctx, ora = build(cfg)
+    idd_g, _ = ctx.step(6)
+    idd_o, _ = ora.step(6)
+    assert rel_err(idd_g, idd_o) < STEP_TOL
+    assert_states(ctx, ora, STEP_TOL)
+
+
+def test_step_api_pieces_agree():
+    """bfpn_step in one call == step by step == async + history download."""
+    cfg = small_cfg()
+    a, _ = build(cfg)
+    b, _ = build(cfg)
+    c, _ = build(cfg)
+    ia, pa = a.step(9)
+    ib = np.concatenate([b.step(1)[0] for _ in range(9)])
+    c.step_async(4)
+    c.step_async(5)
+    c.sync()
+    ic, pc = c.history()
+    assert np.array_equal(ia, ib)
+    assert np.array_equal(ia, ic) and np.array_equal(pa, pc)
+
+
+@pytest.mark.parametrize("grid", ["8_7", "12_9"])
+def test_reference_golden_full_run_fp64(grid):
+    """All 1000 depth steps of the reference's golden water 230 MeV runs."""
+    cfg = golden_config(grid)
+    mu, sig = material_tables(cfg, "water")
+    ctx = Context(cfg.grid(), cfg.phys(), capi.PREC_FP64)
+    ctx.load_tables(mu, sig)
+    ctx.init_beam()
+    idd, _ = ctx.step(cfg.max_steps())
+    gold = load_golden(grid)
+    assert idd.shape[0] == gold.shape[0]
+    assert rel_err(idd, gold[:, 1]) < STEP_TOL
+    big = gold[:, 1] > 0.01 * gold[:, 1].max()
+    assert (np.abs(idd - gold[:, 1])[big] / gold[big, 1]).max() < 1e-9
+
+
+def test_mixed_precision_idd_within_tolerance():
+    cfg = small_cfg(t_final=8.0)
+    mu, sig = read_tables(table_dir("synthetic500"), cfg.ng)
+    ref = Context(cfg.grid(), cfg.phys(), capi.PREC_FP64)
+    mix = Context(cfg.grid(), cfg.phys(), capi.PREC_MIXED)
+    for c in (ref, mix):
+        c.load_tables(mu, sig)
+        c.init_beam()
+    n = cfg.max_steps()
+    i_ref, _ = ref.step(n)
+    i_mix, _ = mix.step(n)
+    assert rel_err(i_mix, i_ref) < 1e-3
+
+
+def test_errors_are_reported_not_fatal():
+    cfg = small_cfg()
+    ctx = Context(cfg.grid(), cfg.phys())
+    with pytest.raises(capi.BfpnError):
+        ctx.step(1)  # tables not loaded
+    mu, sig = read_tables(table_dir("synthetic500"), cfg.ng)
+    with pytest.raises(capi.BfpnError):
+        ctx.load_tables(mu[: cfg.ng - 3], sig)  # too few scattering rows
+    with pytest.raises(capi.BfpnError):
+        ctx.load_tables(mu, sig[:-1])  # sigma rows != Ng
+    ctx.load_tables(mu, sig)
+    with pytest.raises(capi.BfpnError):
+        ctx.step(1)  # beam not initialised
+    ctx.init_beam()
+    ctx.step(2)
+    with pytest.raises(capi.BfpnError):
+        ctx.transport(3, 0, 0.1, False)
