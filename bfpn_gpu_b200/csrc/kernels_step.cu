@@ -9,8 +9,12 @@
 #include "common.cuh"
 
 #include <algorithm>
+#include <cmath>
 
 namespace bfpn {
+
+template <typename T>
+cudaError_t launch_angle_generic(const AngleArgs<T>& a, cudaStream_t s);
 
 // ---------------------------------------------------------------------------
 // Energy sweep (energyDgCnKernel, energy_solver.cu:41-161).
@@ -327,8 +331,137 @@ __global__ void __launch_bounds__(256) angle_kernel(AngleArgs<T> a) {
     }
 }
 
+// Square angular grids (Nom == Nmu == N <= 32): one thread owns a whole row
+// (or column) of a slice in registers.  The DST-I matrix is symmetric and
+// S[m][N-1-i] = (-1)^m S[m][i], so y = S x needs only the first ceil(N/2)
+// columns applied to x[i] +- x[N-1-i]: N*ceil(N/2) FMAs per row instead of N^2.
+// The half table travels by value as a kernel parameter, so its entries are
+// constant-bank operands of the FMAs (no shared-memory traffic for it).
+template <int N, typename T>
+struct SineHalf {
+    T h[N][(N + 1) / 2];
+};
+
+template <int N, typename T>
+__device__ __forceinline__ void dst1(const SineHalf<N, T>& S, const T (&x)[N], T (&y)[N]) {
+    constexpr int H = N / 2, HC = (N + 1) / 2;
+    T p[HC], q[H > 0 ? H : 1];
+#pragma unroll
+    for (int i = 0; i < H; ++i) {
+        p[i] = x[i] + x[N - 1 - i];
+        q[i] = x[i] - x[N - 1 - i];
+    }
+    if (N & 1) p[H] = x[H];
+#pragma unroll
+    for (int m = 0; m < N; ++m) {
+        T acc = T(0);
+        if ((m & 1) == 0) {
+#pragma unroll
+            for (int i = 0; i < HC; ++i) acc += S.h[m][i] * p[i];
+        } else {
+#pragma unroll
+            for (int i = 0; i < H; ++i) acc += S.h[m][i] * q[i];
+        }
+        y[m] = acc;
+    }
+}
+
+template <int N, typename T>
+__global__ void __launch_bounds__(256) angle_dst_kernel(AngleArgs<T> a, SineHalf<N, T> S) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int NA = N * N, RS = N + 1;  // padded row stride: conflict-free row and column access
+    T* X = reinterpret_cast<T*>(smem_raw);
+    const int SL = a.slices_per_block;
+    const long long total = static_cast<long long>(a.Ng) * a.nyz;
+    const long long s0 = static_cast<long long>(blockIdx.x) * SL;
+    const int ns = static_cast<int>(min(static_cast<long long>(SL), total - s0));
+    T* __restrict__ F = a.F + s0 * NA;
+    for (int e = threadIdx.x; e < ns * NA; e += blockDim.x) {
+        const int s = e / NA, r = e - s * NA, v = r / N, u = r - v * N;
+        X[(s * N + v) * RS + u] = F[e];
+    }
+    __syncthreads();
+    T x[N], y[N];
+    for (int row = threadIdx.x; row < ns * N; row += blockDim.x) {  // forward u
+        T* R = X + row * RS;
+#pragma unroll
+        for (int k = 0; k < N; ++k) x[k] = R[k];
+        dst1<N, T>(S, x, y);
+#pragma unroll
+        for (int k = 0; k < N; ++k) R[k] = y[k];
+    }
+    __syncthreads();
+    for (int col = threadIdx.x; col < ns * N; col += blockDim.x) {  // forward v, factor, inverse v
+        const int s = col / N, mu = col - s * N;
+        T* C = X + s * N * RS + mu;
+#pragma unroll
+        for (int k = 0; k < N; ++k) x[k] = C[k * RS];
+        dst1<N, T>(S, x, y);
+        const T* __restrict__ fac = a.fac + ((s0 + s) / a.nyz) * NA + mu;
+#pragma unroll
+        for (int k = 0; k < N; ++k) y[k] *= fac[k * N];
+        dst1<N, T>(S, y, x);
+#pragma unroll
+        for (int k = 0; k < N; ++k) C[k * RS] = x[k];
+    }
+    __syncthreads();
+    for (int row = threadIdx.x; row < ns * N; row += blockDim.x) {  // inverse u
+        T* R = X + row * RS;
+#pragma unroll
+        for (int k = 0; k < N; ++k) x[k] = R[k];
+        dst1<N, T>(S, x, y);
+#pragma unroll
+        for (int k = 0; k < N; ++k) R[k] = y[k];
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < ns * NA; e += blockDim.x) {
+        const int s = e / NA, r = e - s * NA, v = r / N, u = r - v * N;
+        F[e] = X[(s * N + v) * RS + u];
+    }
+}
+
+template <int N, typename T>
+static cudaError_t launch_angle_dst(const AngleArgs<T>& a, cudaStream_t s) {
+    SineHalf<N, T> S;
+    // sine_u lives on the device; the host copy of the half table is built
+    // from the same formula the tables use (angle_diffusion.cu:393-397).
+    for (int m = 0; m < N; ++m)
+        for (int i = 0; i < (N + 1) / 2; ++i)
+            S.h[m][i] = static_cast<T>(std::sin(3.14159265358979323846 * (m + 1) * (i + 1) / (N + 1)));
+    const int SL = std::max(1, 256 / N);
+    const size_t smem = static_cast<size_t>(SL) * N * (N + 1) * sizeof(T);
+    auto kern = angle_dst_kernel<N, T>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    AngleArgs<T> b = a;
+    b.slices_per_block = SL;
+    const long long total = static_cast<long long>(a.Ng) * a.nyz;
+    const long long blocks = (total + SL - 1) / SL;
+    if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+    kern<<<static_cast<unsigned>(blocks), 256, smem, s>>>(b, S);
+    return cudaGetLastError();
+}
+
 template <typename T>
 cudaError_t launch_angle(const AngleArgs<T>& a, cudaStream_t s) {
+    if (a.Nom == a.Nmu) {
+        switch (a.Nom) {
+#define BFPN_DST_CASE(n) \
+    case n: return launch_angle_dst<n, T>(a, s);
+            BFPN_DST_CASE(2) BFPN_DST_CASE(3) BFPN_DST_CASE(4) BFPN_DST_CASE(5) BFPN_DST_CASE(6) BFPN_DST_CASE(7)
+            BFPN_DST_CASE(8) BFPN_DST_CASE(9) BFPN_DST_CASE(10) BFPN_DST_CASE(11) BFPN_DST_CASE(12)
+            BFPN_DST_CASE(13) BFPN_DST_CASE(14) BFPN_DST_CASE(15) BFPN_DST_CASE(16) BFPN_DST_CASE(17)
+            BFPN_DST_CASE(18) BFPN_DST_CASE(19) BFPN_DST_CASE(20) BFPN_DST_CASE(21) BFPN_DST_CASE(22)
+            BFPN_DST_CASE(23) BFPN_DST_CASE(24) BFPN_DST_CASE(28) BFPN_DST_CASE(32)
+#undef BFPN_DST_CASE
+            default: break;
+        }
+    }
+    return launch_angle_generic(a, s);
+}
+
+template <typename T>
+cudaError_t launch_angle_generic(const AngleArgs<T>& a, cudaStream_t s) {
     const int NA = a.Nom * a.Nmu;
     const size_t smem = (static_cast<size_t>(a.Nom) * a.Nom + static_cast<size_t>(a.Nmu) * a.Nmu
                          + 2 * static_cast<size_t>(a.slices_per_block) * NA) * sizeof(T);

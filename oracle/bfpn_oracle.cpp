@@ -100,6 +100,10 @@ struct Model {
     std::vector<double> mu, sigma, S_s, T_c, sig_trg, en, Omend;
     std::vector<double> ker_e1, ker_e2, ker_v, sine_u, sine_v;
     std::vector<int> beg, end;
+    // non-zero entries of ker_v per (source group, input direction), outputs ascending
+    std::vector<size_t> kv_ptr;
+    std::vector<int> kv_out;
+    std::vector<double> kv_w;
     std::vector<double> beam_yza, beam_e;
     std::vector<double> st[2][2];  // [species][coef]
     std::vector<double> source;
@@ -272,6 +276,21 @@ static bool build_tables(Model& m, const double* mu_in, int mu_rows,
             }
         }
     }
+
+    m.kv_ptr.assign(static_cast<size_t>(Ng) * NA + 1, 0);
+    m.kv_out.clear();
+    m.kv_w.clear();
+    for (size_t r = 0; r < static_cast<size_t>(Ng) * NA; ++r) {
+        m.kv_ptr[r] = m.kv_w.size();
+        for (int out = 0; out < NA; ++out) {
+            double w = m.ker_v[r * NA + out];
+            if (w != 0.0) {
+                m.kv_out.push_back(out);
+                m.kv_w.push_back(w);
+            }
+        }
+    }
+    m.kv_ptr[static_cast<size_t>(Ng) * NA] = m.kv_w.size();
 
     // sine tables, angle_diffusion.cu:381-413
     m.sine_u.resize(static_cast<size_t>(m.Nom) * m.Nom);
@@ -621,17 +640,18 @@ static void source_factorised(Model& m) {
     for (long long b = 0; b < static_cast<long long>(Ng) * m.nyz; ++b) {
         int s = static_cast<int>(b / m.nyz);
         if (!used[s]) continue;
-        const double* kv = m.ker_v.data() + static_cast<size_t>(s) * NA * NA;
         const double* p1 = P1 + b * NA;
         const double* p2 = P2 + b * NA;
         double* o1 = m.a1.data() + b * NA;
         double* o2 = m.a2.data() + b * NA;
+        // zero kernel entries are skipped (they add exact zeros), which keeps
+        // the dense order of summation for every output
         for (int in = 0; in < NA; ++in) {
             double x1 = std::max(p1[in], 0.0), x2 = p2[in];
-            const double* row = kv + static_cast<size_t>(in) * NA;
-            for (int out = 0; out < NA; ++out) {
-                o1[out] += x1 * row[out];
-                o2[out] += x2 * row[out];
+            const size_t r = static_cast<size_t>(s) * NA + in;
+            for (size_t k = m.kv_ptr[r]; k < m.kv_ptr[r + 1]; ++k) {
+                o1[m.kv_out[k]] += x1 * m.kv_w[k];
+                o2[m.kv_out[k]] += x2 * m.kv_w[k];
             }
         }
     }
