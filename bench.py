@@ -359,7 +359,11 @@ def main():
     ap.add_argument("--accuracy-steps", type=int, default=1000)
     ap.add_argument("--cpu-steps", type=int, default=1)
     ap.add_argument("--reference-budget-s", type=float, default=120.0)
+    ap.add_argument("--ng", type=int, default=None,
+                    help="energy groups (profiling captures on a smaller state; not for bench lines)")
     args = ap.parse_args()
+    if args.ng:
+        WORKLOAD["ng"] = args.ng
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -33,6 +33,8 @@ FLAG_TRAPEZOIDAL_YZ = 1 << 10
 FLAG_DOSE_CATASTROPHIC_LOSS = 1 << 11
 FLAG_CALIBRATE_CROSS_SECTIONS = 1 << 12
 FLAG_LITE_MEMORY = 1 << 13
+# run-time options
+OPT_TENSOR_CORES, OPT_CUDA_GRAPHS = 0, 1
 # kernel classes of the profile
 KERNEL_CLASSES = ["energy", "transport", "angle", "source_angular", "source_energy", "idd"]
 # tables
@@ -93,6 +95,7 @@ SIGNATURES = {
     "bfpn_kernel_profile_reset": (ctypes.c_int, [_vp]),
     "bfpn_kernels_per_step": (_i32, [_vp]),
     "bfpn_timed_steps": (ctypes.c_int, [_vp, _i32, _dp]),
+    "bfpn_set_option": (ctypes.c_int, [_vp, _i32, _i32]),
     "bfpn_source_groups": (_i32, [_vp]),
     "bfpn_setup_summary": (ctypes.c_int, [_vp, _vp]),
     "bfpn_energy_moments": (ctypes.c_int, [_vp, _dp]),
@@ -315,6 +318,9 @@ class Context:
         ms = ctypes.c_double(0)
         self._check(lib().bfpn_timed_steps(self._h, n, ctypes.byref(ms)))
         return float(ms.value)
+
+    def set_option(self, option, value):
+        self._check(lib().bfpn_set_option(self._h, option, int(value)))
 
     def source_groups(self):
         return int(lib().bfpn_source_groups(self._h))

@@ -77,6 +77,10 @@ struct bfpn_ctx {
     int hist_cap = 0;
     int* counter = nullptr;
     int* zero_counter = nullptr;    // scratch counter for one-off IDD reductions
+    int* dev_err = nullptr;         // device error word (bounded waits that ran out)
+    void* bblob = nullptr;          // split-bf16 angular kernel tiles for the tensor-core source
+    bool use_umma = true;
+    int umma_nt = 0, umma_bk = 32, umma_ntiles = 0;
     double* scalar_out = nullptr;   // [2] one-off IDD / proxy
     double* moments = nullptr;      // [Ng][2]
 
@@ -267,11 +271,12 @@ void free_all(bfpn_ctx* c) {
 void choose_transport(bfpn_ctx* c) {
     const size_t sz = c->elem;
     const int Ny1 = c->Ny + 1, Nz1 = c->Nz + 1;
-    const size_t budget = 100 * 1024;
-    for (int ac : {32, 16, 8, 4}) {
-        if (ac * sz > 128) continue;
+    const size_t budget = 72 * 1024;  // three blocks per SM at least
+    // whole plane per block, the widest angle chunk (32..64 contiguous bytes) that fits
+    for (int ac : {16, 8, 4}) {
+        if (ac * sz > 64) continue;
         if (ac * sz < 32 && c->NA >= 8) break;
-        if (2ull * Ny1 * Nz1 * ac * sz <= budget) {
+        if (transport_smem(Ny1, Nz1, Ny1, Nz1, ac, sz) <= budget) {
             c->tr_ac = ac;
             c->tr_ty = Ny1;
             c->tr_tz = Nz1;
@@ -279,18 +284,18 @@ void choose_transport(bfpn_ctx* c) {
             return;
         }
     }
-    const int ac = static_cast<int>(64 / sz);
-    int t = 8;
-    for (int cand = 64; cand >= 8; cand -= 4) {
-        const size_t s = static_cast<size_t>((cand + 8) * (cand + 8) + (cand + 4) * (cand + 4)) * ac * sz;
-        if (s <= budget) {
-            t = cand;
+    // square tiles with 32-byte angle chunks, balanced over the plane
+    const int ac = std::max(1, static_cast<int>(32 / sz));
+    int tmax = 4;
+    for (int cand = 64; cand >= 4; --cand)
+        if (transport_smem(Ny1, Nz1, cand, cand, ac, sz) <= budget) {
+            tmax = cand;
             break;
         }
-    }
+    const int ky = (Ny1 + tmax - 1) / tmax, kz = (Nz1 + tmax - 1) / tmax;
     c->tr_ac = ac;
-    c->tr_ty = std::min(t, Ny1);
-    c->tr_tz = std::min(t, Nz1);
+    c->tr_ty = (Ny1 + ky - 1) / ky;
+    c->tr_tz = (Nz1 + kz - 1) / kz;
     c->tr_inplace = (c->tr_ty >= Ny1 && c->tr_tz >= Nz1);
 }
 
@@ -392,7 +397,17 @@ cudaError_t enq_source(bfpn_ctx* c) {
     a.nyz = c->nyz;
     a.NA = c->NA;
     a.dg = c->d.dg;
-    cudaError_t e = prof(c, BFPN_KERNEL_SOURCE_ANGULAR, [&] { return launch_source_angular<T>(a, c->stream); });
+    cudaError_t e;
+    if (sizeof(T) == sizeof(float) && c->use_umma && c->bblob) {
+        e = prof(c, BFPN_KERNEL_SOURCE_ANGULAR, [&] {
+            return launch_source_angular_umma(as<const float>(c->st[0][0]), as<const float>(c->st[0][1]),
+                                              static_cast<const uint8_t*>(c->bblob), c->groups, c->n_groups,
+                                              as<float>(c->A1), as<float>(c->A2), c->dev_err, c->nyz, c->NA, c->umma_nt,
+                                              c->umma_bk, c->umma_ntiles, c->stream);
+        });
+    } else {
+        e = prof(c, BFPN_KERNEL_SOURCE_ANGULAR, [&] { return launch_source_angular<T>(a, c->stream); });
+    }
     if (e != cudaSuccess) return e;
     return prof(c, BFPN_KERNEL_SOURCE_ENERGY, [&] { return launch_source_energy<T>(a, c->tile_e, c->stream); });
 }
@@ -552,6 +567,17 @@ bfpn_status download_as(bfpn_ctx* c, const void* dev, double* host, size_t n) {
     return BFPN_OK;
 }
 
+
+// Reads and clears the device error word that kernels with bounded waits set
+// when a wait ran out (the stream must be idle).
+bfpn_status check_device_error(bfpn_ctx* c) {
+    if (!c->dev_err) return BFPN_OK;
+    int h = 0;
+    CUDA_TRY(c, cudaMemcpy(&h, c->dev_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (h == 0) return BFPN_OK;
+    CUDA_TRY(c, cudaMemset(c->dev_err, 0, sizeof(int)));
+    return fail(c, BFPN_TIMEOUT, "a bounded device wait ran out (code " + std::to_string(h) + "); results of the step are invalid");
+}
 
 const std::vector<double>* table_of(const BeamTables& T, int which, std::vector<double>& tmp) {
     switch (which) {
@@ -762,6 +788,7 @@ bfpn_status bfpn_create(const bfpn_grid* grid, const bfpn_phys* phys, int precis
     ALLOC(c->hist_proxy, static_cast<size_t>(c->hist_cap) * sizeof(double));
     ALLOC(c->counter, sizeof(int));
     ALLOC(c->zero_counter, sizeof(int));
+    ALLOC(c->dev_err, sizeof(int));
     ALLOC(c->scalar_out, 2 * sizeof(double));
     ALLOC(c->moments, 2 * static_cast<size_t>(c->Ng) * sizeof(double));
 #undef ALLOC
@@ -775,6 +802,7 @@ bfpn_status bfpn_create(const bfpn_grid* grid, const bfpn_phys* phys, int precis
     }
     if (cudaMemsetAsync(c->counter, 0, sizeof(int), c->stream) != cudaSuccess ||
         cudaMemsetAsync(c->zero_counter, 0, sizeof(int), c->stream) != cudaSuccess ||
+        cudaMemsetAsync(c->dev_err, 0, sizeof(int), c->stream) != cudaSuccess ||
         cudaStreamSynchronize(c->stream) != cudaSuccess) {
         c->err = "memset failed";
         return bail(BFPN_CUDA_ERROR);
@@ -828,6 +856,18 @@ bfpn_status bfpn_load_tables(bfpn_ctx* c, const double* mu, int32_t mu_rows, con
     c->n_groups = static_cast<int>(groups.size());
     if (!groups.empty() && (s = upload_f64(c, c->groups, groups.data(), groups.size() * sizeof(int))) != BFPN_OK)
         return s;
+    if (c->prec == BFPN_PREC_MIXED && c->A1 && !groups.empty()) {
+        // tensor-core source: output tiles of <= 256 columns, multiples of 16
+        c->umma_ntiles = (c->NA + 255) / 256;
+        c->umma_nt = ((c->NA + c->umma_ntiles - 1) / c->umma_ntiles + 15) / 16 * 16;
+        std::vector<uint8_t> blob;
+        build_umma_blob(T.ker_v.data(), groups.data(), c->n_groups, c->NA, c->umma_nt, c->umma_bk, blob);
+        void* d = nullptr;
+        if ((s = dalloc(c, &d, blob.size())) != BFPN_OK) return s;
+        if ((s = upload_f64(c, d, blob.data(), blob.size())) != BFPN_OK) return s;
+        CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+        c->bblob = d;
+    }
     const int tiles = (c->Ng + c->tile_e - 1) / c->tile_e;
     std::vector<int> lo(tiles, 0), hi(tiles, 0);
     for (int tI = 0; tI < tiles; ++tI) {
@@ -886,7 +926,7 @@ bfpn_status bfpn_sync(bfpn_ctx* c) {
     if (!c) return BFPN_INVALID_ARG;
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     CUDA_TRY(c, collect_profile(c));
-    return BFPN_OK;
+    return check_device_error(c);
 }
 
 bfpn_status bfpn_history_download(bfpn_ctx* c, int32_t first, int32_t count, double* idd_out, double* proxy_out) {
@@ -984,6 +1024,26 @@ bfpn_status bfpn_secondary_source(bfpn_ctx* c) {
     if (c->prec == BFPN_PREC_FP64) CUDA_TRY(c, enq_source<double>(c));
     else CUDA_TRY(c, enq_source<float>(c));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return check_device_error(c);
+}
+
+bfpn_status bfpn_set_option(bfpn_ctx* c, int32_t option, int32_t value) {
+    if (!c) return BFPN_INVALID_ARG;
+    switch (option) {
+        case BFPN_OPT_TENSOR_CORES:
+            c->use_umma = value != 0;
+            break;
+        case BFPN_OPT_CUDA_GRAPHS:
+            c->use_graphs = value != 0 && !c->profiling;
+            break;
+        default:
+            return fail(c, BFPN_INVALID_ARG, "unknown option");
+    }
+    if (c->graph_exec) {
+        cudaGraphExecDestroy(c->graph_exec);
+        c->graph_exec = nullptr;
+        c->graph_key = -1;
+    }
     return BFPN_OK;
 }
 
@@ -1106,7 +1166,7 @@ bfpn_status bfpn_timed_steps(bfpn_ctx* c, int32_t nsteps, double* elapsed_ms) {
     CUDA_TRY(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
     *elapsed_ms = ms;
     CUDA_TRY(c, collect_profile(c));
-    return BFPN_OK;
+    return check_device_error(c);
 }
 
 bfpn_status bfpn_setup_summary(bfpn_ctx* c, bfpn_setup_info* out) {

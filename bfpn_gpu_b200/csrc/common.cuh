@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <vector>
 
 namespace bfpn {
 
@@ -125,6 +126,20 @@ cudaError_t launch_energy_moments(const T* F, const T* f, const T* F1, const T* 
                                   double weight, double* out, cudaStream_t s);
 template <typename Tin, typename Tout>
 cudaError_t launch_convert(const Tin* in, Tout* out, long long n, cudaStream_t s);
+
+// Tensor-core (tcgen05) angular contraction of the source, float state
+// (kernels_umma.cu).  bblob from build_umma_blob; err receives a non-zero
+// code if a CTA's bounded wait ran out.
+cudaError_t launch_source_angular_umma(const float* P1, const float* P2, const uint8_t* bblob, const int* groups,
+                                       int n_groups, float* A1, float* A2, int* err, int nyz, int NA, int NT, int BK,
+                                       int n_ntiles, cudaStream_t s);
+// Host: split-bf16 B tiles of ker_v ([Ng][NA][NA] double) for the listed
+// groups, in the kernel's shared-memory layout.
+void build_umma_blob(const double* ker_v, const int* groups, int n_groups, int NA, int NT, int BK,
+                     std::vector<uint8_t>& blob);
+
+// Dynamic shared memory of one transport block (tile ty x tz, ac angles).
+size_t transport_smem(int Ny1, int Nz1, int ty, int tz, int ac, size_t elem);
 
 int energy_grid(long long lanes, int block);
 int idd_partials_grid(long long lanes);

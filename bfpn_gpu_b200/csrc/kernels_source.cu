@@ -99,47 +99,87 @@ cudaError_t launch_source_angular(const SourceArgs<T>& a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-// Energy stage: one thread per lane, TE output groups per block; the source
-// groups of the union band of those outputs are streamed once and applied to
-// all TE accumulators (zeros outside each output's band contribute nothing).
-// Accumulation in double; blockIdx.x walks the output tiles so that blocks
-// sharing a lane range run together and share A rows through L2.
-template <typename T, int TE>
+// Energy stage: TE output groups per block and LN lanes per thread.  The
+// source groups of the union band of the TE outputs are streamed once; the
+// band coefficients of a chunk of SC source groups are staged in shared
+// memory as [s][t] rows (one vector broadcast load feeds 4 (float) or 2
+// (double) accumulators), and zeros outside an output's own band add
+// nothing.  Accumulation in the state precision; blockIdx.x walks the output
+// tiles so blocks sharing a lane range run together and share A rows in L2.
+template <typename T, int TE, int LN>
 __global__ void __launch_bounds__(128) source_energy_kernel(SourceArgs<T> a) {
+    constexpr int SC = 32;
+    __shared__ __align__(16) T E1[SC][TE];
+    __shared__ __align__(16) T E2[SC][TE];
     const int tile = blockIdx.x;
     const long long per_e = static_cast<long long>(a.nyz) * a.NA;
-    const long long l = static_cast<long long>(blockIdx.y) * blockDim.x + threadIdx.x;
-    if (l >= per_e) return;
+    const long long l0 = static_cast<long long>(blockIdx.y) * blockDim.x * LN + threadIdx.x;
     const int Ng = a.Ng, e0 = tile * TE;
     const int lo = a.tile_lo[tile], hi = a.tile_hi[tile];
-    double q1[TE], q2[TE];
+    T q1[TE][LN], q2[TE][LN];
 #pragma unroll
-    for (int t = 0; t < TE; ++t) { q1[t] = 0.0; q2[t] = 0.0; }
-    for (int s = lo; s < hi; ++s) {
-        const double x1 = static_cast<double>(a.A1[s * per_e + l]);
-        const double x2 = static_cast<double>(a.A2[s * per_e + l]);
+    for (int t = 0; t < TE; ++t)
 #pragma unroll
-        for (int t = 0; t < TE; ++t) {
-            const int e = min(e0 + t, Ng - 1);
-            q1[t] += __ldg(a.e1 + static_cast<size_t>(e) * Ng + s) * x1;
-            q2[t] += __ldg(a.e2 + static_cast<size_t>(e) * Ng + s) * x2;
+        for (int j = 0; j < LN; ++j) { q1[t][j] = T(0); q2[t][j] = T(0); }
+    long long lj[LN];
+    bool ok[LN];
+#pragma unroll
+    for (int j = 0; j < LN; ++j) {
+        lj[j] = l0 + static_cast<long long>(j) * blockDim.x;
+        ok[j] = lj[j] < per_e;
+    }
+    for (int s0 = lo; s0 < hi; s0 += SC) {
+        const int n = min(SC, hi - s0);
+        __syncthreads();
+        for (int k = threadIdx.x; k < SC * TE; k += blockDim.x) {
+            const int ss = k / TE, t = k - ss * TE, e = e0 + t;
+            const bool in = ss < n && e < Ng;
+            E1[ss][t] = in ? static_cast<T>(a.e1[static_cast<size_t>(e) * Ng + s0 + ss]) : T(0);
+            E2[ss][t] = in ? static_cast<T>(a.e2[static_cast<size_t>(e) * Ng + s0 + ss]) : T(0);
+        }
+        __syncthreads();
+#pragma unroll 2
+        for (int ss = 0; ss < n; ++ss) {
+            T x1[LN], x2[LN];
+            const long long row = static_cast<long long>(s0 + ss) * per_e;
+#pragma unroll
+            for (int j = 0; j < LN; ++j) {
+                x1[j] = ok[j] ? a.A1[row + lj[j]] : T(0);
+                x2[j] = ok[j] ? a.A2[row + lj[j]] : T(0);
+            }
+#pragma unroll
+            for (int t = 0; t < TE; ++t) {
+                const T c1 = E1[ss][t], c2 = E2[ss][t];
+#pragma unroll
+                for (int j = 0; j < LN; ++j) {
+                    q1[t][j] += c1 * x1[j];
+                    q2[t][j] += c2 * x2[j];
+                }
+            }
         }
     }
+    const T dg = static_cast<T>(a.dg), third = T(1) / T(3);
 #pragma unroll
     for (int t = 0; t < TE; ++t) {
         const int e = e0 + t;
-        if (e < Ng) a.S[e * per_e + l] = static_cast<T>(a.dg * (q1[t] + q2[t] / 3.0));
+        if (e >= Ng) continue;
+#pragma unroll
+        for (int j = 0; j < LN; ++j)
+            if (ok[j]) a.S[e * per_e + lj[j]] = dg * (q1[t][j] + q2[t][j] * third);
     }
 }
 
 template <typename T>
 cudaError_t launch_source_energy(const SourceArgs<T>& a, int tile_e, cudaStream_t s) {
+    constexpr int LN = sizeof(T) == 4 ? 2 : 1;
     const long long per_e = static_cast<long long>(a.nyz) * a.NA;
     const int tiles = (a.Ng + tile_e - 1) / tile_e;
-    dim3 grid(tiles, static_cast<unsigned>((per_e + 127) / 128));
+    const long long ly = (per_e + 128 * LN - 1) / (128 * LN);
+    if (ly > 65535) return cudaErrorInvalidConfiguration;
+    dim3 grid(tiles, static_cast<unsigned>(ly));
     switch (tile_e) {
-        case 8: source_energy_kernel<T, 8><<<grid, 128, 0, s>>>(a); break;
-        case 16: source_energy_kernel<T, 16><<<grid, 128, 0, s>>>(a); break;
+        case 8: source_energy_kernel<T, 8, LN><<<grid, 128, 0, s>>>(a); break;
+        case 16: source_energy_kernel<T, 16, LN><<<grid, 128, 0, s>>>(a); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

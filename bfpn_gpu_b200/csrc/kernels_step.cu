@@ -10,6 +10,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 
 namespace bfpn {
 
@@ -39,10 +40,17 @@ __global__ void __launch_bounds__(256) energy_kernel(EnergyArgs<T> a) {
         T* __restrict__ Fp = a.F + lane;
         T* __restrict__ fp = a.f + lane;
         const T* __restrict__ sp = a.src ? a.src + lane : nullptr;
-        int ek = a.Ng - 1;
-        double Fn = static_cast<double>(Fp[ek * L]);
-        double fn = static_cast<double>(fp[ek * L]);
-        double sn = sp ? static_cast<double>(sp[ek * L]) : 0.0;
+        const int Ng = a.Ng;
+        // ring of the next D groups' old values, loaded D groups ahead of use
+        constexpr int D = 8;
+        T rF[D], rf[D], rs[D];
+#pragma unroll
+        for (int k = 0; k < D; ++k) {
+            const int e = Ng - 1 - k;
+            rF[k] = e >= 0 ? Fp[e * L] : T(0);
+            rf[k] = e >= 0 ? fp[e * L] : T(0);
+            rs[k] = (e >= 0 && sp) ? sp[e * L] : T(0);
+        }
         double F_hi_old = 0.0, f_hi_old = 0.0;  // old values at ek+1
         double next_F = 0.0, next_f = 0.0;      // new values at ek+1
         double w_pos = 1.0;
@@ -52,13 +60,21 @@ __global__ void __launch_bounds__(256) energy_kernel(EnergyArgs<T> a) {
             if (iy == 0 || iy == a.Ny) w_pos *= 0.5;
             if (iz == 0 || iz == a.Nz) w_pos *= 0.5;
         }
-        for (; ek >= 0; --ek) {
-            const double Fg = Fn, fg = fn, sg = sn;
-            if (ek > 0) {
-                Fn = static_cast<double>(Fp[(ek - 1) * L]);
-                fn = static_cast<double>(fp[(ek - 1) * L]);
-                if (sp) sn = static_cast<double>(sp[(ek - 1) * L]);
+        for (int base = Ng - 1; base >= 0; base -= D)
+#pragma unroll
+        for (int k = 0; k < D; ++k) {
+            const int ek = base - k;
+            if (ek < 0) break;
+            const double Fg = static_cast<double>(rF[k]), fg = static_cast<double>(rf[k]),
+                         sg = static_cast<double>(rs[k]);
+            const int ep = ek - D;  // refill this slot D groups ahead
+            if (ep >= 0) {
+                rF[k] = Fp[ep * L];
+                rf[k] = fp[ep * L];
+                if (sp) rs[k] = sp[ep * L];
             }
+            // old value of group ek-1 (straggling): the next slot, or the refill of slot 0
+            const double Fn = static_cast<double>(rF[(k + 1) % D]);
             const double* __restrict__ c = a.coef + ek * kEnergyCoef;
             double Fv, fv;
             if (MODE == EMODE_LEGACY) {
@@ -150,95 +166,234 @@ cudaError_t launch_energy(const EnergyArgs<T>& a, int block, cudaStream_t s) {
 // cell (the reference does 4 launches and ~10 array passes).  Boundary
 // indices clamp exactly as the reference's (max(0,i-2) .. min(Ny,i+2)).
 // ---------------------------------------------------------------------------
+// MUSCL slope of the reference (muscl_paper_slope, spatial_transport.cu:23-29):
+// fwd * max(0, max(min(2 theta, 1), min(theta, 2))) with theta = back / fwd,
+// and 0 when |fwd| < 1e-10.  Written without the division: with
+// sg = sign(fwd) and b = sg * back, the limited slope is
+// sg * max(0, max(min(2b, |fwd|), min(b, 2|fwd|))) -- case by case equal to
+// fwd * eta (theta <= 0, <= 1/2, <= 1, <= 2, > 2).
 template <typename T>
-__device__ __forceinline__ T muscl_slope(T l, T c, T r) {
+__device__ __forceinline__ T superbee(T l, T c, T r) {
     const T fwd = r - c;
-    if (fabs(fwd) < static_cast<T>(kEpsilon)) return T(0);
-    const T theta = (c - l) / fwd;
-    const T eta = max(T(0), max(min(T(2) * theta, T(1)), min(theta, T(2))));
-    return fwd * eta;
+    const T sg = fwd >= T(0) ? T(1) : T(-1);
+    const T af = fabs(fwd), b = sg * (c - l);
+    const T m = max(T(0), max(min(T(2) * b, af), min(b, T(2) * af)));
+    return af < static_cast<T>(kEpsilon) ? T(0) : sg * m;
 }
 
-template <typename T, typename Get>
-__device__ __forceinline__ T flux_divergence(const Get& get, int gy, int gz, int Ny, int Nz, T wy, T wz, T dy,
-                                             T dz) {
-    const T c = get(gy, gz);
-    const T ym2 = get(max(0, gy - 2), gz), ym1 = get(max(0, gy - 1), gz);
-    const T yp1 = get(min(Ny, gy + 1), gz), yp2 = get(min(Ny, gy + 2), gz);
-    T lfy, rfy;
-    if (wy >= T(0)) {
-        lfy = wy * (ym1 + T(0.5) * muscl_slope(ym2, ym1, c));
-        rfy = wy * (c + T(0.5) * muscl_slope(ym1, c, yp1));
-    } else {
-        lfy = wy * (c - T(0.5) * muscl_slope(ym1, c, yp1));
-        rfy = wy * (yp1 - T(0.5) * muscl_slope(c, yp1, yp2));
+// A rectangle of positions [y0, y1) x [z0, z1) staged in shared memory with
+// AC angles per position (angle fastest).
+struct Rect {
+    int y0, y1, z0, z1;
+    __device__ int w() const { return y1 - y0; }
+    __device__ int n() const { return (y1 - y0) * (z1 - z0); }
+    __device__ int at(int gy, int gz) const { return (gz - z0) * (y1 - y0) + (gy - y0); }
+    __device__ Rect grow(int h, int Ny1, int Nz1) const {
+        return Rect{max(0, y0 - h), min(Ny1, y1 + h), max(0, z0 - h), min(Nz1, z1 + h)};
     }
-    const T zm2 = get(gy, max(0, gz - 2)), zm1 = get(gy, max(0, gz - 1));
-    const T zp1 = get(gy, min(Nz, gz + 1)), zp2 = get(gy, min(Nz, gz + 2));
-    T lfz, rfz;
-    if (wz >= T(0)) {
-        lfz = wz * (zm1 + T(0.5) * muscl_slope(zm2, zm1, c));
-        rfz = wz * (c + T(0.5) * muscl_slope(zm1, c, zp1));
-    } else {
-        lfz = wz * (c - T(0.5) * muscl_slope(zm1, c, zp1));
-        rfz = wz * (zp1 - T(0.5) * muscl_slope(c, zp1, zp2));
-    }
-    return (rfy - lfy) / dy + (rfz - lfz) / dz;
+};
+
+// position index p of a rectangle -> global (gy, gz); w < 2^12 so the float
+// quotient is exact after truncation
+__device__ __forceinline__ void rect_pos(const Rect& r, int p, float inv_w, int& gy, int& gz) {
+    const int zz = __float2int_rz((p + 0.5f) * inv_w);
+    gz = r.z0 + zz;
+    gy = r.y0 + p - zz * r.w();
 }
 
+// AC consecutive values of one position in shared memory (16-byte aligned).
+template <typename T, int AC>
+struct Vec {
+    T v[AC];
+};
+template <typename T, int AC>
+__device__ __forceinline__ void lds(const T* p, T (&v)[AC]) {
+    if (sizeof(T) * AC % 16 == 0) {
+#pragma unroll
+        for (int q = 0; q < AC; q += 16 / sizeof(T)) {
+            const float4 x = *reinterpret_cast<const float4*>(p + q);
+            memcpy(&v[q], &x, 16);
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < AC; ++q) v[q] = p[q];
+    }
+}
+template <typename T, int AC>
+__device__ __forceinline__ void sts(T* p, const T (&v)[AC]) {
+    if (sizeof(T) * AC % 16 == 0) {
+#pragma unroll
+        for (int q = 0; q < AC; q += 16 / sizeof(T)) {
+            float4 x;
+            memcpy(&x, &v[q], 16);
+            *reinterpret_cast<float4*>(p + q) = x;
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < AC; ++q) p[q] = v[q];
+    }
+}
+
+// Face values of X over `region` (X staged over rx, which holds every clamped
+// neighbour): Gy = X + 0.5 sgn(wy) s_y, Gz likewise; one thread per position,
+// all AC angles of it.
+template <typename T, int AC>
+__device__ __forceinline__ void build_faces(const T* X, const Rect& rx, T* Gy, T* Gz, const Rect& rg,
+                                            const Rect& region, int Ny, int Nz, const T (&hy)[AC], const T (&hz)[AC]) {
+    const float inv_w = 1.0f / region.w();
+    for (int p = threadIdx.x; p < region.n(); p += blockDim.x) {
+        int gy, gz;
+        rect_pos(region, p, inv_w, gy, gz);
+        T c[AC], m[AC], n[AC], fy[AC], fz[AC];
+        lds<T, AC>(X + rx.at(gy, gz) * AC, c);
+        lds<T, AC>(X + rx.at(max(0, gy - 1), gz) * AC, m);
+        lds<T, AC>(X + rx.at(min(Ny, gy + 1), gz) * AC, n);
+#pragma unroll
+        for (int q = 0; q < AC; ++q) fy[q] = c[q] + hy[q] * superbee(m[q], c[q], n[q]);
+        lds<T, AC>(X + rx.at(gy, max(0, gz - 1)) * AC, m);
+        lds<T, AC>(X + rx.at(gy, min(Nz, gz + 1)) * AC, n);
+#pragma unroll
+        for (int q = 0; q < AC; ++q) fz[q] = c[q] + hz[q] * superbee(m[q], c[q], n[q]);
+        sts<T, AC>(Gy + rg.at(gy, gz) * AC, fy);
+        sts<T, AC>(Gz + rg.at(gy, gz) * AC, fz);
+    }
+}
+
+// Upwind flux divergence of X at (gy, gz), all AC angles, from the face
+// values G = X + 0.5 sgn(omega) slope (spatial_flux_divergence_value,
+// spatial_transport.cu:31-102).  At a boundary the reference's clamped
+// stencil makes the outer face value X itself (the slope of a constant
+// triple is 0).
+template <typename T, int AC>
+__device__ __forceinline__ void face_divergence(const T* X, const Rect& rx, const T* Gy, const T* Gz, const Rect& rg,
+                                                int gy, int gz, int Ny, int Nz, const T (&wy)[AC], const T (&wz)[AC],
+                                                T rdy, T rdz, T (&div)[AC]) {
+    T c[AC], l[AC], r[AC];
+    lds<T, AC>(Gy + rg.at(gy, gz) * AC, c);
+    lds<T, AC>(gy > 0 ? Gy + rg.at(gy - 1, gz) * AC : X + rx.at(0, gz) * AC, l);
+    lds<T, AC>(gy < Ny ? Gy + rg.at(gy + 1, gz) * AC : X + rx.at(Ny, gz) * AC, r);
+#pragma unroll
+    for (int q = 0; q < AC; ++q) {
+        const bool pos = wy[q] >= T(0);
+        const T lf = wy[q] * (pos ? l[q] : c[q]);
+        const T rf = wy[q] * (pos ? c[q] : r[q]);
+        div[q] = (rf - lf) * rdy;
+    }
+    lds<T, AC>(Gz + rg.at(gy, gz) * AC, c);
+    lds<T, AC>(gz > 0 ? Gz + rg.at(gy, gz - 1) * AC : X + rx.at(gy, 0) * AC, l);
+    lds<T, AC>(gz < Nz ? Gz + rg.at(gy, gz + 1) * AC : X + rx.at(gy, Nz) * AC, r);
+#pragma unroll
+    for (int q = 0; q < AC; ++q) {
+        const bool pos = wz[q] >= T(0);
+        const T lf = wz[q] * (pos ? l[q] : c[q]);
+        const T rf = wz[q] * (pos ? c[q] : r[q]);
+        div[q] += (rf - lf) * rdz;
+    }
+}
+
+// One block = one energy group, AC consecutive angles, one tile of output
+// positions; one thread per position with all AC angles in registers.
+// Shared memory holds F over the tile plus a 4-cell halo (overwritten in
+// place by H = F - dt/2 div F on the tile once it is no longer read), the
+// face values (3-cell halo, reused for the predictor's faces) and the
+// predictor (2-cell halo).  Every slope is evaluated once per cell and
+// direction.
 template <typename T, int AC>
 __global__ void __launch_bounds__(256) transport_kernel(TransportArgs<T> a, int tiles_y, int tiles_z, int n_chunks) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* Fs = reinterpret_cast<T*>(smem_raw);
     int b = blockIdx.x;
-    const int tyi = b % tiles_y; b /= tiles_y;
-    const int tzi = b % tiles_z; b /= tiles_z;
+    const int tyi = b % tiles_y;
+    b /= tiles_y;
+    const int tzi = b % tiles_z;
+    b /= tiles_z;
     const int chunk = b % n_chunks;
     const int ek = b / n_chunks;
     const int Ny = a.Ny, Nz = a.Nz, Ny1 = a.Ny + 1, Nz1 = a.Nz + 1, NA = a.NA;
-    const int y0 = tyi * a.tile_y, y1 = min(y0 + a.tile_y, Ny1);
-    const int z0 = tzi * a.tile_z, z1 = min(z0 + a.tile_z, Nz1);
-    const int fy0 = max(0, y0 - 4), fy1 = min(Ny1, y1 + 4), fz0 = max(0, z0 - 4), fz1 = min(Nz1, z1 + 4);
-    const int py0 = max(0, y0 - 2), py1 = min(Ny1, y1 + 2), pz0 = max(0, z0 - 2), pz1 = min(Nz1, z1 + 2);
-    const int FRY = fy1 - fy0, FRZ = fz1 - fz0, PRY = py1 - py0, PRZ = pz1 - pz0;
-    T* Ps = Fs + FRY * FRZ * AC;
+    const Rect t{tyi * a.tile_y, min(tyi * a.tile_y + a.tile_y, Ny1), tzi * a.tile_z, min(tzi * a.tile_z + a.tile_z, Nz1)};
+    const Rect r1 = t.grow(1, Ny1, Nz1), r2 = t.grow(2, Ny1, Nz1), r3 = t.grow(3, Ny1, Nz1), r4 = t.grow(4, Ny1, Nz1);
+    T* Fs = reinterpret_cast<T*>(smem_raw);
+    T* Gy = Fs + r4.n() * AC;
+    T* Gz = Gy + r3.n() * AC;
+    T* Ps = Gz + r3.n() * AC;
     const int a0 = chunk * AC;
     const size_t plane = static_cast<size_t>(ek) * Ny1 * Nz1 * NA + a0;
     const T* __restrict__ in = a.in + plane;
     T* __restrict__ out = a.out + plane;
-
-    for (int e = threadIdx.x; e < FRY * FRZ * AC; e += blockDim.x) {
-        const int aa = e % AC, p = e / AC, yy = p % FRY, zz = p / FRY;
-        Fs[e] = (a0 + aa < NA) ? in[(static_cast<size_t>(fz0 + zz) * Ny1 + fy0 + yy) * NA + aa] : T(0);
+    const T dt = a.dt, rdy = T(1) / a.dy, rdz = T(1) / a.dz, hdt = T(0.5) * a.dt;
+    const bool full = a0 + AC <= NA;
+    T wy[AC], wz[AC], hy[AC], hz[AC];
+#pragma unroll
+    for (int q = 0; q < AC; ++q) {
+        const int ang = min(a0 + q, NA - 1);
+        wy[q] = a.omega[2 * ang];
+        wz[q] = a.omega[2 * ang + 1];
+        hy[q] = wy[q] >= T(0) ? T(0.5) : T(-0.5);
+        hz[q] = wz[q] >= T(0) ? T(0.5) : T(-0.5);
+    }
+    {
+        const float inv_w = 1.0f / r4.w();
+        for (int p = threadIdx.x; p < r4.n(); p += blockDim.x) {
+            int gy, gz;
+            rect_pos(r4, p, inv_w, gy, gz);
+            const T* src = in + (static_cast<size_t>(gz) * Ny1 + gy) * NA;
+            T v[AC];
+#pragma unroll
+            for (int q = 0; q < AC; ++q) v[q] = (full || a0 + q < NA) ? src[q] : T(0);
+            sts<T, AC>(Fs + p * AC, v);
+        }
     }
     __syncthreads();
-
-    const T dt = a.dt, dy = a.dy, dz = a.dz;
-    for (int e = threadIdx.x; e < PRY * PRZ * AC; e += blockDim.x) {
-        const int aa = e % AC, p = e / AC, yy = p % PRY, zz = p / PRY;
-        const int ang = min(a0 + aa, NA - 1);
-        const T wy = a.omega[2 * ang], wz = a.omega[2 * ang + 1];
-        auto getF = [&](int gy, int gz) { return Fs[((gz - fz0) * FRY + (gy - fy0)) * AC + aa]; };
-        const int gy = py0 + yy, gz = pz0 + zz;
-        const T v = getF(gy, gz) - dt * flux_divergence<T>(getF, gy, gz, Ny, Nz, wy, wz, dy, dz);
-        Ps[e] = a.preserve_sign ? v : max(v, T(0));
+    build_faces<T, AC>(Fs, r4, Gy, Gz, r3, r3, Ny, Nz, hy, hz);
+    __syncthreads();
+    {  // predictor over r2; H over the tile into F's own slots (each thread reads F only at its position)
+        const float inv_w = 1.0f / r2.w();
+        for (int p = threadIdx.x; p < r2.n(); p += blockDim.x) {
+            int gy, gz;
+            rect_pos(r2, p, inv_w, gy, gz);
+            T d[AC], f[AC], v[AC];
+            face_divergence<T, AC>(Fs, r4, Gy, Gz, r3, gy, gz, Ny, Nz, wy, wz, rdy, rdz, d);
+            T* fp = Fs + r4.at(gy, gz) * AC;
+            lds<T, AC>(fp, f);
+#pragma unroll
+            for (int q = 0; q < AC; ++q) {
+                const T x = f[q] - dt * d[q];
+                v[q] = a.preserve_sign ? x : max(x, T(0));
+            }
+            sts<T, AC>(Ps + p * AC, v);
+            if (gy >= t.y0 && gy < t.y1 && gz >= t.z0 && gz < t.z1) {
+#pragma unroll
+                for (int q = 0; q < AC; ++q) v[q] = f[q] - hdt * d[q];
+                sts<T, AC>(fp, v);
+            }
+        }
     }
     __syncthreads();
-
-    const int TY = y1 - y0, TZ = z1 - z0;
-    for (int e = threadIdx.x; e < TY * TZ * AC; e += blockDim.x) {
-        const int aa = e % AC, p = e / AC, yy = p % TY, zz = p / TY;
-        if (a0 + aa >= NA) continue;
-        const int ang = a0 + aa;
-        const T wy = a.omega[2 * ang], wz = a.omega[2 * ang + 1];
-        auto getF = [&](int gy, int gz) { return Fs[((gz - fz0) * FRY + (gy - fy0)) * AC + aa]; };
-        auto getP = [&](int gy, int gz) { return Ps[((gz - pz0) * PRY + (gy - py0)) * AC + aa]; };
-        const int gy = y0 + yy, gz = z0 + zz;
-        const T d0 = flux_divergence<T>(getF, gy, gz, Ny, Nz, wy, wz, dy, dz);
-        const T d1 = flux_divergence<T>(getP, gy, gz, Ny, Nz, wy, wz, dy, dz);
-        const T v = getF(gy, gz) - T(0.5) * dt * (d0 + d1);
-        out[(static_cast<size_t>(gz) * Ny1 + gy) * NA + aa] = a.preserve_sign ? v : max(v, T(0));
+    build_faces<T, AC>(Ps, r2, Gy, Gz, r3, r1, Ny, Nz, hy, hz);
+    __syncthreads();
+    {  // corrector over the tile
+        const float inv_w = 1.0f / t.w();
+        for (int p = threadIdx.x; p < t.n(); p += blockDim.x) {
+            int gy, gz;
+            rect_pos(t, p, inv_w, gy, gz);
+            T d[AC], h[AC];
+            face_divergence<T, AC>(Ps, r2, Gy, Gz, r3, gy, gz, Ny, Nz, wy, wz, rdy, rdz, d);
+            lds<T, AC>(Fs + r4.at(gy, gz) * AC, h);
+            T* dst = out + (static_cast<size_t>(gz) * Ny1 + gy) * NA;
+#pragma unroll
+            for (int q = 0; q < AC; ++q) {
+                const T x = h[q] - hdt * d[q];
+                if (full || a0 + q < NA) dst[q] = a.preserve_sign ? x : max(x, T(0));
+            }
+        }
     }
+}
+
+// Shared memory of one transport block for a tile of ty x tz positions.
+size_t transport_smem(int Ny1, int Nz1, int ty, int tz, int ac, size_t elem) {
+    auto n = [&](int h) {
+        return static_cast<size_t>(std::min(Ny1, ty + 2 * h)) * std::min(Nz1, tz + 2 * h);
+    };
+    return (n(4) + 2 * n(3) + n(2)) * ac * elem;
 }
 
 template <typename T, int AC>
@@ -246,15 +401,17 @@ static cudaError_t launch_transport_ac(const TransportArgs<T>& a, cudaStream_t s
     const int Ny1 = a.Ny + 1, Nz1 = a.Nz + 1;
     const int tiles_y = (Ny1 + a.tile_y - 1) / a.tile_y, tiles_z = (Nz1 + a.tile_z - 1) / a.tile_z;
     const int n_chunks = (a.NA + AC - 1) / AC;
-    const int fy = std::min(Ny1, a.tile_y + 8), fz = std::min(Nz1, a.tile_z + 8);
-    const int py = std::min(Ny1, a.tile_y + 4), pz = std::min(Nz1, a.tile_z + 4);
-    const size_t smem = static_cast<size_t>(fy * fz + py * pz) * AC * sizeof(T);
+    const size_t smem = transport_smem(Ny1, Nz1, a.tile_y, a.tile_z, AC, sizeof(T));
     auto kern = transport_kernel<T, AC>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return e;
     const long long blocks = static_cast<long long>(a.Ng) * n_chunks * tiles_y * tiles_z;
     if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
-    kern<<<static_cast<unsigned>(blocks), 256, smem, s>>>(a, tiles_y, tiles_z, n_chunks);
+    // one thread per position of the largest staged region, in whole warps, at most 256
+    const int npos = std::min(Ny1, a.tile_y + 8) * std::min(Nz1, a.tile_z + 8);
+    const int rounds = (npos + 255) / 256;
+    const int threads = std::min(256, ((npos + rounds - 1) / rounds + 31) / 32 * 32);
+    kern<<<static_cast<unsigned>(blocks), threads, smem, s>>>(a, tiles_y, tiles_z, n_chunks);
     return cudaGetLastError();
 }
 
@@ -264,7 +421,6 @@ cudaError_t launch_transport(const TransportArgs<T>& a, int ang_chunk, cudaStrea
         case 4: return launch_transport_ac<T, 4>(a, s);
         case 8: return launch_transport_ac<T, 8>(a, s);
         case 16: return launch_transport_ac<T, 16>(a, s);
-        case 32: return launch_transport_ac<T, 32>(a, s);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -236,6 +236,14 @@ int32_t bfpn_kernels_per_step(bfpn_ctx* ctx);
 /* Source groups whose angular contraction the secondary source computes. */
 int32_t bfpn_source_groups(bfpn_ctx* ctx);
 
+/* Run-time options (take effect from the next step; graphs are re-captured).
+ * BFPN_OPT_TENSOR_CORES: 1 (default) computes the source's angular
+ *   contraction on the tcgen05 tensor cores in mixed precision (split-bf16
+ *   operands, fp32 accumulation); 0 uses the fp32 CUDA-core kernel.
+ * BFPN_OPT_CUDA_GRAPHS: 1 (default) replays each depth step as a CUDA graph. */
+enum { BFPN_OPT_TENSOR_CORES = 0, BFPN_OPT_CUDA_GRAPHS = 1 };
+bfpn_status bfpn_set_option(bfpn_ctx* ctx, int32_t option, int32_t value);
+
 /* bfpn_step_async(nsteps) bracketed by CUDA events on the context stream;
  * waits and returns the device time of the steps in *elapsed_ms. */
 bfpn_status bfpn_timed_steps(bfpn_ctx* ctx, int32_t nsteps, double* elapsed_ms);

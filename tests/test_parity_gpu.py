@@ -221,3 +221,31 @@ def test_errors_are_reported_not_fatal():
     ctx.step(2)
     with pytest.raises(capi.BfpnError):
         ctx.transport(3, 0, 0.1, False)
+
+
+@pytest.mark.parametrize("shape", [dict(nmu=20, nom=20, ny=4, nz=4),   # NA 400: two output tiles of 208
+                                   dict(nmu=7, nom=7, ny=9, nz=8),     # NA 49, 90 positions: two position tiles
+                                   dict(nmu=3, nom=5, ny=2, nz=3)])    # NA 15: one padded tile
+def test_tensor_core_source_mixed(shape):
+    """tcgen05 split-bf16 angular contraction (mixed precision) against the
+    FP64 oracle and against the fp32 CUDA-core path."""
+    cfg = small_cfg(**shape)
+    mu, sig = read_tables(table_dir("synthetic500"), cfg.ng)
+    ctx = Context(cfg.grid(), cfg.phys(), capi.PREC_MIXED)
+    ctx.load_tables(mu, sig)
+    ctx.init_beam()
+    ora = O.Oracle(cfg.grid(), cfg.phys(), mu, sig)
+    F, f, F1, f1 = seeded_states(ctx, 11)
+    for k, arr in enumerate((F, f, F1, f1)):
+        # the mixed state holds floats: give the oracle the same rounded values
+        arr32 = arr.astype(np.float32).astype(np.float64)
+        ctx.set_state(k // 2, k % 2, arr32)
+        ora.set_state(k // 2, k % 2, arr32)
+    s_ref = ora.source()
+    ctx.secondary_source()
+    s_tc = ctx.source()
+    assert rel_err(s_tc, s_ref) < 2e-5
+    ctx.set_option(capi.OPT_TENSOR_CORES, 0)
+    ctx.secondary_source()
+    s_simt = ctx.source()
+    assert rel_err(s_simt, s_ref) < 2e-6
