@@ -272,9 +272,9 @@ void choose_transport(bfpn_ctx* c) {
     const size_t sz = c->elem;
     const int Ny1 = c->Ny + 1, Nz1 = c->Nz + 1;
     const size_t budget = 72 * 1024;  // three blocks per SM at least
-    // whole plane per block, the widest angle chunk (32..64 contiguous bytes) that fits
-    for (int ac : {16, 8, 4}) {
-        if (ac * sz > 64) continue;
+    // whole plane per block, the widest angle chunk (32..128 contiguous bytes) that fits
+    for (int ac : {32, 16, 8, 4}) {
+        if (ac * sz > 128) continue;
         if (ac * sz < 32 && c->NA >= 8) break;
         if (transport_smem(Ny1, Nz1, Ny1, Nz1, ac, sz) <= budget) {
             c->tr_ac = ac;

@@ -31,91 +31,105 @@ cudaError_t launch_angle_generic(const AngleArgs<T>& a, cudaStream_t s);
 // When partials != nullptr the kernel also accumulates this species' share of
 // the Eq. 24 depth dose and the psi^2 sum, and writes one pair per block.
 // ---------------------------------------------------------------------------
-template <int MODE, typename T>
-__global__ void __launch_bounds__(256) energy_kernel(EnergyArgs<T> a) {
-    const long long lane = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-    double acc = 0.0, accp = 0.0;
-    if (lane < a.lanes) {
-        const long long L = a.lanes;
-        T* __restrict__ Fp = a.F + lane;
-        T* __restrict__ fp = a.f + lane;
-        const T* __restrict__ sp = a.src ? a.src + lane : nullptr;
-        const int Ng = a.Ng;
-        // ring of the next D groups' old values, loaded D groups ahead of use
-        constexpr int D = 8;
-        T rF[D], rf[D], rs[D];
+constexpr int kEnergyLanesPerThread = 2;
+
+template <int MODE, typename T, int LPT>
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 5 : 4) energy_kernel(EnergyArgs<T> a) {
+    constexpr int D = 4;  // groups prefetched ahead of use
+    const long long L = a.lanes;
+    const int Ng = a.Ng;
+    long long lane[LPT];
+    bool ok[LPT];
 #pragma unroll
-        for (int k = 0; k < D; ++k) {
+    for (int j = 0; j < LPT; ++j) {
+        lane[j] = static_cast<long long>(blockIdx.x) * blockDim.x * LPT + threadIdx.x + j * blockDim.x;
+        ok[j] = lane[j] < L;
+    }
+    const T* __restrict__ sp = a.src;
+    // ring of the next D groups' old values for each lane
+    T rF[D][LPT], rf[D][LPT], rs[D][LPT];
+#pragma unroll
+    for (int k = 0; k < D; ++k)
+#pragma unroll
+        for (int j = 0; j < LPT; ++j) {
             const int e = Ng - 1 - k;
-            rF[k] = e >= 0 ? Fp[e * L] : T(0);
-            rf[k] = e >= 0 ? fp[e * L] : T(0);
-            rs[k] = (e >= 0 && sp) ? sp[e * L] : T(0);
+            const bool in = ok[j] && e >= 0;
+            rF[k][j] = in ? a.F[e * L + lane[j]] : T(0);
+            rf[k][j] = in ? a.f[e * L + lane[j]] : T(0);
+            rs[k][j] = (in && sp) ? sp[e * L + lane[j]] : T(0);
         }
-        double F_hi_old = 0.0, f_hi_old = 0.0;  // old values at ek+1
-        double next_F = 0.0, next_f = 0.0;      // new values at ek+1
-        double w_pos = 1.0;
-        if (a.partials && a.trapezoidal) {
-            const int pos = static_cast<int>(lane / a.NA);
-            const int iy = pos % (a.Ny + 1), iz = pos / (a.Ny + 1);
-            if (iy == 0 || iy == a.Ny) w_pos *= 0.5;
-            if (iz == 0 || iz == a.Nz) w_pos *= 0.5;
-        }
-        for (int base = Ng - 1; base >= 0; base -= D)
+    double F_hi_old[LPT], f_hi_old[LPT], next_F[LPT], next_f[LPT], w_pos[LPT], acc = 0.0, accp = 0.0;
 #pragma unroll
-        for (int k = 0; k < D; ++k) {
-            const int ek = base - k;
-            if (ek < 0) break;
-            const double Fg = static_cast<double>(rF[k]), fg = static_cast<double>(rf[k]),
-                         sg = static_cast<double>(rs[k]);
-            const int ep = ek - D;  // refill this slot D groups ahead
-            if (ep >= 0) {
-                rF[k] = Fp[ep * L];
-                rf[k] = fp[ep * L];
-                if (sp) rs[k] = sp[ep * L];
+    for (int j = 0; j < LPT; ++j) {
+        F_hi_old[j] = f_hi_old[j] = next_F[j] = next_f[j] = 0.0;
+        w_pos[j] = 1.0;
+        if (a.partials && a.trapezoidal && ok[j]) {
+            const int pos = static_cast<int>(lane[j] / a.NA);
+            const int iy = pos % (a.Ny + 1), iz = pos / (a.Ny + 1);
+            if (iy == 0 || iy == a.Ny) w_pos[j] *= 0.5;
+            if (iz == 0 || iz == a.Nz) w_pos[j] *= 0.5;
+        }
+    }
+    for (int base = Ng - 1; base >= 0; base -= D)
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        const int ek = base - k;
+        if (ek < 0) break;
+        const double* __restrict__ c = a.coef + ek * kEnergyCoef;
+        const double* __restrict__ dc = a.dose_coef + 2 * ek;
+        const int ep = ek - D;  // the group that refills this slot
+#pragma unroll
+        for (int j = 0; j < LPT; ++j) {
+            const double Fg = static_cast<double>(rF[k][j]), fg = static_cast<double>(rf[k][j]),
+                         sg = static_cast<double>(rs[k][j]);
+            if (ep >= 0 && ok[j]) {
+                rF[k][j] = a.F[ep * L + lane[j]];
+                rf[k][j] = a.f[ep * L + lane[j]];
+                if (sp) rs[k][j] = sp[ep * L + lane[j]];
             }
             // old value of group ek-1 (straggling): the next slot, or the refill of slot 0
-            const double Fn = static_cast<double>(rF[(k + 1) % D]);
-            const double* __restrict__ c = a.coef + ek * kEnergyCoef;
+            const double Fn = static_cast<double>(rF[(k + 1) % D][j]);
             double Fv, fv;
             if (MODE == EMODE_LEGACY) {
                 const double idt = __ldg(c + EC_L_IDT), hi = __ldg(c + EC_L_HI), inv = __ldg(c + EC_L_INV_DEN);
-                Fv = (fmax(Fg, 0.0) * idt + hi * next_F + sg) * inv;
-                fv = (fg * idt + hi * next_f) * inv;
+                Fv = (fmax(Fg, 0.0) * idt + hi * next_F[j] + sg) * inv;
+                fv = (fg * idt + hi * next_f[j]) * inv;
                 const double lapc = __ldg(c + EC_L_LAP);
                 if (lapc > 0.0) {
                     const double Flo = (ek > 0) ? Fn : 0.0;
-                    Fv += lapc * (fmax(F_hi_old, 0.0) - 2.0 * fmax(Fg, 0.0) + fmax(Flo, 0.0));
+                    Fv += lapc * (fmax(F_hi_old[j], 0.0) - 2.0 * fmax(Fg, 0.0) + fmax(Flo, 0.0));
                 }
                 Fv = fmax(Fv, 0.0);
                 fv = fmax(fv, 0.0);
             } else {
-                const double up = F_hi_old - f_hi_old;
+                const double up = F_hi_old[j] - f_hi_old[j];
                 const double cur = Fg - fg;
-                double common = __ldg(c + EC_C_UP) * up + __ldg(c + EC_C_CUR) * cur + __ldg(c + EC_C_F) * Fg + sg;
+                double common =
+                    __ldg(c + EC_C_UP) * up + __ldg(c + EC_C_CUR) * cur + __ldg(c + EC_C_F) * Fg + sg;
                 if (MODE == EMODE_EQ15_STRAG) {
                     const double Flo = (ek > 0) ? Fn : 0.0;
-                    common += __ldg(c + EC_S_HI) * F_hi_old + __ldg(c + EC_S_LO) * Flo - __ldg(c + EC_S_G) * Fg;
+                    common += __ldg(c + EC_S_HI) * F_hi_old[j] + __ldg(c + EC_S_LO) * Flo - __ldg(c + EC_S_G) * Fg;
                 }
-                const double hi_delta = next_F - next_f;
-                const double rhs = __ldg(c + EC_R_F) * fg + __ldg(c + EC_R_UP) * up + __ldg(c + EC_R_CUR) * cur
-                                 + __ldg(c + EC_R_FG) * Fg - __ldg(c + EC_A) * common + __ldg(c + EC_R_HI) * hi_delta;
+                const double hi_delta = next_F[j] - next_f[j];
+                const double rhs = __ldg(c + EC_R_F) * fg + __ldg(c + EC_R_UP) * up + __ldg(c + EC_R_CUR) * cur +
+                                   __ldg(c + EC_R_FG) * Fg - __ldg(c + EC_A) * common + __ldg(c + EC_R_HI) * hi_delta;
                 fv = rhs * __ldg(c + EC_INV_COE);
                 Fv = __ldg(c + EC_F_FROM_F) * fv + __ldg(c + EC_INV_F) * common + __ldg(c + EC_F_FROM_HI) * hi_delta;
             }
             const T Fs = static_cast<T>(Fv), fs = static_cast<T>(fv);
-            Fp[ek * L] = Fs;
-            fp[ek * L] = fs;
-            if (a.partials) {
-                const double* dc = a.dose_coef + 2 * ek;
-                acc += __ldg(dc) * static_cast<double>(Fs) + __ldg(dc + 1) * static_cast<double>(fs);
-                accp += static_cast<double>(fs);
+            if (ok[j]) {
+                a.F[ek * L + lane[j]] = Fs;
+                a.f[ek * L + lane[j]] = fs;
+                if (a.partials) {
+                    acc += w_pos[j] * (__ldg(dc) * static_cast<double>(Fs) + __ldg(dc + 1) * static_cast<double>(fs));
+                    accp += static_cast<double>(fs);
+                }
             }
-            F_hi_old = Fg;
-            f_hi_old = fg;
-            next_F = Fv;
-            next_f = fv;
+            F_hi_old[j] = Fg;
+            f_hi_old[j] = fg;
+            next_F[j] = Fv;
+            next_f[j] = fv;
         }
-        acc *= w_pos;
     }
     if (a.partials) {
         __shared__ double red[2][32];
@@ -124,7 +138,10 @@ __global__ void __launch_bounds__(256) energy_kernel(EnergyArgs<T> a) {
             accp += __shfl_down_sync(0xffffffffu, accp, o);
         }
         const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-        if (l == 0) { red[0][w] = acc; red[1][w] = accp; }
+        if (l == 0) {
+            red[0][w] = acc;
+            red[1][w] = accp;
+        }
         __syncthreads();
         if (w == 0) {
             const int nw = blockDim.x >> 5;
@@ -142,15 +159,19 @@ __global__ void __launch_bounds__(256) energy_kernel(EnergyArgs<T> a) {
     }
 }
 
-int energy_grid(long long lanes, int block) { return static_cast<int>((lanes + block - 1) / block); }
+int energy_grid(long long lanes, int block) {
+    const long long per_block = static_cast<long long>(block) * kEnergyLanesPerThread;
+    return static_cast<int>((lanes + per_block - 1) / per_block);
+}
 
 template <typename T>
 cudaError_t launch_energy(const EnergyArgs<T>& a, int block, cudaStream_t s) {
+    constexpr int LPT = kEnergyLanesPerThread;
     const int grid = energy_grid(a.lanes, block);
     switch (a.mode) {
-        case EMODE_EQ15: energy_kernel<EMODE_EQ15, T><<<grid, block, 0, s>>>(a); break;
-        case EMODE_EQ15_STRAG: energy_kernel<EMODE_EQ15_STRAG, T><<<grid, block, 0, s>>>(a); break;
-        default: energy_kernel<EMODE_LEGACY, T><<<grid, block, 0, s>>>(a); break;
+        case EMODE_EQ15: energy_kernel<EMODE_EQ15, T, LPT><<<grid, block, 0, s>>>(a); break;
+        case EMODE_EQ15_STRAG: energy_kernel<EMODE_EQ15_STRAG, T, LPT><<<grid, block, 0, s>>>(a); break;
+        default: energy_kernel<EMODE_LEGACY, T, LPT><<<grid, block, 0, s>>>(a); break;
     }
     return cudaGetLastError();
 }
@@ -181,125 +202,61 @@ __device__ __forceinline__ T superbee(T l, T c, T r) {
     return af < static_cast<T>(kEpsilon) ? T(0) : sg * m;
 }
 
-// A rectangle of positions [y0, y1) x [z0, z1) staged in shared memory with
-// AC angles per position (angle fastest).
+// A rectangle of positions [y0, y1) x [z0, z1) of one energy plane, staged in
+// shared memory with AC angles per position (angle fastest).
 struct Rect {
     int y0, y1, z0, z1;
     __device__ int w() const { return y1 - y0; }
+    __device__ int h() const { return z1 - z0; }
     __device__ int n() const { return (y1 - y0) * (z1 - z0); }
     __device__ int at(int gy, int gz) const { return (gz - z0) * (y1 - y0) + (gy - y0); }
-    __device__ Rect grow(int h, int Ny1, int Nz1) const {
-        return Rect{max(0, y0 - h), min(Ny1, y1 + h), max(0, z0 - h), min(Nz1, z1 + h)};
+    __device__ Rect grow(int m, int Ny1, int Nz1) const {
+        return Rect{max(0, y0 - m), min(Ny1, y1 + m), max(0, z0 - m), min(Nz1, z1 + m)};
     }
 };
 
-// position index p of a rectangle -> global (gy, gz); w < 2^12 so the float
-// quotient is exact after truncation
-__device__ __forceinline__ void rect_pos(const Rect& r, int p, float inv_w, int& gy, int& gz) {
-    const int zz = __float2int_rz((p + 0.5f) * inv_w);
-    gz = r.z0 + zz;
-    gy = r.y0 + p - zz * r.w();
-}
-
-// AC consecutive values of one position in shared memory (16-byte aligned).
-template <typename T, int AC>
-struct Vec {
-    T v[AC];
-};
-template <typename T, int AC>
-__device__ __forceinline__ void lds(const T* p, T (&v)[AC]) {
-    if (sizeof(T) * AC % 16 == 0) {
-#pragma unroll
-        for (int q = 0; q < AC; q += 16 / sizeof(T)) {
-            const float4 x = *reinterpret_cast<const float4*>(p + q);
-            memcpy(&v[q], &x, 16);
-        }
-    } else {
-#pragma unroll
-        for (int q = 0; q < AC; ++q) v[q] = p[q];
-    }
-}
-template <typename T, int AC>
-__device__ __forceinline__ void sts(T* p, const T (&v)[AC]) {
-    if (sizeof(T) * AC % 16 == 0) {
-#pragma unroll
-        for (int q = 0; q < AC; q += 16 / sizeof(T)) {
-            float4 x;
-            memcpy(&x, &v[q], 16);
-            *reinterpret_cast<float4*>(p + q) = x;
-        }
-    } else {
-#pragma unroll
-        for (int q = 0; q < AC; ++q) p[q] = v[q];
-    }
-}
-
-// Face values of X over `region` (X staged over rx, which holds every clamped
-// neighbour): Gy = X + 0.5 sgn(wy) s_y, Gz likewise; one thread per position,
-// all AC angles of it.
-template <typename T, int AC>
-__device__ __forceinline__ void build_faces(const T* X, const Rect& rx, T* Gy, T* Gz, const Rect& rg,
-                                            const Rect& region, int Ny, int Nz, const T (&hy)[AC], const T (&hz)[AC]) {
-    const float inv_w = 1.0f / region.w();
-    for (int p = threadIdx.x; p < region.n(); p += blockDim.x) {
-        int gy, gz;
-        rect_pos(region, p, inv_w, gy, gz);
-        T c[AC], m[AC], n[AC], fy[AC], fz[AC];
-        lds<T, AC>(X + rx.at(gy, gz) * AC, c);
-        lds<T, AC>(X + rx.at(max(0, gy - 1), gz) * AC, m);
-        lds<T, AC>(X + rx.at(min(Ny, gy + 1), gz) * AC, n);
-#pragma unroll
-        for (int q = 0; q < AC; ++q) fy[q] = c[q] + hy[q] * superbee(m[q], c[q], n[q]);
-        lds<T, AC>(X + rx.at(gy, max(0, gz - 1)) * AC, m);
-        lds<T, AC>(X + rx.at(gy, min(Nz, gz + 1)) * AC, n);
-#pragma unroll
-        for (int q = 0; q < AC; ++q) fz[q] = c[q] + hz[q] * superbee(m[q], c[q], n[q]);
-        sts<T, AC>(Gy + rg.at(gy, gz) * AC, fy);
-        sts<T, AC>(Gz + rg.at(gy, gz) * AC, fz);
-    }
-}
-
-// Upwind flux divergence of X at (gy, gz), all AC angles, from the face
-// values G = X + 0.5 sgn(omega) slope (spatial_flux_divergence_value,
-// spatial_transport.cu:31-102).  At a boundary the reference's clamped
-// stencil makes the outer face value X itself (the slope of a constant
-// triple is 0).
-template <typename T, int AC>
-__device__ __forceinline__ void face_divergence(const T* X, const Rect& rx, const T* Gy, const T* Gz, const Rect& rg,
-                                                int gy, int gz, int Ny, int Nz, const T (&wy)[AC], const T (&wz)[AC],
-                                                T rdy, T rdz, T (&div)[AC]) {
-    T c[AC], l[AC], r[AC];
-    lds<T, AC>(Gy + rg.at(gy, gz) * AC, c);
-    lds<T, AC>(gy > 0 ? Gy + rg.at(gy - 1, gz) * AC : X + rx.at(0, gz) * AC, l);
-    lds<T, AC>(gy < Ny ? Gy + rg.at(gy + 1, gz) * AC : X + rx.at(Ny, gz) * AC, r);
-#pragma unroll
-    for (int q = 0; q < AC; ++q) {
-        const bool pos = wy[q] >= T(0);
-        const T lf = wy[q] * (pos ? l[q] : c[q]);
-        const T rf = wy[q] * (pos ? c[q] : r[q]);
-        div[q] = (rf - lf) * rdy;
-    }
-    lds<T, AC>(Gz + rg.at(gy, gz) * AC, c);
-    lds<T, AC>(gz > 0 ? Gz + rg.at(gy, gz - 1) * AC : X + rx.at(gy, 0) * AC, l);
-    lds<T, AC>(gz < Nz ? Gz + rg.at(gy, gz + 1) * AC : X + rx.at(gy, Nz) * AC, r);
-#pragma unroll
-    for (int q = 0; q < AC; ++q) {
-        const bool pos = wz[q] >= T(0);
-        const T lf = wz[q] * (pos ? l[q] : c[q]);
-        const T rf = wz[q] * (pos ? c[q] : r[q]);
-        div[q] += (rf - lf) * rdz;
+// One-dimensional upwind MUSCL flux divergence along a line of a field X
+// (spatial_flux_divergence_value, spatial_transport.cu:31-102, one axis).
+// With h = 0.5 sgn(w) and face values G(j) = X(j) + h * s(j), where s(j) is the
+// limited slope of the clamped triple around j, the divergence at i is
+// w (G(i) - G(i-1)) for w >= 0 and w (G(i+1) - G(i)) for w < 0.  Evaluating
+// G at j = -1 or N+1 on clamped indices gives X(0) or X(N) exactly (the slope
+// of a constant triple is 0), which is the reference's boundary flux, so the
+// walk needs no special cases.  The line is walked i = i0 .. i1-1 with a
+// sliding window: one load and one slope per step.
+// ld(j) reads X at a clamped index j in [0, N]; emit(i, div) consumes div(i).
+template <typename T, typename Ld, typename Emit>
+__device__ __forceinline__ void walk_line(const Ld& ld, const Emit& emit, int i0, int i1, int N, T w, T rd) {
+    const T h = w >= T(0) ? T(0.5) : T(-0.5);
+    const bool up = w >= T(0);
+    auto X = [&](int j) { return ld(min(max(j, 0), N)); };
+    // window: x1 = X(i-1), x2 = X(i), x3 = X(i+1), x4 = X(i+2); faces g0 = G(i-1), g1 = G(i)
+    T x0 = X(i0 - 2), x1 = X(i0 - 1), x2 = X(i0), x3 = X(i0 + 1);
+    T g0 = x1 + h * superbee(x0, x1, x2);
+    T g1 = x2 + h * superbee(x1, x2, x3);
+    for (int i = i0; i < i1; ++i) {
+        const T x4 = X(i + 2);
+        const T g2 = x3 + h * superbee(x2, x3, x4);  // G(i+1)
+        const T lf = w * (up ? g0 : g1);
+        const T rf = w * (up ? g1 : g2);
+        emit(i, (rf - lf) * rd);
+        g0 = g1;
+        g1 = g2;
+        x2 = x3;
+        x3 = x4;
     }
 }
 
 // One block = one energy group, AC consecutive angles, one tile of output
-// positions; one thread per position with all AC angles in registers.
-// Shared memory holds F over the tile plus a 4-cell halo (overwritten in
-// place by H = F - dt/2 div F on the tile once it is no longer read), the
-// face values (3-cell halo, reused for the predictor's faces) and the
-// predictor (2-cell halo).  Every slope is evaluated once per cell and
-// direction.
+// positions.  Shared memory holds F over the tile plus a 4-cell halo, the
+// y-part of a divergence and the predictor (2-cell halo).  Each stage is two
+// line walks: threads (row z, angle) walk y and store the y-part; threads
+// (column y, angle) walk z, add the z-part and form the predictor (stage 1)
+// or the corrector (stage 2).  H = F - dt/2 div F is written over F in place
+// (a column's walk never reads behind itself).  Warps run along angles, so
+// every shared access is a contiguous row of AC values.
 template <typename T, int AC>
-__global__ void __launch_bounds__(256) transport_kernel(TransportArgs<T> a, int tiles_y, int tiles_z, int n_chunks) {
+__global__ void __launch_bounds__(512) transport_kernel(TransportArgs<T> a, int tiles_y, int tiles_z, int n_chunks) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     int b = blockIdx.x;
     const int tyi = b % tiles_y;
@@ -310,82 +267,60 @@ __global__ void __launch_bounds__(256) transport_kernel(TransportArgs<T> a, int 
     const int ek = b / n_chunks;
     const int Ny = a.Ny, Nz = a.Nz, Ny1 = a.Ny + 1, Nz1 = a.Nz + 1, NA = a.NA;
     const Rect t{tyi * a.tile_y, min(tyi * a.tile_y + a.tile_y, Ny1), tzi * a.tile_z, min(tzi * a.tile_z + a.tile_z, Nz1)};
-    const Rect r1 = t.grow(1, Ny1, Nz1), r2 = t.grow(2, Ny1, Nz1), r3 = t.grow(3, Ny1, Nz1), r4 = t.grow(4, Ny1, Nz1);
+    const Rect r2 = t.grow(2, Ny1, Nz1), r4 = t.grow(4, Ny1, Nz1);
     T* Fs = reinterpret_cast<T*>(smem_raw);
-    T* Gy = Fs + r4.n() * AC;
-    T* Gz = Gy + r3.n() * AC;
-    T* Ps = Gz + r3.n() * AC;
+    T* Ds = Fs + r4.n() * AC;
+    T* Ps = Ds + r2.n() * AC;
     const int a0 = chunk * AC;
     const size_t plane = static_cast<size_t>(ek) * Ny1 * Nz1 * NA + a0;
     const T* __restrict__ in = a.in + plane;
     T* __restrict__ out = a.out + plane;
-    const T dt = a.dt, rdy = T(1) / a.dy, rdz = T(1) / a.dz, hdt = T(0.5) * a.dt;
-    const bool full = a0 + AC <= NA;
-    T wy[AC], wz[AC], hy[AC], hz[AC];
-#pragma unroll
-    for (int q = 0; q < AC; ++q) {
-        const int ang = min(a0 + q, NA - 1);
-        wy[q] = a.omega[2 * ang];
-        wz[q] = a.omega[2 * ang + 1];
-        hy[q] = wy[q] >= T(0) ? T(0.5) : T(-0.5);
-        hz[q] = wz[q] >= T(0) ? T(0.5) : T(-0.5);
-    }
-    {
-        const float inv_w = 1.0f / r4.w();
-        for (int p = threadIdx.x; p < r4.n(); p += blockDim.x) {
-            int gy, gz;
-            rect_pos(r4, p, inv_w, gy, gz);
-            const T* src = in + (static_cast<size_t>(gz) * Ny1 + gy) * NA;
-            T v[AC];
-#pragma unroll
-            for (int q = 0; q < AC; ++q) v[q] = (full || a0 + q < NA) ? src[q] : T(0);
-            sts<T, AC>(Fs + p * AC, v);
-        }
+    const T dt = a.dt, hdt = T(0.5) * a.dt, rdy = T(1) / a.dy, rdz = T(1) / a.dz;
+    const int q = threadIdx.x % AC, lane0 = threadIdx.x / AC, lstep = blockDim.x / AC;
+    const bool qok = a0 + q < NA;
+    const int ang = min(a0 + q, NA - 1);
+    const T wy = a.omega[2 * ang], wz = a.omega[2 * ang + 1];
+
+    for (int e = threadIdx.x; e < r4.n() * AC; e += blockDim.x) {
+        const int aa = e % AC, p = e / AC;
+        const int gz = r4.z0 + p / r4.w(), gy = r4.y0 + p % r4.w();
+        Fs[e] = (a0 + aa < NA) ? in[(static_cast<size_t>(gz) * Ny1 + gy) * NA + aa] : T(0);
     }
     __syncthreads();
-    build_faces<T, AC>(Fs, r4, Gy, Gz, r3, r3, Ny, Nz, hy, hz);
+    // stage 1, y-part of div F over r2
+    for (int gz = r2.z0 + lane0; gz < r2.z1; gz += lstep)
+        walk_line<T>([&](int y) { return Fs[r4.at(y, gz) * AC + q]; },
+                     [&](int y, T d) { Ds[r2.at(y, gz) * AC + q] = d; }, r2.y0, r2.y1, Ny, wy, rdy);
     __syncthreads();
-    {  // predictor over r2; H over the tile into F's own slots (each thread reads F only at its position)
-        const float inv_w = 1.0f / r2.w();
-        for (int p = threadIdx.x; p < r2.n(); p += blockDim.x) {
-            int gy, gz;
-            rect_pos(r2, p, inv_w, gy, gz);
-            T d[AC], f[AC], v[AC];
-            face_divergence<T, AC>(Fs, r4, Gy, Gz, r3, gy, gz, Ny, Nz, wy, wz, rdy, rdz, d);
-            T* fp = Fs + r4.at(gy, gz) * AC;
-            lds<T, AC>(fp, f);
-#pragma unroll
-            for (int q = 0; q < AC; ++q) {
-                const T x = f[q] - dt * d[q];
-                v[q] = a.preserve_sign ? x : max(x, T(0));
-            }
-            sts<T, AC>(Ps + p * AC, v);
-            if (gy >= t.y0 && gy < t.y1 && gz >= t.z0 && gz < t.z1) {
-#pragma unroll
-                for (int q = 0; q < AC; ++q) v[q] = f[q] - hdt * d[q];
-                sts<T, AC>(fp, v);
-            }
-        }
+    // stage 1, z-part; predictor over r2, H over the tile (in place of F)
+    for (int gy = r2.y0 + lane0; gy < r2.y1; gy += lstep) {
+        const bool col_in_t = gy >= t.y0 && gy < t.y1;
+        walk_line<T>([&](int z) { return Fs[r4.at(gy, z) * AC + q]; },
+                     [&](int z, T dz) {
+                         const int ip = r2.at(gy, z) * AC + q, iF = r4.at(gy, z) * AC + q;
+                         const T d = Ds[ip] + dz;
+                         const T f = Fs[iF];
+                         const T v = f - dt * d;
+                         Ps[ip] = a.preserve_sign ? v : max(v, T(0));
+                         if (col_in_t && z >= t.z0 && z < t.z1) Fs[iF] = f - hdt * d;
+                     },
+                     r2.z0, r2.z1, Nz, wz, rdz);
     }
     __syncthreads();
-    build_faces<T, AC>(Ps, r2, Gy, Gz, r3, r1, Ny, Nz, hy, hz);
+    // stage 2, y-part of div P over the tile
+    for (int gz = t.z0 + lane0; gz < t.z1; gz += lstep)
+        walk_line<T>([&](int y) { return Ps[r2.at(y, gz) * AC + q]; },
+                     [&](int y, T d) { Ds[r2.at(y, gz) * AC + q] = d; }, t.y0, t.y1, Ny, wy, rdy);
     __syncthreads();
-    {  // corrector over the tile
-        const float inv_w = 1.0f / t.w();
-        for (int p = threadIdx.x; p < t.n(); p += blockDim.x) {
-            int gy, gz;
-            rect_pos(t, p, inv_w, gy, gz);
-            T d[AC], h[AC];
-            face_divergence<T, AC>(Ps, r2, Gy, Gz, r3, gy, gz, Ny, Nz, wy, wz, rdy, rdz, d);
-            lds<T, AC>(Fs + r4.at(gy, gz) * AC, h);
-            T* dst = out + (static_cast<size_t>(gz) * Ny1 + gy) * NA;
-#pragma unroll
-            for (int q = 0; q < AC; ++q) {
-                const T x = h[q] - hdt * d[q];
-                if (full || a0 + q < NA) dst[q] = a.preserve_sign ? x : max(x, T(0));
-            }
-        }
-    }
+    // stage 2, z-part and corrector
+    for (int gy = t.y0 + lane0; gy < t.y1; gy += lstep)
+        walk_line<T>([&](int z) { return Ps[r2.at(gy, z) * AC + q]; },
+                     [&](int z, T dz) {
+                         const T d = Ds[r2.at(gy, z) * AC + q] + dz;
+                         const T v = Fs[r4.at(gy, z) * AC + q] - hdt * d;
+                         if (qok) out[(static_cast<size_t>(z) * Ny1 + gy) * NA + q] = a.preserve_sign ? v : max(v, T(0));
+                     },
+                     t.z0, t.z1, Nz, wz, rdz);
 }
 
 // Shared memory of one transport block for a tile of ty x tz positions.
@@ -393,7 +328,7 @@ size_t transport_smem(int Ny1, int Nz1, int ty, int tz, int ac, size_t elem) {
     auto n = [&](int h) {
         return static_cast<size_t>(std::min(Ny1, ty + 2 * h)) * std::min(Nz1, tz + 2 * h);
     };
-    return (n(4) + 2 * n(3) + n(2)) * ac * elem;
+    return (n(4) + 2 * n(2)) * ac * elem;
 }
 
 template <typename T, int AC>
@@ -407,11 +342,10 @@ static cudaError_t launch_transport_ac(const TransportArgs<T>& a, cudaStream_t s
     if (e != cudaSuccess) return e;
     const long long blocks = static_cast<long long>(a.Ng) * n_chunks * tiles_y * tiles_z;
     if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
-    // one thread per position of the largest staged region, in whole warps, at most 256
-    const int npos = std::min(Ny1, a.tile_y + 8) * std::min(Nz1, a.tile_z + 8);
-    const int rounds = (npos + 255) / 256;
-    const int threads = std::min(256, ((npos + rounds - 1) / rounds + 31) / 32 * 32);
-    kern<<<static_cast<unsigned>(blocks), threads, smem, s>>>(a, tiles_y, tiles_z, n_chunks);
+    // one thread per (line, angle) of the longest stage-1 walk set, in whole warps, at most 512
+    const int lines = std::max(std::min(Ny1, a.tile_y + 4), std::min(Nz1, a.tile_z + 4));
+    const int threads = std::min(512, std::max(32, (lines * AC + 31) / 32 * 32));
+    kern<<<static_cast<unsigned>(blocks), (threads / AC) * AC, smem, s>>>(a, tiles_y, tiles_z, n_chunks);
     return cudaGetLastError();
 }
 
@@ -421,6 +355,7 @@ cudaError_t launch_transport(const TransportArgs<T>& a, int ang_chunk, cudaStrea
         case 4: return launch_transport_ac<T, 4>(a, s);
         case 8: return launch_transport_ac<T, 8>(a, s);
         case 16: return launch_transport_ac<T, 16>(a, s);
+        case 32: return launch_transport_ac<T, 32>(a, s);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -498,6 +433,14 @@ struct SineHalf {
     T h[N][(N + 1) / 2];
 };
 
+// Four copies of the half table, one per transform of a slice: separate
+// constant-bank addresses keep the compiler from holding one copy's entries in
+// registers across transforms.
+template <int N, typename T>
+struct SineQuad {
+    SineHalf<N, T> t[4];
+};
+
 template <int N, typename T>
 __device__ __forceinline__ void dst1(const SineHalf<N, T>& S, const T (&x)[N], T (&y)[N]) {
     constexpr int H = N / 2, HC = (N + 1) / 2;
@@ -523,49 +466,58 @@ __device__ __forceinline__ void dst1(const SineHalf<N, T>& S, const T (&x)[N], T
 }
 
 template <int N, typename T>
-__global__ void __launch_bounds__(256) angle_dst_kernel(AngleArgs<T> a, SineHalf<N, T> S) {
+__global__ void __launch_bounds__(256) angle_dst_kernel(AngleArgs<T> a, SineQuad<N, T> S) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int NA = N * N, RS = N + 1;  // padded row stride: conflict-free row and column access
-    T* X = reinterpret_cast<T*>(smem_raw);
     const int SL = a.slices_per_block;
+    T* X = reinterpret_cast<T*>(smem_raw);
+    T* Fac = X + SL * N * RS;  // CN factor rows of the (at most two) groups of this block's slices
     const long long total = static_cast<long long>(a.Ng) * a.nyz;
     const long long s0 = static_cast<long long>(blockIdx.x) * SL;
     const int ns = static_cast<int>(min(static_cast<long long>(SL), total - s0));
+    const long long ek0 = s0 / a.nyz;
+    const int split = static_cast<int>((ek0 + 1) * a.nyz - s0);  // first local slice of group ek0 + 1
+    const int nrows = (split < ns && ek0 + 1 < a.Ng) ? 2 : 1;
     T* __restrict__ F = a.F + s0 * NA;
     for (int e = threadIdx.x; e < ns * NA; e += blockDim.x) {
         const int s = e / NA, r = e - s * NA, v = r / N, u = r - v * N;
         X[(s * N + v) * RS + u] = F[e];
     }
+    for (int e = threadIdx.x; e < nrows * NA; e += blockDim.x) Fac[e] = a.fac[ek0 * NA + e];
     __syncthreads();
     T x[N], y[N];
-    for (int row = threadIdx.x; row < ns * N; row += blockDim.x) {  // forward u
+    // ns * N <= blockDim: every row / column has its own thread (no loop, so the
+    // table's constant-bank operands are not hoisted into registers)
+    if (const int row = threadIdx.x; row < ns * N) {  // forward u
         T* R = X + row * RS;
 #pragma unroll
         for (int k = 0; k < N; ++k) x[k] = R[k];
-        dst1<N, T>(S, x, y);
+        dst1<N, T>(S.t[0], x, y);
 #pragma unroll
         for (int k = 0; k < N; ++k) R[k] = y[k];
     }
     __syncthreads();
-    for (int col = threadIdx.x; col < ns * N; col += blockDim.x) {  // forward v, factor, inverse v
+    if (const int col = threadIdx.x; col < ns * N) {  // forward v, factor, inverse v
         const int s = col / N, mu = col - s * N;
         T* C = X + s * N * RS + mu;
 #pragma unroll
         for (int k = 0; k < N; ++k) x[k] = C[k * RS];
-        dst1<N, T>(S, x, y);
-        const T* __restrict__ fac = a.fac + ((s0 + s) / a.nyz) * NA + mu;
+        dst1<N, T>(S.t[1], x, y);
+        const T* fac = Fac + (s >= split ? NA : 0) + mu;
 #pragma unroll
         for (int k = 0; k < N; ++k) y[k] *= fac[k * N];
-        dst1<N, T>(S, y, x);
+        dst1<N, T>(S.t[2], y, x);
 #pragma unroll
         for (int k = 0; k < N; ++k) C[k * RS] = x[k];
     }
     __syncthreads();
-    for (int row = threadIdx.x; row < ns * N; row += blockDim.x) {  // inverse u
+    // ns * N <= blockDim: every row / column has its own thread (no loop, so the
+    // table's constant-bank operands are not hoisted into registers)
+    if (const int row = threadIdx.x; row < ns * N) {  // inverse u
         T* R = X + row * RS;
 #pragma unroll
         for (int k = 0; k < N; ++k) x[k] = R[k];
-        dst1<N, T>(S, x, y);
+        dst1<N, T>(S.t[3], x, y);
 #pragma unroll
         for (int k = 0; k < N; ++k) R[k] = y[k];
     }
@@ -578,14 +530,15 @@ __global__ void __launch_bounds__(256) angle_dst_kernel(AngleArgs<T> a, SineHalf
 
 template <int N, typename T>
 static cudaError_t launch_angle_dst(const AngleArgs<T>& a, cudaStream_t s) {
-    SineHalf<N, T> S;
+    SineQuad<N, T> S;
     // sine_u lives on the device; the host copy of the half table is built
     // from the same formula the tables use (angle_diffusion.cu:393-397).
     for (int m = 0; m < N; ++m)
         for (int i = 0; i < (N + 1) / 2; ++i)
-            S.h[m][i] = static_cast<T>(std::sin(3.14159265358979323846 * (m + 1) * (i + 1) / (N + 1)));
-    const int SL = std::max(1, 256 / N);
-    const size_t smem = static_cast<size_t>(SL) * N * (N + 1) * sizeof(T);
+            S.t[0].h[m][i] = static_cast<T>(std::sin(3.14159265358979323846 * (m + 1) * (i + 1) / (N + 1)));
+    S.t[1] = S.t[2] = S.t[3] = S.t[0];
+    const int SL = std::max(1, std::min(256 / N, a.nyz));  // at most two groups per block
+    const size_t smem = (static_cast<size_t>(SL) * N * (N + 1) + 2 * static_cast<size_t>(N) * N) * sizeof(T);
     auto kern = angle_dst_kernel<N, T>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return e;

@@ -161,6 +161,26 @@ __global__ void __launch_bounds__(128, 1) source_angular_umma_kernel(UmmaSourceA
     const uint8_t* __restrict__ blob =
         a.bblob + (static_cast<size_t>(gz) * a.n_ntiles + nt) * a.nk * static_cast<size_t>(2 * b_part);
 
+    // this thread's row for one stage: BK values, loaded one stage ahead of use
+    const bool vec = (a.NA % 4) == 0;
+    float xa[BK];
+    auto load_row = [&](int k0) {
+        if (vec && row_ok && k0 + BK <= a.NA) {
+#pragma unroll
+            for (int c = 0; c < BK / 4; ++c) {
+                const float4 v = __ldg(reinterpret_cast<const float4*>(src + k0) + c);
+                xa[4 * c] = v.x;
+                xa[4 * c + 1] = v.y;
+                xa[4 * c + 2] = v.z;
+                xa[4 * c + 3] = v.w;
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < BK; ++q) xa[q] = (row_ok && k0 + q < a.NA) ? __ldg(src + k0 + q) : 0.f;
+        }
+    };
+    load_row(0);
+
     bool failed = false;
     int commits[2] = {0, 0};   // MMA commits per stage (thread 0)
     int copies[2] = {0, 0};    // B copies issued per stage (thread 0)
@@ -181,20 +201,15 @@ __global__ void __launch_bounds__(128, 1) source_angular_umma_kernel(UmmaSourceA
             bulk_copy_g2s(sB, blob + static_cast<size_t>(it) * 2 * b_part, 2 * b_part, &bar_b[st]);
             ++copies[st];
         }
-        // A: this thread's row, BK k-values, split into hi / lo bf16
-        const int k0 = it * BK;
+        // A: split the prefetched row into hi / lo bf16, core-matrix layout
 #pragma unroll
         for (int c = 0; c < BK / 8; ++c) {
-            float x[8];
+            float x[8], r[8];
 #pragma unroll
             for (int q = 0; q < 8; ++q) {
-                const int k = k0 + c * 8 + q;
-                const float v = (row_ok && k < a.NA) ? src[k] : 0.f;
-                x[q] = is_p2 ? v : fmaxf(v, 0.f);
+                x[q] = is_p2 ? xa[c * 8 + q] : fmaxf(xa[c * 8 + q], 0.f);
+                r[q] = x[q] - __bfloat162float(__float2bfloat16_rn(x[q]));
             }
-            float r[8];
-#pragma unroll
-            for (int q = 0; q < 8; ++q) r[q] = x[q] - __bfloat162float(__float2bfloat16_rn(x[q]));
             uint4 hi, lo;
             hi.x = pack_bf16(x[0], x[1]);
             hi.y = pack_bf16(x[2], x[3]);
@@ -208,6 +223,7 @@ __global__ void __launch_bounds__(128, 1) source_angular_umma_kernel(UmmaSourceA
             *reinterpret_cast<uint4*>(sA + off) = hi;
             *reinterpret_cast<uint4*>(sA + a_part + off) = lo;
         }
+        if (it + 1 < a.nk) load_row((it + 1) * BK);  // in flight while this stage's MMAs run
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         bool bad = false;

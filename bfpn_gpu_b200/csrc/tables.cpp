@@ -9,7 +9,9 @@
 #include <algorithm>
 #include <cmath>
 #include <fstream>
+#include <atomic>
 #include <limits>
+#include <thread>
 
 namespace bfpn {
 namespace {
@@ -188,9 +190,9 @@ void angular_kernel(BeamTables& t) {
         jac[in] = std::pow(1.0 + iy * iy + iz * iz, -1.5);
     }
     t.ker_v.assign(static_cast<size_t>(Ng) * NA * NA, 0.0);
-    for (int ek = 0; ek < Ng - 1; ++ek) {
+    auto group = [&](int ek) {
         const double m1 = t.mu[ek * 3], m2 = t.mu[ek * 3 + 1];
-        if (m1 == 0.0 || m2 == 0.0) continue;
+        if (m1 == 0.0 || m2 == 0.0) return;
         double* K = t.ker_v.data() + static_cast<size_t>(ek) * NA * NA;
         for (int out = 0; out < NA; ++out) {
             double col = 0.0;
@@ -208,7 +210,22 @@ void angular_kernel(BeamTables& t) {
                     if (v < kKernelThreshold) v = 0.0;
                 }
         }
+    };
+    // groups are independent: split them over the host's cores (same values
+    // whatever the split)
+    const int n_threads = static_cast<int>(std::max(1u, std::min(32u, std::thread::hardware_concurrency())));
+    const long long work = static_cast<long long>(Ng) * NA * NA;
+    if (n_threads == 1 || work < (1 << 20)) {
+        for (int ek = 0; ek < Ng - 1; ++ek) group(ek);
+        return;
     }
+    std::atomic<int> next{0};
+    std::vector<std::thread> pool;
+    for (int i = 0; i < n_threads; ++i)
+        pool.emplace_back([&] {
+            for (int ek = next++; ek < Ng - 1; ek = next++) group(ek);
+        });
+    for (auto& th : pool) th.join();
 }
 
 // Initial beam factors (initializeDistribution, bfpm_solver.cu:1815-2000).
