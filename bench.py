@@ -104,16 +104,21 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def dist_setup():
+def dist_setup(backend="nccl"):
+    """Rank / world from the torchrun environment; a process group when N > 1
+    (nccl on GPUs; gloo for the CPU tests of this path)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if world > 1:
+        import datetime
+
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", init_method="env://", world_size=world, rank=rank,
-                                timeout=__import__("datetime").timedelta(seconds=300))
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, init_method="env://", world_size=world, rank=rank,
+                                timeout=datetime.timedelta(seconds=300))
     return world, rank, local
 
 
@@ -123,14 +128,20 @@ def barrier(world):
         dist.barrier()
 
 
-def max_over_ranks(x, world, local):
+def max_over_ranks(x, world, local, device=None):
+    """Max of a per-rank float over the ranks (device time of the slowest replica)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda:%d" % local)
+    t = torch.tensor([x], dtype=torch.float64, device=device if device is not None else "cuda:%d" % local)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def job_throughput(world, updates_per_step_per_rank, steps, max_ms):
+    """Whole-job updates/s: every replica's updates over the slowest replica's time."""
+    return world * updates_per_step_per_rank * steps / (max_ms / 1e3)
 
 
 def kernel_bytes(cls, cells, elem, n_groups, nyz, NA):
@@ -174,8 +185,7 @@ def run_ours(args):
     barrier(world)
     clocks = sampler.stop()
     ms = max_over_ranks(ms, world, local)
-    sec = ms / 1e3
-    value = world * updates_per_step * args.steps / sec
+    value = job_throughput(world, updates_per_step, args.steps, ms)
     kps = ctx.kernels_per_step()
 
     # per-kernel device times, eager launches bracketed by CUDA events

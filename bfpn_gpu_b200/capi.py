@@ -99,6 +99,7 @@ SIGNATURES = {
     "bfpn_source_groups": (_i32, [_vp]),
     "bfpn_setup_summary": (ctypes.c_int, [_vp, _vp]),
     "bfpn_energy_moments": (ctypes.c_int, [_vp, _dp]),
+    "bfpn_spot_plane": (ctypes.c_int, [_vp, _dp]),
     "bfpn_device_count": (_i32, []),
     "bfpn_device_info": (_i32, [_i32, ctypes.c_char_p, _i32]),
     "bfpn_stream": (_vp, [_vp]),
@@ -324,6 +325,12 @@ class Context:
 
     def source_groups(self):
         return int(lib().bfpn_source_groups(self._h))
+
+    def spot_plane(self):
+        g = self.grid
+        out = np.zeros((g.Ny + 1) * (g.Nz + 1))
+        self._check(lib().bfpn_spot_plane(self._h, _ptr(out)))
+        return out
 
     def energy_moments(self):
         out = np.zeros(2 * self.grid.Ng)

@@ -83,6 +83,7 @@ struct bfpn_ctx {
     int umma_nt = 0, umma_bk = 32, umma_ntiles = 0;
     double* scalar_out = nullptr;   // [2] one-off IDD / proxy
     double* moments = nullptr;      // [Ng][2]
+    double* plane = nullptr;        // [nyz] spot dose plane
 
     BeamTables tables;
     std::vector<double> raw_sigma;  // sigma_c as given, before the optional calibration
@@ -791,6 +792,7 @@ bfpn_status bfpn_create(const bfpn_grid* grid, const bfpn_phys* phys, int precis
     ALLOC(c->dev_err, sizeof(int));
     ALLOC(c->scalar_out, 2 * sizeof(double));
     ALLOC(c->moments, 2 * static_cast<size_t>(c->Ng) * sizeof(double));
+    ALLOC(c->plane, static_cast<size_t>(c->nyz) * sizeof(double));
 #undef ALLOC
     if (need_secondary) {
         if (cudaMemsetAsync(c->A1, 0, arr, c->stream) != cudaSuccess ||
@@ -1202,6 +1204,26 @@ bfpn_status bfpn_energy_moments(bfpn_ctx* c, double* out) {
                                                  as<float>(c->st[1][1]), c->Ng, c->per_e, w, c->moments, c->stream));
     CUDA_TRY(c, cudaMemcpyAsync(out, c->moments, 2 * static_cast<size_t>(c->Ng) * sizeof(double),
                                 cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return BFPN_OK;
+}
+
+bfpn_status bfpn_spot_plane(bfpn_ctx* c, double* plane) {
+    if (!c || !plane) return BFPN_INVALID_ARG;
+    if (!c->tables_loaded) return fail(c, BFPN_NOT_READY, "tables not loaded");
+    bfpn_status s = set_device(c);
+    if (s != BFPN_OK) return s;
+    const double dudv = c->d.du * c->d.dv;
+    if (c->prec == BFPN_PREC_FP64)
+        CUDA_TRY(c, launch_spot_plane<double>(as<double>(c->st[0][0]), as<double>(c->st[0][1]), as<double>(c->st[1][0]),
+                                              as<double>(c->st[1][1]), c->dose_coef, c->Ng, c->nyz, c->NA, dudv,
+                                              c->plane, c->stream));
+    else
+        CUDA_TRY(c, launch_spot_plane<float>(as<float>(c->st[0][0]), as<float>(c->st[0][1]), as<float>(c->st[1][0]),
+                                             as<float>(c->st[1][1]), c->dose_coef, c->Ng, c->nyz, c->NA, dudv,
+                                             c->plane, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(plane, c->plane, static_cast<size_t>(c->nyz) * sizeof(double), cudaMemcpyDeviceToHost,
+                                c->stream));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     return BFPN_OK;
 }

@@ -126,6 +126,10 @@ cudaError_t launch_energy_moments(const T* F, const T* f, const T* F1, const T* 
                                   double weight, double* out, cudaStream_t s);
 template <typename Tin, typename Tout>
 cudaError_t launch_convert(const Tin* in, Tout* out, long long n, cudaStream_t s);
+// YZ dose plane of the current state (spot diagnostics): plane[pos], nyz values.
+template <typename T>
+cudaError_t launch_spot_plane(const T* F, const T* f, const T* F1, const T* f1, const double* dose_coef, int Ng,
+                              int nyz, int NA, double dudv, double* plane, cudaStream_t s);
 
 // Tensor-core (tcgen05) angular contraction of the source, float state
 // (kernels_umma.cu).  bblob from build_umma_blob; err receives a non-zero

@@ -725,6 +725,43 @@ cudaError_t launch_energy_moments(const T* F, const T* f, const T* F1, const T* 
     return cudaGetLastError();
 }
 
+// YZ dose plane (spotDosePlaneKernel, bfpm_solver.cu:433-475): per position,
+// the Eq. 24 dose of primary + secondary summed over groups and angles,
+// times du dv.  One block per position; dose_coef holds the per-group weights
+// already divided by the density.
+template <typename T>
+__global__ void __launch_bounds__(256) spot_plane_kernel(const T* F, const T* f, const T* F1, const T* f1,
+                                                         const double* __restrict__ dc, int Ng, int nyz, int NA,
+                                                         double dudv, double* plane) {
+    const int pos = blockIdx.x;
+    const long long per_e = static_cast<long long>(nyz) * NA;
+    double acc = 0.0;
+    for (int e = threadIdx.x; e < Ng * NA; e += blockDim.x) {
+        const int ek = e / NA, a = e - ek * NA;
+        const long long i = ek * per_e + static_cast<long long>(pos) * NA + a;
+        const double p1 = static_cast<double>(F[i]) + static_cast<double>(F1[i]);
+        const double p2 = static_cast<double>(f[i]) + static_cast<double>(f1[i]);
+        acc += dc[2 * ek] * p1 + dc[2 * ek + 1] * p2;
+    }
+    __shared__ double red[32];
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) red[w] = acc;
+    __syncthreads();
+    if (w == 0) {
+        acc = (l < (int)(blockDim.x >> 5)) ? red[l] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+        if (l == 0) plane[pos] = acc * dudv;
+    }
+}
+
+template <typename T>
+cudaError_t launch_spot_plane(const T* F, const T* f, const T* F1, const T* f1, const double* dc, int Ng, int nyz,
+                              int NA, double dudv, double* plane, cudaStream_t s) {
+    spot_plane_kernel<T><<<nyz, 256, 0, s>>>(F, f, F1, f1, dc, Ng, nyz, NA, dudv, plane);
+    return cudaGetLastError();
+}
+
 // Initial beam, full mode (bfpm_solver.cu:1966-2000): F = f1(pos, ang) * f2(ek),
 // the product of the two factors evaluated on the host exactly as there.
 template <typename T>
@@ -767,7 +804,9 @@ cudaError_t launch_convert(const Tin* in, Tout* out, long long n, cudaStream_t s
                                                 int, int, double*, int, cudaStream_t);                            \
     template cudaError_t launch_energy_moments<T>(const T*, const T*, const T*, const T*, int, long long, double, \
                                                   double*, cudaStream_t);                                         \
-    template cudaError_t launch_init_beam<T>(T*, const double*, const double*, long long, int, cudaStream_t);
+    template cudaError_t launch_init_beam<T>(T*, const double*, const double*, long long, int, cudaStream_t);      \
+    template cudaError_t launch_spot_plane<T>(const T*, const T*, const T*, const T*, const double*, int, int, int, \
+                                              double, double*, cudaStream_t);
 
 BFPN_INSTANTIATE(double)
 BFPN_INSTANTIATE(float)

@@ -74,6 +74,9 @@ void printHelp(const char* prog) {
               << "  --no-cross-section-calibration Use fitted sigma_c directly (default)\n"
               << "  --legacy-cross-section-calibration Apply the legacy empirical sigma_c correction\n"
               << "  --sigma-yz <cm>  Initial transverse Gaussian sigma (default: 0.1)\n"
+              << "  --idd-stride <n> Accepted (streaming-mode option; IDD is computed every step)\n"
+              << "  --spot-depths <x,...> Save YZ dose planes near requested depths\n"
+              << "  --spot-prefix <path> Prefix for spot plane files (default: spot)\n"
               << "  --print-config   Print the parsed run as JSON and exit\n"
               << "  --test           Run in test mode\n"
               << "  --help           Show this help\n";

@@ -135,8 +135,24 @@ void BFPnSolver::solve(double tFinal) {  // bfpm_solver.cu:2166-2267
     const auto t0 = std::chrono::steady_clock::now();
     double t = 0.0;
     int step = 0;
+    std::vector<char> spot_saved(phys.spot_depths.size(), 0);
     while (step < max_steps) {
         int chunk = per_step ? 1 : std::min(100 - step % 100, max_steps - step);
+        // end a chunk at the first step after which an unsaved spot plane is due
+        // (bfpm_solver.cu:2241-2246, depth accumulated the same way)
+        if (!phys.spot_depths.empty()) {
+            double tt = t;
+            for (int k = 1; k <= chunk; ++k) {
+                tt += grid.dt;
+                bool due = false;
+                for (size_t i = 0; i < phys.spot_depths.size(); ++i)
+                    if (!spot_saved[i] && tt + 0.5 * grid.dt >= phys.spot_depths[i]) due = true;
+                if (due) {
+                    chunk = k;
+                    break;
+                }
+            }
+        }
         std::vector<double> idd(chunk), proxy(chunk);
         check(bfpn_step(ctx_, chunk, idd.data(), proxy.data()), "depth step");
         if (phys.save_energy_moments) {
@@ -151,6 +167,11 @@ void BFPnSolver::solve(double tFinal) {  // bfpm_solver.cu:2166-2267
             if (step % 100 == 0)
                 std::cout << "Step " << step << ", t = " << t << "/" << tFinal << ", IDD = " << idd[i] << std::endl;
         }
+        for (size_t i = 0; i < phys.spot_depths.size(); ++i)
+            if (!spot_saved[i] && t + 0.5 * grid.dt >= phys.spot_depths[i]) {
+                saveSpotPlane(phys.spot_depths[i], t);
+                spot_saved[i] = 1;
+            }
     }
     const double seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     saveResults(idd_history_, "idd_output.txt");
@@ -181,6 +202,29 @@ void BFPnSolver::saveResults(const std::vector<double>& values, const std::strin
     out << std::setprecision(17);
     out << "# x_cm value\n";
     for (size_t i = 0; i < values.size(); i++) out << (i + 1) * grid.dt << " " << values[i] << "\n";
+}
+
+void BFPnSolver::saveSpotPlane(double requested_depth, double actual_depth) {  // bfpm_solver.cu:3560-3612
+    if (phys.spot_prefix.empty()) return;
+    std::vector<double> plane(static_cast<size_t>(grid.Ny + 1) * (grid.Nz + 1));
+    check(bfpn_spot_plane(ctx_, plane.data()), "spot plane");
+    std::ostringstream name;
+    name << phys.spot_prefix << "_req" << std::fixed << std::setprecision(2) << requested_depth << "_x" << std::fixed
+         << std::setprecision(2) << actual_depth << ".txt";
+    std::ofstream out(name.str());
+    out << "# requested_x_cm " << requested_depth << "\n";
+    out << "# actual_x_cm " << actual_depth << "\n";
+    out << "# y_cm z_cm dose\n";
+    const int Ny1 = grid.Ny + 1, Nz1 = grid.Nz + 1;
+    for (int j = 0; j < Nz1; ++j) {
+        const double z = -0.5 * grid.Lz + j * grid.dz;
+        for (int i = 0; i < Ny1; ++i) {
+            const double y = -0.5 * grid.Ly + i * grid.dy;
+            out << y << " " << z << " " << plane[j * Ny1 + i] << "\n";
+        }
+        out << "\n";
+    }
+    std::cout << "Spot dose plane saved to " << name.str() << std::endl;
 }
 
 void BFPnSolver::saveEnergyMoments(const std::vector<double>& values, const std::string& filename) {

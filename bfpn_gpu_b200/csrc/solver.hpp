@@ -71,6 +71,7 @@ public:
 
     void saveResults(const std::vector<double>& values, const std::string& filename);
     void saveEnergyMoments(const std::vector<double>& values, const std::string& filename);
+    void saveSpotPlane(double requested_depth, double actual_depth);
 
     const std::vector<double>& iddHistory() const { return idd_history_; }
     const std::vector<double>& proxyHistory() const { return proxy_history_; }

@@ -266,6 +266,11 @@ bfpn_status bfpn_setup_summary(bfpn_ctx* ctx, bfpn_setup_info* out);
  * Eq. 25 diagnostic: out[2*g] = psi^1 integral, out[2*g+1] = psi^2 integral. */
 bfpn_status bfpn_energy_moments(bfpn_ctx* ctx, double* out);
 
+/* YZ dose plane of the current state (spotDosePlaneKernel,
+ * bfpm_solver.cu:433-475): plane[iz*(Ny+1)+iy] = du dv * sum over groups and
+ * angles of the Eq. 24 dose of primary + secondary / density.  nyz doubles. */
+bfpn_status bfpn_spot_plane(bfpn_ctx* ctx, double* plane);
+
 /* ---- devices (printGPUInfo, main.cu:25-42) ---------------------------- */
 int32_t bfpn_device_count(void);
 /* One line per device property in the reference's format; returns the number

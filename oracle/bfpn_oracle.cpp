@@ -742,6 +742,33 @@ static void energy_moments(const Model& m, double* out) {
     }
 }
 
+// spotDosePlaneKernel (bfpm_solver.cu:433-475): per (y, z) position, the Eq.
+// 24 dose of primary + secondary over groups and angles, times du dv.
+static void spot_plane(const Model& m, double* plane) {
+    const bool cat = m.p.flags & BFPN_FLAG_DOSE_CATASTROPHIC_LOSS;
+#pragma omp parallel for schedule(static)
+    for (int s = 0; s < m.nyz; ++s) {
+        double sum = 0.0;
+        for (int ek = 0; ek < m.Ng; ++ek) {
+            double S_mid = 0.5 * (m.S_s[ek] + m.S_s[ek + 1]);
+            double slope_w = (m.S_s[ek + 1] - m.S_s[ek]) / 6.0;
+            for (int a = 0; a < m.NA; ++a) {
+                size_t id = m.idx(ek, s, a);
+                double psi1 = m.st[0][0][id] + m.st[1][0][id];
+                double psi2 = m.st[0][1][id] + m.st[1][1][id];
+                double dose = psi1 * S_mid * m.dg + psi2 * slope_w * m.dg;
+                if (cat) {
+                    double sigma = std::max(m.sigma[ek], 0.0);
+                    double E_mid = 0.5 * (m.en[ek] + m.en[ek + 1]);
+                    dose += psi1 * E_mid * sigma * m.dg + psi2 * (m.en[ek + 1] - m.en[ek]) * sigma * m.dg / 6.0;
+                }
+                sum += dose / m.p.density;
+            }
+        }
+        plane[s] = sum * m.du * m.dv;
+    }
+}
+
 // stepPrimary (bfpm_solver.cu:3238-3311), stepPrimaryEnergyOnly
 // (3313-3333), stepSecondary (3335-3394), and the loop body of solve
 // (2190-2254).
@@ -869,6 +896,8 @@ void oracle_source(void* h, double* out) {
 void oracle_idd(void* h, double* idd, double* proxy) { orc::idd(*static_cast<Model*>(h), idd, proxy); }
 
 void oracle_energy_moments(void* h, double* out) { orc::energy_moments(*static_cast<Model*>(h), out); }
+
+void oracle_spot_plane(void* h, double* out) { orc::spot_plane(*static_cast<Model*>(h), out); }
 
 // Table access by the same ids as bfpn_table_download.  Returns the count
 // written, or -1 for an unknown id / too small a buffer.

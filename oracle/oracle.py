@@ -58,6 +58,7 @@ def lib():
         L.oracle_source.argtypes = [vp, dp]
         L.oracle_idd.argtypes = [vp, dp, dp]
         L.oracle_energy_moments.argtypes = [vp, dp]
+        L.oracle_spot_plane.argtypes = [vp, dp]
         L.oracle_table.restype = ctypes.c_longlong
         L.oracle_table.argtypes = [vp, ctypes.c_int, dp, ctypes.c_ulonglong]
         L.oracle_read_tables.restype = ctypes.c_int
@@ -175,6 +176,12 @@ class Oracle:
     def energy_moments(self):
         out = np.empty(2 * self.grid.Ng)
         lib().oracle_energy_moments(self._h, _dp(out))
+        return out
+
+    def spot_plane(self):
+        g = self.grid
+        out = np.empty((g.Ny + 1) * (g.Nz + 1))
+        lib().oracle_spot_plane(self._h, _dp(out))
         return out
 
     def table(self, which, n):

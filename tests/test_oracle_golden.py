@@ -32,3 +32,19 @@ def test_oracle_matches_reference_golden_full(grid):
     idd, _ = o.step(cfg.max_steps())
     gold = load_golden(grid)
     assert np.abs(idd - gold[:, 1]).max() / np.abs(gold[:, 1]).max() < 1e-11
+
+
+def test_c1_fixture_matches_current_oracle_prefix():
+    """tests/golden/idd_c1_oracle.txt (full 250-step oracle run, made by
+    tests/golden/make_c1_fixture.py) agrees with the oracle as built."""
+    import os
+    from conftest import GOLDEN, table_dir
+    from bfpn_gpu_b200 import parse_args, read_tables
+    fx = os.path.join(GOLDEN, "idd_c1_oracle.txt")
+    args = open(fx).readline().split("oracle FP64:")[1].split()
+    cfg = parse_args(args)
+    ref = np.loadtxt(fx)
+    mu, sig = read_tables(table_dir("synthetic200_lg104"), cfg.ng)
+    o = O.Oracle(cfg.grid(), cfg.phys(), mu, sig)
+    idd, proxy = o.step(3)
+    assert np.array_equal(idd, ref[:3, 1]) and np.array_equal(proxy, ref[:3, 2])

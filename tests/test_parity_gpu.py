@@ -249,3 +249,24 @@ def test_tensor_core_source_mixed(shape):
     ctx.secondary_source()
     s_simt = ctx.source()
     assert rel_err(s_simt, s_ref) < 2e-6
+
+
+def test_fp64_100mev_configuration_full_run():
+    """The 100 MeV FP64 configuration (16x16 yz, 8x8 angles, 200 groups over
+    104 MeV, 10 cm) against the oracle's full-run fixture, 1e-10 relative."""
+    import os
+    from conftest import GOLDEN
+    from bfpn_gpu_b200 import parse_args
+    fx = os.path.join(GOLDEN, "idd_c1_oracle.txt")
+    header = open(fx).readline()
+    args = header.split("oracle FP64:")[1].strip().split()
+    cfg = parse_args(args)
+    ref = np.loadtxt(fx)
+    mu, sig = read_tables(table_dir("synthetic200_lg104"), cfg.ng)
+    ctx = Context(cfg.grid(), cfg.phys(), capi.PREC_FP64)
+    ctx.load_tables(mu, sig)
+    ctx.init_beam()
+    idd, proxy = ctx.step(cfg.max_steps())
+    assert idd.shape[0] == ref.shape[0] == 250
+    assert np.abs(idd - ref[:, 1]).max() <= 1e-10 * np.abs(ref[:, 1]).max()
+    assert np.abs(proxy - ref[:, 2]).max() <= 1e-10 * np.abs(ref[:, 2]).max()
