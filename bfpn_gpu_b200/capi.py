@@ -100,6 +100,7 @@ SIGNATURES = {
     "bfpn_setup_summary": (ctypes.c_int, [_vp, _vp]),
     "bfpn_energy_moments": (ctypes.c_int, [_vp, _dp]),
     "bfpn_spot_plane": (ctypes.c_int, [_vp, _dp]),
+    "bfpn_idd_noalloc": (ctypes.c_int, [ctypes.POINTER(Grid), _i32, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _vp]),
     "bfpn_device_count": (_i32, []),
     "bfpn_device_info": (_i32, [_i32, ctypes.c_char_p, _i32]),
     "bfpn_stream": (_vp, [_vp]),
@@ -169,6 +170,20 @@ def footprint_bytes(grid, phys, precision=PREC_FP64):
     if rc != OK:
         raise BfpnError(rc, lib().bfpn_last_error(None).decode())
     return int(out.value)
+
+
+def idd_noalloc(grid, precision, trapezoidal_yz, F0, f0, F1, f1, dose_coef, out, device=0, stream=None):
+    """bfpn_idd_noalloc: IDD and psi^2 proxy of caller-owned device arrays,
+    with no device allocation by the library.
+
+    F0, f0, F1, f1, dose_coef and out are device addresses (ints; F1 and f1
+    may be None); the result lands in out[0:2] on `stream` (a raw
+    cudaStream_t address, None = legacy default stream) without a wait.
+    """
+    rc = lib().bfpn_idd_noalloc(ctypes.byref(grid), precision, 1 if trapezoidal_yz else 0, F0, f0, F1, f1,
+                                dose_coef, out, device, stream)
+    if rc != OK:
+        raise BfpnError(rc, lib().bfpn_last_error(None).decode())
 
 
 class Context:

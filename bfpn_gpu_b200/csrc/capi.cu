@@ -614,6 +614,8 @@ bfpn_status set_device(bfpn_ctx* c) {
 // ============================================================================
 // C ABI
 // ============================================================================
+void bfpn::set_context_free_error(const std::string& msg) { g_create_error = msg; }
+
 extern "C" {
 
 const char* bfpn_version(void) { return "bfpn-b200 0.1.0 (sm_100a)"; }

@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <string>
 #include <vector>
 
 namespace bfpn {
@@ -147,5 +148,9 @@ size_t transport_smem(int Ny1, int Nz1, int ty, int tz, int ac, size_t elem);
 
 int energy_grid(long long lanes, int block);
 int idd_partials_grid(long long lanes);
+
+// Message that bfpn_last_error(NULL) returns on this thread, for entry points
+// that take no context.
+void set_context_free_error(const std::string& msg);
 
 }  // namespace bfpn

@@ -271,6 +271,41 @@ bfpn_status bfpn_energy_moments(bfpn_ctx* ctx, double* out);
  * angles of the Eq. 24 dose of primary + secondary / density.  nyz doubles. */
 bfpn_status bfpn_spot_plane(bfpn_ctx* ctx, double* plane);
 
+/* ---- integrated depth dose without device allocation -------------------
+ * No counterpart in the reference: its IDD (computeIntegratedDepthDose +
+ * computeScalarDoseProxy, bfpm_solver.cu:3473-3502, 3418-3444) always runs
+ * inside a solver that owns its buffers.  This variant is for callers that may
+ * not have a library allocate device memory -- a serving process that has
+ * reserved the GPU for its own pool, or a framework whose caching allocator
+ * owns the state and must stay the only allocator -- and for callers that
+ * cannot take the device synchronisation cudaMalloc/cudaFree imply.  It
+ * allocates nothing: the caller passes the state, the dose weights and the
+ * output as device pointers, and the only working memory is a fixed 64 KiB
+ * device array inside the library.
+ *
+ * Computes out[0] = IDD (both species) and out[1] = psi^2 proxy of the primary,
+ * the two numbers bfpn_idd returns, from device arrays laid out as a context
+ * holds them: [Ng][(Ny+1)(Nz+1)][Nmu*Nom], double for BFPN_PREC_FP64, float for
+ * BFPN_PREC_MIXED.  F1/f1 (secondary) may both be NULL.  dose_coef is the
+ * device array of 2*Ng doubles (weight of psi^1, weight of psi^2 per group:
+ * (S mid + catastrophic term) dg / density and its psi^2 counterpart, as in
+ * Eq. 24).  out is a device array of 2 doubles.  grid gives the sizes and
+ * lengths; trapezoidal_yz halves the yz edge weights.  Work is enqueued on
+ * `stream` (a cudaStream_t of `device`; NULL = legacy default stream) and the
+ * call returns without waiting; the caller's current device is left as it was.
+ *
+ * Limits: (Ny+1)(Nz+1)*Nmu*Nom <= 4,194,304 lanes (the scratch holds 4096
+ * block partials of 1024 lanes each); a larger plane returns
+ * BFPN_INVALID_ARG with a message.  The first call on each device does set-up
+ * (it looks up the scratch's device address) and should come before any
+ * stream capture on that device.  All calls on one device share the scratch:
+ * calls that overlap in time on that device (two streams, two host threads)
+ * race and give wrong results -- order them on one stream.  Errors are
+ * reported through bfpn_last_error(NULL). */
+bfpn_status bfpn_idd_noalloc(const bfpn_grid* grid, int32_t precision, int32_t trapezoidal_yz,
+                             const void* F0, const void* f0, const void* F1, const void* f1,
+                             const double* dose_coef, double* out, int32_t device, void* stream);
+
 /* ---- devices (printGPUInfo, main.cu:25-42) ---------------------------- */
 int32_t bfpn_device_count(void);
 /* One line per device property in the reference's format; returns the number

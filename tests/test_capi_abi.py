@@ -117,3 +117,23 @@ def test_create_without_device_fails_cleanly():
     with pytest.raises(capi.BfpnError) as e:
         capi.Context(cfg.grid(), cfg.phys())
     assert e.value.status == capi.NO_DEVICE
+
+
+def test_idd_noalloc_checks_arguments_before_any_device_work():
+    # fake, never dereferenced addresses: every case fails validation first
+    fake = 0x1000
+    cfg = make_config(ny=4, nz=4, nmu=3, nom=3, ng=10)
+    big = make_config(ny=127, nz=127, nmu=17, nom=17, ng=10)  # 128 * 128 * 289 lanes > 4096 * 1024
+    with pytest.raises(capi.BfpnError, match="exceeds the 4194304 lanes") as e:
+        capi.idd_noalloc(big.grid(), capi.PREC_FP64, False, fake, fake, None, None, fake, fake)
+    assert e.value.status == capi.INVALID_ARG
+    with pytest.raises(capi.BfpnError, match="both secondary arrays"):
+        capi.idd_noalloc(cfg.grid(), capi.PREC_FP64, False, fake, fake, fake, None, fake, fake)
+    with pytest.raises(capi.BfpnError, match="null"):
+        capi.idd_noalloc(cfg.grid(), capi.PREC_MIXED, False, fake, fake, None, None, None, fake)
+    with pytest.raises(capi.BfpnError, match="precision"):
+        capi.idd_noalloc(cfg.grid(), 5, False, fake, fake, None, None, fake, fake)
+    if capi.lib().bfpn_device_count() == 0:
+        with pytest.raises(capi.BfpnError) as e:
+            capi.idd_noalloc(cfg.grid(), capi.PREC_FP64, False, fake, fake, None, None, fake, fake)
+        assert e.value.status == capi.NO_DEVICE
