@@ -159,6 +159,18 @@ def kernel_bytes(cls, cells, elem, n_groups, nyz, NA):
     return "hbm", 0.0
 
 
+# DRAM bytes (read + write) per cell of one launch of each kernel class, from ncu captures of
+# the same kernels on this workload with 250 groups (profiles/*_water230_ng250.txt), mixed
+# precision; traffic grows in proportion to the cells, so a full launch is this times cells.
+NCU_DRAM_BYTES_PER_CELL = {
+    "transport": (176.44e6 + 123.78e6) / 44.1e6,
+    "angle": (176.84e6 + 116.88e6) / 44.1e6,
+    "energy": (352.91e6 + 295.51e6) / 44.1e6,
+    "source_angular": (286.05e6 + 155.84e6) / 44.1e6,
+    "source_energy": (221.78e6 + 146.64e6) / 44.1e6,
+}
+
+
 def run_ours(args):
     import torch
     from bfpn_gpu_b200 import Context, capi, make_config, read_tables
@@ -215,16 +227,18 @@ def run_ours(args):
     dom = max(prof.items(), key=lambda kv: kv[1][0])[0]
     bound, work = kernel_bytes(dom, cells, elem, n_groups, nyz, NA)
     avg_s = prof[dom][0] / prof[dom][1] / 1e3
+    per_cell = NCU_DRAM_BYTES_PER_CELL.get(dom) if prec == capi.PREC_MIXED else None
+    traffic = per_cell * cells if per_cell else None  # bytes per launch
     if bound == "hbm":
         achieved = work / avg_s / 1e9
         peak = pk["hbm_gbs"]
         roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": None, "peak_source": pk_kind}
+                "frac": achieved / peak, "traffic": traffic, "peak_source": pk_kind}
     else:
         achieved = work / avg_s / 1e12
         peak = pk.get("bf16_tflops_sustained", pk["bf16_tflops"])
         roof = {"kernel": dom, "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                "frac": achieved / peak, "traffic": None, "peak_source": pk_kind}
+                "frac": achieved / peak, "traffic": traffic, "peak_source": pk_kind}
     ctx.close()
 
     out = {"metric": METRIC, "value": value, "unit": "updates/s", "n_gpus": world, "steps": args.steps,

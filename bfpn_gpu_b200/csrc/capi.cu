@@ -95,6 +95,9 @@ struct bfpn_ctx {
     // transport launch shape
     int tr_ac = 16, tr_ty = 1, tr_tz = 1;
     bool tr_inplace = true;
+    bool tr_plane_ok = false;   // a compiled whole-plane kernel exists for this plane
+    bool tr_plane = false;      // use it
+    int tr_plane_ac = 8;
     int ang_slices = 4;
     int energy_block = 128;
 
@@ -300,6 +303,19 @@ void choose_transport(bfpn_ctx* c) {
     c->tr_inplace = (c->tr_ty >= Ny1 && c->tr_tz >= Nz1);
 }
 
+// The unrolled whole-plane kernel, where one is compiled for this plane
+// size; it works in place whatever the line-walk kernel's shape.
+void choose_plane_transport(bfpn_ctx* c) {
+    // 16 float / 4 double angles per block: 64 / 32 contiguous bytes per position
+    // (16 float angles measured 7% faster than 8 on a 21x21 plane)
+    c->tr_plane_ac = c->elem == 4 ? 16 : 4;
+    c->tr_plane_ok = transport_plane_supported(c->Ny, c->Nz) &&
+                     transport_plane_smem(c->Ny + 1, c->tr_plane_ac, c->elem) <= 200 * 1024;
+    c->tr_plane = c->tr_plane_ok;
+}
+
+bool transport_in_place(const bfpn_ctx* c) { return c->tr_plane || c->tr_inplace; }
+
 template <typename T>
 bfpn_status upload_as(bfpn_ctx* c, void* dst, const double* host, size_t n) {
     if (sizeof(T) == sizeof(double)) {
@@ -361,6 +377,8 @@ cudaError_t enq_transport(bfpn_ctx* c, const void* in, void* out, double dt, boo
     a.tile_y = c->tr_ty;
     a.tile_z = c->tr_tz;
     a.preserve_sign = preserve_sign ? 1 : 0;
+    if (c->tr_plane)
+        return prof(c, BFPN_KERNEL_TRANSPORT, [&] { return launch_transport_plane<T>(a, c->tr_plane_ac, c->stream); });
     return prof(c, BFPN_KERNEL_TRANSPORT, [&] { return launch_transport<T>(a, c->tr_ac, c->stream); });
 }
 
@@ -422,7 +440,7 @@ cudaError_t enq_tat(bfpn_ctx* c, int species, int coef, bool do_tr, bool do_an, 
     const double h = 0.5 * c->d.dt;
     cudaError_t e = cudaSuccess;
     if (do_tr) {
-        void* Y = c->tr_inplace ? X : c->tmp;
+        void* Y = transport_in_place(c) ? X : c->tmp;
         e = enq_transport<T>(c, X, Y, h, preserve);
         if (e != cudaSuccess) return e;
         if (do_an) {
@@ -744,6 +762,7 @@ bfpn_status bfpn_create(const bfpn_grid* grid, const bfpn_phys* phys, int precis
         }
     }
     choose_transport(c);
+    choose_plane_transport(c);
     {
         const size_t per_slice = 2 * static_cast<size_t>(c->NA) * c->elem;
         c->ang_slices = static_cast<int>(std::max<size_t>(1, std::min<size_t>(32, (48 * 1024) / per_slice)));
@@ -993,7 +1012,7 @@ bfpn_status bfpn_transport_eq18(bfpn_ctx* c, int32_t species, int32_t coef, doub
     bfpn_status s = set_device(c);
     if (s != BFPN_OK) return s;
     void* X = c->st[species][coef];
-    void* Y = c->tr_inplace ? X : c->tmp;
+    void* Y = transport_in_place(c) ? X : c->tmp;
     if (c->prec == BFPN_PREC_FP64) CUDA_TRY(c, enq_transport<double>(c, X, Y, dt, preserve_sign != 0));
     else CUDA_TRY(c, enq_transport<float>(c, X, Y, dt, preserve_sign != 0));
     if (Y != X)
@@ -1040,6 +1059,20 @@ bfpn_status bfpn_set_option(bfpn_ctx* c, int32_t option, int32_t value) {
         case BFPN_OPT_CUDA_GRAPHS:
             c->use_graphs = value != 0 && !c->profiling;
             break;
+        case BFPN_OPT_PLANE_TRANSPORT: {
+            const bool f32 = c->elem == 4;
+            if (value != 0 && value != 1 && !(f32 ? (value == 8 || value == 16) : (value == 4 || value == 8)))
+                return fail(c, BFPN_INVALID_ARG, "plane transport: 0, 1 or an angle chunk of 8/16 (float), 4/8 (double)");
+            if (value != 0 && !c->tr_plane_ok)
+                return fail(c, BFPN_INVALID_ARG, "no whole-plane transport kernel for this plane size");
+            if (value > 1 && transport_plane_smem(c->Ny + 1, value, c->elem) > 200 * 1024)
+                return fail(c, BFPN_INVALID_ARG, "plane transport chunk needs too much shared memory");
+            if (value == 0 && !c->tr_inplace && !c->tmp)
+                return fail(c, BFPN_INVALID_ARG, "the line-walk kernel needs a buffer this context did not allocate");
+            c->tr_plane = value != 0;
+            if (value > 1) c->tr_plane_ac = value;
+            break;
+        }
         default:
             return fail(c, BFPN_INVALID_ARG, "unknown option");
     }

@@ -145,6 +145,11 @@ void build_umma_blob(const double* ker_v, const int* groups, int n_groups, int N
 
 // Dynamic shared memory of one transport block (tile ty x tz, ac angles).
 size_t transport_smem(int Ny1, int Nz1, int ty, int tz, int ac, size_t elem);
+// Whole-plane transport for square planes of the compiled sizes
+// (transport_plane_supported); ang_chunk 8 or 16 (float), 4 or 8 (double).
+template <typename T> cudaError_t launch_transport_plane(const TransportArgs<T>& a, int ang_chunk, cudaStream_t s);
+bool transport_plane_supported(int Ny, int Nz);
+size_t transport_plane_smem(int NP, int ac, size_t elem);
 
 int energy_grid(long long lanes, int block);
 int idd_partials_grid(long long lanes);

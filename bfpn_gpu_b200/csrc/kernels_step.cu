@@ -193,13 +193,31 @@ cudaError_t launch_energy(const EnergyArgs<T>& a, int block, cudaStream_t s) {
 // sg = sign(fwd) and b = sg * back, the limited slope is
 // sg * max(0, max(min(2b, |fwd|), min(b, 2|fwd|))) -- case by case equal to
 // fwd * eta (theta <= 0, <= 1/2, <= 1, <= 2, > 2).
+//
+// x with its sign flipped where s has its sign bit set: sign(s) * x for
+// s != 0, done on the bits (one logic op instead of a compare and a multiply).
+__device__ __forceinline__ float flip_by_sign(float x, float s) {
+    return __int_as_float(__float_as_int(x) ^ (__float_as_int(s) & static_cast<int>(0x80000000u)));
+}
+__device__ __forceinline__ double flip_by_sign(double x, double s) {
+    return __longlong_as_double(__double_as_longlong(x) ^
+                                (__double_as_longlong(s) & static_cast<long long>(0x8000000000000000ull)));
+}
+
+// superbee_diff(back, fwd) takes the two differences of the triple around a
+// face.  b = sg * back and the slope sg * m are the sign flips above
+// (fwd = -0 flips where sg = +1 would not, but then |fwd| < eps and the
+// slope is 0 either way).
+template <typename T>
+__device__ __forceinline__ T superbee_diff(T back, T fwd) {
+    const T af = fabs(fwd), b = flip_by_sign(back, fwd);
+    const T m = max(T(0), max(min(b + b, af), min(b, af + af)));
+    return af < static_cast<T>(kEpsilon) ? T(0) : flip_by_sign(m, fwd);
+}
+
 template <typename T>
 __device__ __forceinline__ T superbee(T l, T c, T r) {
-    const T fwd = r - c;
-    const T sg = fwd >= T(0) ? T(1) : T(-1);
-    const T af = fabs(fwd), b = sg * (c - l);
-    const T m = max(T(0), max(min(T(2) * b, af), min(b, T(2) * af)));
-    return af < static_cast<T>(kEpsilon) ? T(0) : sg * m;
+    return superbee_diff(c - l, r - c);
 }
 
 // A rectangle of positions [y0, y1) x [z0, z1) of one energy plane, staged in
@@ -361,6 +379,178 @@ cudaError_t launch_transport(const TransportArgs<T>& a, int ang_chunk, cudaStrea
 }
 
 // ---------------------------------------------------------------------------
+// Whole-plane transport for square planes of compile-time size.
+//
+// One block = one energy group and AC consecutive angles of an NP x NP plane
+// (NP = Ny+1 = Nz+1), staged whole in shared memory with rows padded to an
+// odd length (conflict-free row walks).  Every line walk is unrolled at
+// compile time, so shared-memory offsets are immediates and the clamped ends
+// fold away.  The numerics are those of walk_line: with face values
+// G(-1) = G(0) = X(0), G(N) = G(N+1) = X(N) (the slope of a clamped triple at
+// either end is 0) and D(j) = w (G(j) - G(j-1)) / h, the divergence at cell i
+// is D(i) for w >= 0 and D(i+1) for w < 0; a thread computes each D(j) once
+// and writes it to cell j - s, s = (w < 0), and the cell that receives
+// D(0) = 0 or D(N+1) = 0 is handled after the walk.  Two shared planes: F
+// (then H = F - dt/2 div F, then H - dt/2 d_y P) and the y-part of div F
+// (then the predictor P).
+// ---------------------------------------------------------------------------
+// Walks X[0], X[S], ..., X[N*S] and calls emit(j, D(j), X(j), X(j-1)) for
+// j = 1..N.
+template <typename T, int N, int S, typename Emit>
+__device__ __forceinline__ void walk_plane_line(const T* X, T wr, T h, const Emit& emit) {
+    T xp = X[0];  // X(j-1)
+    T xn = X[S];  // X(j)
+    T fwd = xn - xp;
+    T gp = xp;    // G(0)
+#pragma unroll
+    for (int j = 1; j < N; ++j) {
+        const T xnn = X[(j + 1) * S];
+        const T back = fwd;
+        fwd = xnn - xn;
+        const T g = xn + h * superbee_diff(back, fwd);
+        emit(j, wr * (g - gp), xn, xp);
+        gp = g;
+        xp = xn;
+        xn = xnn;
+    }
+    emit(N, wr * (xn - gp), xn, xp);  // G(N) = X(N)
+}
+
+template <typename T, int NP, int AC>
+__global__ void __launch_bounds__((NP * AC + 31) / 32 * 32) transport_plane_kernel(TransportArgs<T> a, int n_chunks) {
+    constexpr int N = NP - 1, RP = NP | 1, RS = RP * AC, PL = NP * RS;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* Fs = reinterpret_cast<T*>(smem_raw);
+    T* Ps = Fs + PL;
+    const int chunk = blockIdx.x % n_chunks, ek = blockIdx.x / n_chunks;
+    const int NA = a.NA, a0 = chunk * AC;
+    const size_t plane = static_cast<size_t>(ek) * NP * NP * NA + a0;
+    const T* __restrict__ in = a.in + plane;
+    T* __restrict__ out = a.out + plane;
+    const int q = threadIdx.x % AC, line = threadIdx.x / AC;
+    const bool qok = a0 + q < NA;
+    const int ang = min(a0 + q, NA - 1);
+    const T wy = a.omega[2 * ang], wz = a.omega[2 * ang + 1];
+    const T wry = wy / a.dy, wrz = wz / a.dz;
+    const bool dny = wy < T(0), dnz = wz < T(0);
+    const T hy = dny ? T(-0.5) : T(0.5), hz = dnz ? T(-0.5) : T(0.5);
+    const int sy = dny ? 1 : 0, sz = dnz ? 1 : 0;
+    const T dt = a.dt, hdt = T(0.5) * a.dt;
+    const T lo = a.preserve_sign ? -INFINITY : T(0);
+
+    for (int e = threadIdx.x; e < NP * NP * AC; e += blockDim.x) {
+        const int aa = e % AC, p = e / AC;
+        const int z = p / NP, y = p - z * NP;
+        Fs[z * RS + y * AC + aa] = (a0 + aa < NA) ? in[static_cast<size_t>(p) * NA + aa] : T(0);
+    }
+    __syncthreads();
+    const bool act = line < NP;
+    // stage 1, y-part of div F (rows z = line) into Ps
+    if (act) {
+        const T* X = Fs + line * RS + q;
+        T* D = Ps + line * RS + q - sy * AC;
+        walk_plane_line<T, N, AC>(X, wry, hy, [&](int j, T d, T, T) { D[j * AC] = d; });
+        Ps[line * RS + q + sy * N * AC] = T(0);
+    }
+    __syncthreads();
+    // stage 1, z-part (columns y = line): predictor into Ps, H over F
+    if (act) {
+        T* Xc = Fs + line * AC + q;
+        T* Pc = Ps + line * AC + q;
+        T* Xe = Xc - sz * RS;
+        T* Pe = Pc - sz * RS;
+        walk_plane_line<T, N, RS>(Xc, wrz, hz, [&](int j, T dz, T xj, T xjm1) {
+            const T f = dnz ? xjm1 : xj;
+            const T d = Pe[j * RS] + dz;
+            Pe[j * RS] = max(f - dt * d, lo);
+            Xe[j * RS] = f - hdt * d;
+        });
+        const int cb = sz * N * RS;  // the cell whose z-part is 0
+        const T f = Xc[cb], d = Pc[cb];
+        Pc[cb] = max(f - dt * d, lo);
+        Xc[cb] = f - hdt * d;
+    }
+    __syncthreads();
+    // stage 2, y-part of div P (rows): H - dt/2 d_y P over F
+    if (act) {
+        const T* X = Ps + line * RS + q;
+        T* Fe = Fs + line * RS + q - sy * AC;
+        walk_plane_line<T, N, AC>(X, wry, hy, [&](int j, T d, T, T) { Fe[j * AC] -= hdt * d; });
+    }
+    __syncthreads();
+    // stage 2, z-part (columns) and the corrector, to global
+    if (act) {
+        const T* X = Ps + line * AC + q;
+        const T* Fc = Fs + line * AC + q;
+        const T* Fe = Fc - sz * RS;
+        T* o = out + static_cast<size_t>(line) * NA + q;
+        const size_t zs = static_cast<size_t>(NP) * NA;
+        T* oe = o - sz * zs;
+        walk_plane_line<T, N, RS>(X, wrz, hz, [&](int j, T d, T, T) {
+            const T v = max(Fe[j * RS] - hdt * d, lo);
+            if (qok) oe[j * zs] = v;
+        });
+        const int cb = sz * N;
+        if (qok) o[cb * zs] = max(Fc[cb * RS], lo);
+    }
+}
+
+size_t transport_plane_smem(int NP, int ac, size_t elem) {
+    return 2 * static_cast<size_t>(NP) * (NP | 1) * ac * elem;
+}
+
+template <typename T, int NP, int AC>
+static cudaError_t launch_plane_np(const TransportArgs<T>& a, cudaStream_t s) {
+    const int n_chunks = (a.NA + AC - 1) / AC;
+    const size_t smem = transport_plane_smem(NP, AC, sizeof(T));
+    auto kern = transport_plane_kernel<T, NP, AC>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    const long long blocks = static_cast<long long>(a.Ng) * n_chunks;
+    if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+    kern<<<static_cast<unsigned>(blocks), (NP * AC + 31) / 32 * 32, smem, s>>>(a, n_chunks);
+    return cudaGetLastError();
+}
+
+// Plane sizes (Ny+1 = Nz+1) with a compiled whole-plane kernel.
+#define BFPN_PLANE_SIZES(X) X(5) X(7) X(9) X(11) X(13) X(15) X(17) X(21) X(25) X(33)
+
+bool transport_plane_supported(int Ny, int Nz) {
+    if (Ny != Nz) return false;
+    switch (Ny + 1) {
+#define BFPN_CASE(NP) case NP:
+        BFPN_PLANE_SIZES(BFPN_CASE)
+#undef BFPN_CASE
+        return true;
+        default: return false;
+    }
+}
+
+template <typename T, int AC>
+static cudaError_t launch_plane_ac(const TransportArgs<T>& a, cudaStream_t s) {
+    if (a.Ny != a.Nz) return cudaErrorNotSupported;
+    switch (a.Ny + 1) {
+#define BFPN_CASE(NP) \
+    case NP: return launch_plane_np<T, NP, AC>(a, s);
+        BFPN_PLANE_SIZES(BFPN_CASE)
+#undef BFPN_CASE
+        default: return cudaErrorNotSupported;
+    }
+}
+
+template <typename T>
+cudaError_t launch_transport_plane(const TransportArgs<T>& a, int ang_chunk, cudaStream_t s) {
+    if constexpr (sizeof(T) == 4) {
+        if (ang_chunk == 8) return launch_plane_ac<T, 8>(a, s);
+        if (ang_chunk == 16) return launch_plane_ac<T, 16>(a, s);
+    } else {
+        if (ang_chunk == 4) return launch_plane_ac<T, 4>(a, s);
+        if (ang_chunk == 8) return launch_plane_ac<T, 8>(a, s);
+    }
+    return cudaErrorInvalidValue;
+}
+
+// ---------------------------------------------------------------------------
 // Angular diffusion, Eq. (19)-(21) (angle_diffusion.cu:7-34, 254-362).
 //
 // Each (ek, pos) slice X[v][u] is NA contiguous values.  One block stages
@@ -479,10 +669,9 @@ __global__ void __launch_bounds__(256) angle_dst_kernel(AngleArgs<T> a, SineQuad
     const int split = static_cast<int>((ek0 + 1) * a.nyz - s0);  // first local slice of group ek0 + 1
     const int nrows = (split < ns && ek0 + 1 < a.Ng) ? 2 : 1;
     T* __restrict__ F = a.F + s0 * NA;
-    for (int e = threadIdx.x; e < ns * NA; e += blockDim.x) {
-        const int s = e / NA, r = e - s * NA, v = r / N, u = r - v * N;
-        X[(s * N + v) * RS + u] = F[e];
-    }
+    // the block's slices are contiguous: element e of the run goes to row e / N
+    // of the padded layout, i.e. to e + e / N
+    for (int e = threadIdx.x; e < ns * NA; e += blockDim.x) X[e + e / N] = F[e];
     for (int e = threadIdx.x; e < nrows * NA; e += blockDim.x) Fac[e] = a.fac[ek0 * NA + e];
     __syncthreads();
     T x[N], y[N];
@@ -522,10 +711,7 @@ __global__ void __launch_bounds__(256) angle_dst_kernel(AngleArgs<T> a, SineQuad
         for (int k = 0; k < N; ++k) R[k] = y[k];
     }
     __syncthreads();
-    for (int e = threadIdx.x; e < ns * NA; e += blockDim.x) {
-        const int s = e / NA, r = e - s * NA, v = r / N, u = r - v * N;
-        F[e] = X[(s * N + v) * RS + u];
-    }
+    for (int e = threadIdx.x; e < ns * NA; e += blockDim.x) F[e] = X[e + e / N];
 }
 
 template <int N, typename T>
@@ -799,6 +985,7 @@ cudaError_t launch_convert(const Tin* in, Tout* out, long long n, cudaStream_t s
 #define BFPN_INSTANTIATE(T)                                                                                       \
     template cudaError_t launch_energy<T>(const EnergyArgs<T>&, int, cudaStream_t);                               \
     template cudaError_t launch_transport<T>(const TransportArgs<T>&, int, cudaStream_t);                         \
+    template cudaError_t launch_transport_plane<T>(const TransportArgs<T>&, int, cudaStream_t);                   \
     template cudaError_t launch_angle<T>(const AngleArgs<T>&, cudaStream_t);                                      \
     template cudaError_t launch_idd_partials<T>(const T*, const T*, const double*, int, long long, int, int, int,  \
                                                 int, int, double*, int, cudaStream_t);                            \

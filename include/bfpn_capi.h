@@ -240,8 +240,13 @@ int32_t bfpn_source_groups(bfpn_ctx* ctx);
  * BFPN_OPT_TENSOR_CORES: 1 (default) computes the source's angular
  *   contraction on the tcgen05 tensor cores in mixed precision (split-bf16
  *   operands, fp32 accumulation); 0 uses the fp32 CUDA-core kernel.
- * BFPN_OPT_CUDA_GRAPHS: 1 (default) replays each depth step as a CUDA graph. */
-enum { BFPN_OPT_TENSOR_CORES = 0, BFPN_OPT_CUDA_GRAPHS = 1 };
+ * BFPN_OPT_CUDA_GRAPHS: 1 (default) replays each depth step as a CUDA graph.
+ * BFPN_OPT_PLANE_TRANSPORT: 1 (default where compiled: square planes with
+ *   Ny = Nz in {4,6,8,10,12,14,16,20,24,32}) runs the transport with the
+ *   unrolled whole-plane kernel; 0 uses the general line-walk kernel; 8 or 16
+ *   (mixed) / 4 or 8 (FP64) selects the whole-plane kernel with that many
+ *   angles per block.  Both kernels compute the same values. */
+enum { BFPN_OPT_TENSOR_CORES = 0, BFPN_OPT_CUDA_GRAPHS = 1, BFPN_OPT_PLANE_TRANSPORT = 2 };
 bfpn_status bfpn_set_option(bfpn_ctx* ctx, int32_t option, int32_t value);
 
 /* bfpn_step_async(nsteps) bracketed by CUDA events on the context stream;

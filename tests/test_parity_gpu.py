@@ -100,6 +100,41 @@ def test_transport_operator(preserve, shape):
     assert_states(ctx, ora, OP_TOL, ((0, 0), (0, 1)))
 
 
+@pytest.mark.parametrize("preserve", [False, True])
+@pytest.mark.parametrize("n,ang", [(4, (3, 3)), (8, (7, 6)), (16, (4, 5)), (32, (3, 2))])
+def test_plane_transport_operator(preserve, n, ang):
+    """The unrolled whole-plane kernel (square planes) at both angle chunks,
+    and the line-walk kernel on the same plane, against the oracle."""
+    cfg = small_cfg(ny=n, nz=n, nmu=ang[0], nom=ang[1], ng=6, lz=2.0)
+    ctx, ora = build(cfg)
+    states = seeded_states(ctx, 6)
+    for opt in (1, 8, 0):  # whole plane (4 angles per block), whole plane (8), line walks
+        ctx.set_option(capi.OPT_PLANE_TRANSPORT, opt)
+        set_both(ctx, ora, states)
+        for sp, cf in ((0, 0), (1, 1)):
+            ctx.transport(sp, cf, 0.5 * cfg.dt(), preserve)
+            ora.transport(sp, cf, 0.5 * cfg.dt(), preserve)
+        assert_states(ctx, ora, OP_TOL, ((0, 0), (1, 1)))
+
+
+def test_plane_transport_mixed_matches_line_walks():
+    cfg = small_cfg(ny=20, nz=20, nmu=6, nom=7, ng=5, lz=2.0)
+    ctx, _ = build(cfg, precision=capi.PREC_MIXED)
+    states = seeded_states(ctx, 7)
+    out = {}
+    for opt in (1, 8, 0):  # whole plane (16 angles per block), whole plane (8), line walks
+        for k, arr in enumerate(states):
+            ctx.set_state(k // 2, k % 2, arr)
+        ctx.transport(0, 0, 0.5 * cfg.dt(), False)
+        ctx.transport(0, 1, 0.5 * cfg.dt(), True)
+        out[opt] = (ctx.get_state(0, 0), ctx.get_state(0, 1))
+    for opt in (1, 8):
+        for a, b in zip(out[opt], out[0]):
+            assert rel_err(a, b) < 2e-6
+    with pytest.raises(capi.BfpnError):
+        ctx.set_option(capi.OPT_PLANE_TRANSPORT, 4)  # 4 angles per block is the FP64 chunk
+
+
 def test_angle_operator():
     cfg = small_cfg(nmu=7, nom=6)
     ctx, ora = build(cfg)
