@@ -84,6 +84,8 @@ struct bfpn_ctx {
     double* scalar_out = nullptr;   // [2] one-off IDD / proxy
     double* moments = nullptr;      // [Ng][2]
     double* plane = nullptr;        // [nyz] spot dose plane
+    bool lite = false;              // lite-memory mode: psi^1 of the primary only
+    double* lite_coef = nullptr;    // [Ng][2] lite step constants
 
     BeamTables tables;
     std::vector<double> raw_sigma;  // sigma_c as given, before the optional calibration
@@ -168,16 +170,27 @@ Layout layout_of(const bfpn_grid& g, int prec, int energy_block) {
     L.per_e = static_cast<long long>(g.Ny + 1) * (g.Nz + 1) * g.Nmu * g.Nom;
     L.cells = L.per_e * g.Ng;
     L.elem = prec == BFPN_PREC_FP64 ? sizeof(double) : sizeof(float);
-    L.part_blocks = std::max(energy_grid(L.per_e, energy_block), idd_partials_grid(L.per_e));
+    L.part_blocks = std::max({energy_grid(L.per_e, energy_block), idd_partials_grid(L.per_e),
+                              lite_energy_grid(L.per_e)});
     L.hist_cap = std::max(2 * g.Nx + 16, 4096);
     return L;
 }
 
-uint64_t footprint(const bfpn_grid& g, int prec) {
+uint64_t footprint(const bfpn_grid& g, int prec, bool lite) {
     const Layout L = layout_of(g, prec, 128);
     const uint64_t arr = static_cast<uint64_t>(L.cells) * L.elem;
     const uint64_t NA = static_cast<uint64_t>(g.Nmu) * g.Nom;
     uint64_t b = 0;
+    if (lite) {  // psi^1 of the primary and the small tables (bfpm_solver.cu:1338-1345)
+        b += arr;
+        b += 2 * static_cast<uint64_t>(g.Ng) * g.Ng * sizeof(double);  // e1, e2
+        b += 2 * static_cast<uint64_t>(g.Ng) * NA * L.elem;            // angle factors
+        b += static_cast<uint64_t>(L.per_e) * sizeof(double);          // beam factor
+        b += 4 * static_cast<uint64_t>(L.part_blocks) * sizeof(double);
+        b += 2 * static_cast<uint64_t>(L.hist_cap) * sizeof(double);
+        b += 64ull * g.Ng * sizeof(double) + (1u << 20);
+        return b;
+    }
     b += 4 * arr;   // F, f, F1, f1
     b += arr;       // transport target
     b += arr;       // source
@@ -454,8 +467,27 @@ cudaError_t enq_tat(bfpn_ctx* c, int species, int coef, bool do_tr, bool do_an, 
 }
 
 // One depth step: the loop body of BFPnSolver::solve (bfpm_solver.cu:2201-2232).
+// Lite-memory step (the lite branch of solve, bfpm_solver.cu:2191-2210):
+// stepLitePrimary and computeIntegratedDepthDoseLite, proxy 0.
+template <typename T>
+cudaError_t enq_lite_step(bfpn_ctx* c) {
+    const int trap = (c->p.flags & BFPN_FLAG_TRAPEZOIDAL_YZ) ? 1 : 0;
+    const int n = lite_energy_grid(c->per_e);
+    cudaError_t e = prof(c, BFPN_KERNEL_ENERGY, [&] {
+        return launch_lite_energy<T>(as<T>(c->st[0][0]), c->lite_coef, c->d.dt, c->Ng, c->per_e, c->dose_coef, c->NA,
+                                     c->Ny, c->Nz, trap, c->partials, c->stream);
+    });
+    if (e != cudaSuccess) return e;
+    const double w = c->d.du * c->d.dv * c->d.dy * c->d.dz;
+    return prof(c, BFPN_KERNEL_IDD, [&] {
+        return launch_finalize_idd(c->partials, n, nullptr, 0, w, c->d.dg, c->hist_idd, c->hist_proxy, c->counter,
+                                   c->hist_cap, 1, c->stream);
+    });
+}
+
 template <typename T>
 cudaError_t enq_step(bfpn_ctx* c, bool first, bool secondary_zero) {
+    if (c->lite) return enq_lite_step<T>(c);
     const unsigned fl = c->p.flags;
     const bool energy_only = fl & BFPN_FLAG_ENERGY_ONLY;
     const bool do_tr = !(fl & BFPN_FLAG_NO_TRANSPORT), do_an = !(fl & BFPN_FLAG_NO_ANGLE);
@@ -688,13 +720,12 @@ bfpn_status bfpn_host_table(const bfpn_grid* grid, const bfpn_phys* phys, const 
 }
 
 bfpn_status bfpn_footprint_bytes(const bfpn_grid* grid, const bfpn_phys* phys, int precision, uint64_t* bytes) {
-    (void)phys;
     if (!grid || !bytes) return fail(nullptr, BFPN_INVALID_ARG, "null argument");
     std::string why;
     if (!valid_grid(*grid, why)) return fail(nullptr, BFPN_INVALID_ARG, why);
     if (precision != BFPN_PREC_FP64 && precision != BFPN_PREC_MIXED)
         return fail(nullptr, BFPN_INVALID_ARG, "unknown precision");
-    *bytes = footprint(*grid, precision);
+    *bytes = footprint(*grid, precision, phys && (phys->flags & BFPN_FLAG_LITE_MEMORY));
     return BFPN_OK;
 }
 
@@ -707,8 +738,6 @@ bfpn_status bfpn_create(const bfpn_grid* grid, const bfpn_phys* phys, int precis
         return fail(nullptr, BFPN_INVALID_ARG, "unknown precision");
     if (!(phys->density > 0) || !(phys->energy_density > 0) || !(phys->sig_E > 0))
         return fail(nullptr, BFPN_INVALID_ARG, "density and sigma_E must be positive");
-    if (phys->flags & BFPN_FLAG_LITE_MEMORY)
-        return fail(nullptr, BFPN_INVALID_ARG, "lite-memory mode is not provided by this solver");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         cudaGetLastError();
@@ -750,7 +779,7 @@ bfpn_status bfpn_create(const bfpn_grid* grid, const bfpn_phys* phys, int precis
     {
         size_t free_b = 0, total_b = 0;
         if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
-            const uint64_t need = footprint(*grid, precision);
+            const uint64_t need = footprint(*grid, precision, (phys->flags & BFPN_FLAG_LITE_MEMORY) != 0);
             if (need > free_b) {
                 char msg[256];
                 std::snprintf(msg, sizeof msg,
@@ -776,10 +805,12 @@ bfpn_status bfpn_create(const bfpn_grid* grid, const bfpn_phys* phys, int precis
 #define ALLOC(dst, bytes)                                      \
     if ((s = dalloc(c, &v, (bytes))) != BFPN_OK) return bail(s); \
     dst = static_cast<std::remove_reference_t<decltype(dst)>>(v);
+    c->lite = (phys->flags & BFPN_FLAG_LITE_MEMORY) != 0;
     for (int sp = 0; sp < 2; ++sp)
-        for (int cf = 0; cf < 2; ++cf) { ALLOC(c->st[sp][cf], arr); }
-    if (!c->tr_inplace) { ALLOC(c->tmp, arr); }
-    const bool need_secondary = !(phys->flags & (BFPN_FLAG_PRIMARY_ONLY | BFPN_FLAG_ENERGY_ONLY));
+        for (int cf = 0; cf < 2; ++cf)
+            if (!c->lite || (sp == 0 && cf == 0)) { ALLOC(c->st[sp][cf], arr); }
+    if (!c->tr_inplace && !c->lite) { ALLOC(c->tmp, arr); }
+    const bool need_secondary = !c->lite && !(phys->flags & (BFPN_FLAG_PRIMARY_ONLY | BFPN_FLAG_ENERGY_ONLY));
     if (need_secondary) {
         ALLOC(c->src, arr);
         ALLOC(c->A1, arr);
@@ -814,6 +845,7 @@ bfpn_status bfpn_create(const bfpn_grid* grid, const bfpn_phys* phys, int precis
     ALLOC(c->scalar_out, 2 * sizeof(double));
     ALLOC(c->moments, 2 * static_cast<size_t>(c->Ng) * sizeof(double));
     ALLOC(c->plane, static_cast<size_t>(c->nyz) * sizeof(double));
+    ALLOC(c->lite_coef, 2 * static_cast<size_t>(c->Ng) * sizeof(double));
 #undef ALLOC
     if (need_secondary) {
         if (cudaMemsetAsync(c->A1, 0, arr, c->stream) != cudaSuccess ||
@@ -862,6 +894,8 @@ bfpn_status bfpn_load_tables(bfpn_ctx* c, const double* mu, int32_t mu_rows, con
     if ((s = upload_f64(c, c->ecoef_half, ecoef.data(), ecoef.size() * sizeof(double))) != BFPN_OK) return s;
     const auto dose = dose_coefficients(T, c->p);
     if ((s = upload_f64(c, c->dose_coef, dose.data(), dose.size() * sizeof(double))) != BFPN_OK) return s;
+    const auto lite = lite_coefficients(T, c->d.dt);
+    if ((s = upload_f64(c, c->lite_coef, lite.data(), lite.size() * sizeof(double))) != BFPN_OK) return s;
     if ((s = upload_state_table(c, c->omega, T.omega)) != BFPN_OK) return s;
     if ((s = upload_state_table(c, c->fac_step, angle_factor(T, c->p, c->d.dt))) != BFPN_OK) return s;
     if ((s = upload_state_table(c, c->sine_u, T.sine_u)) != BFPN_OK) return s;
@@ -927,9 +961,8 @@ bfpn_status bfpn_init_beam(bfpn_ctx* c) {
     } else {
         CUDA_TRY(c, launch_init_beam<float>(as<float>(c->st[0][0]), c->beam_yza, c->beam_e, c->per_e, c->Ng, c->stream));
     }
-    CUDA_TRY(c, cudaMemsetAsync(c->st[0][1], 0, arr, c->stream));
-    CUDA_TRY(c, cudaMemsetAsync(c->st[1][0], 0, arr, c->stream));
-    CUDA_TRY(c, cudaMemsetAsync(c->st[1][1], 0, arr, c->stream));
+    for (void* X : {c->st[0][1], c->st[1][0], c->st[1][1]})
+        if (X) CUDA_TRY(c, cudaMemsetAsync(X, 0, arr, c->stream));
     CUDA_TRY(c, cudaMemsetAsync(c->counter, 0, sizeof(int), c->stream));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     c->beam_ready = true;
@@ -989,6 +1022,7 @@ bfpn_status bfpn_energy_eq15(bfpn_ctx* c, int32_t species, double dt, int32_t wi
     if (!c) return BFPN_INVALID_ARG;
     if (!c->tables_loaded) return fail(c, BFPN_NOT_READY, "tables not loaded");
     if (species < 0 || species > 1 || !(dt > 0)) return fail(c, BFPN_INVALID_ARG, "bad species or dt");
+    if (c->lite) return fail(c, BFPN_INVALID_ARG, "not available in lite-memory mode (psi^1 of the primary only)");
     if (with_source && (species != 1 || !c->A1))
         return fail(c, BFPN_INVALID_ARG, "the source applies to the secondary species of a context that has one");
     bfpn_status s = set_device(c);
@@ -1009,6 +1043,7 @@ bfpn_status bfpn_transport_eq18(bfpn_ctx* c, int32_t species, int32_t coef, doub
     if (!c->tables_loaded) return fail(c, BFPN_NOT_READY, "tables not loaded");
     if (species < 0 || species > 1 || coef < 0 || coef > 1 || !(dt > 0))
         return fail(c, BFPN_INVALID_ARG, "bad species, coef or dt");
+    if (c->lite) return fail(c, BFPN_INVALID_ARG, "not available in lite-memory mode (psi^1 of the primary only)");
     bfpn_status s = set_device(c);
     if (s != BFPN_OK) return s;
     void* X = c->st[species][coef];
@@ -1026,6 +1061,7 @@ bfpn_status bfpn_angle_eq19(bfpn_ctx* c, int32_t species, int32_t coef, double d
     if (!c->tables_loaded) return fail(c, BFPN_NOT_READY, "tables not loaded");
     if (species < 0 || species > 1 || coef < 0 || coef > 1 || !(dt > 0))
         return fail(c, BFPN_INVALID_ARG, "bad species, coef or dt");
+    if (c->lite) return fail(c, BFPN_INVALID_ARG, "not available in lite-memory mode (psi^1 of the primary only)");
     bfpn_status s = set_device(c);
     if (s != BFPN_OK) return s;
     if (dt != c->fac_op_dt) {
@@ -1090,6 +1126,24 @@ bfpn_status bfpn_idd(bfpn_ctx* c, double* idd, double* proxy) {
     bfpn_status s = set_device(c);
     if (s != BFPN_OK) return s;
     const int n = idd_partials_grid(c->per_e);
+    if (c->lite) {  // computeIntegratedDepthDoseLite (bfpm_solver.cu:3528-3558): psi^1 only, proxy 0
+        const int trap = (c->p.flags & BFPN_FLAG_TRAPEZOIDAL_YZ) ? 1 : 0;
+        if (c->prec == BFPN_PREC_FP64)
+            CUDA_TRY(c, launch_idd_partials<double>(as<double>(c->st[0][0]), nullptr, c->dose_coef, c->Ng, c->per_e,
+                                                    c->NA, c->Ny, c->Nz, trap, 0, c->partials, n, c->stream));
+        else
+            CUDA_TRY(c, launch_idd_partials<float>(as<float>(c->st[0][0]), nullptr, c->dose_coef, c->Ng, c->per_e,
+                                                   c->NA, c->Ny, c->Nz, trap, 0, c->partials, n, c->stream));
+        const double w = c->d.du * c->d.dv * c->d.dy * c->d.dz;
+        CUDA_TRY(c, launch_finalize_idd(c->partials, n, nullptr, 0, w, c->d.dg, c->scalar_out, c->scalar_out + 1,
+                                        c->zero_counter, 1, 0, c->stream));
+        double h[2] = {0, 0};
+        CUDA_TRY(c, cudaMemcpyAsync(h, c->scalar_out, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+        if (idd) *idd = h[0];
+        if (proxy) *proxy = h[1];
+        return BFPN_OK;
+    }
     const int trap = (c->p.flags & BFPN_FLAG_TRAPEZOIDAL_YZ) ? 1 : 0;
     double* pP = c->partials;
     double* pS = c->partials + 2 * c->n_part;
@@ -1118,6 +1172,8 @@ bfpn_status bfpn_idd(bfpn_ctx* c, double* idd, double* proxy) {
 bfpn_status bfpn_state_upload(bfpn_ctx* c, int32_t species, int32_t coef, const double* host) {
     if (!c || !host) return BFPN_INVALID_ARG;
     if (species < 0 || species > 1 || coef < 0 || coef > 1) return fail(c, BFPN_INVALID_ARG, "bad species or coef");
+    if (!c->st[species][coef])
+        return fail(c, BFPN_INVALID_ARG, "lite-memory mode holds only psi^1 of the primary (species 0, coef 0)");
     bfpn_status s = set_device(c);
     if (s != BFPN_OK) return s;
     s = c->prec == BFPN_PREC_FP64 ? upload_as<double>(c, c->st[species][coef], host, c->cells)
@@ -1132,6 +1188,8 @@ bfpn_status bfpn_state_upload(bfpn_ctx* c, int32_t species, int32_t coef, const 
 bfpn_status bfpn_state_download(bfpn_ctx* c, int32_t species, int32_t coef, double* host) {
     if (!c || !host) return BFPN_INVALID_ARG;
     if (species < 0 || species > 1 || coef < 0 || coef > 1) return fail(c, BFPN_INVALID_ARG, "bad species or coef");
+    if (!c->st[species][coef])
+        return fail(c, BFPN_INVALID_ARG, "lite-memory mode holds only psi^1 of the primary (species 0, coef 0)");
     bfpn_status s = set_device(c);
     if (s != BFPN_OK) return s;
     return c->prec == BFPN_PREC_FP64 ? download_as<double>(c, c->st[species][coef], host, c->cells)
@@ -1228,6 +1286,7 @@ bfpn_status bfpn_setup_summary(bfpn_ctx* c, bfpn_setup_info* out) {
 
 bfpn_status bfpn_energy_moments(bfpn_ctx* c, double* out) {
     if (!c || !out) return BFPN_INVALID_ARG;
+    if (c->lite) return fail(c, BFPN_INVALID_ARG, "not available in lite-memory mode (psi^1 of the primary only)");
     bfpn_status s = set_device(c);
     if (s != BFPN_OK) return s;
     const double w = c->d.du * c->d.dv * c->d.dy * c->d.dz;
@@ -1245,6 +1304,7 @@ bfpn_status bfpn_energy_moments(bfpn_ctx* c, double* out) {
 
 bfpn_status bfpn_spot_plane(bfpn_ctx* c, double* plane) {
     if (!c || !plane) return BFPN_INVALID_ARG;
+    if (c->lite) return fail(c, BFPN_INVALID_ARG, "not available in lite-memory mode (psi^1 of the primary only)");
     if (!c->tables_loaded) return fail(c, BFPN_NOT_READY, "tables not loaded");
     bfpn_status s = set_device(c);
     if (s != BFPN_OK) return s;

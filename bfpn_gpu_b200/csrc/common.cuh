@@ -100,6 +100,12 @@ struct SourceArgs {
 
 // Launchers (kernels_*.cu).  All return the launch status.
 template <typename T> cudaError_t launch_energy(const EnergyArgs<T>& a, int block, cudaStream_t s);
+// Lite-memory primary step over psi^1 with fused IDD partials (psi^2 column 0);
+// lc = [Ng][2] (S_hi/dg, max(denom, eps)); lite_energy_grid(lanes) partial pairs.
+template <typename T>
+cudaError_t launch_lite_energy(T* F, const double* lc, double dt, int Ng, long long lanes, const double* dc, int NA,
+                               int Ny, int Nz, int trap, double* partials, cudaStream_t s);
+int lite_energy_grid(long long lanes);
 template <typename T> cudaError_t launch_transport(const TransportArgs<T>& a, int ang_chunk, cudaStream_t s);
 template <typename T> cudaError_t launch_angle(const AngleArgs<T>& a, cudaStream_t s);
 template <typename T> cudaError_t launch_source_angular(const SourceArgs<T>& a, cudaStream_t s);

@@ -177,6 +177,74 @@ cudaError_t launch_energy(const EnergyArgs<T>& a, int block, cudaStream_t s) {
 }
 
 // ---------------------------------------------------------------------------
+// Lite-memory primary step (litePrimaryEnergyStepKernel, bfpm_solver.cu:593-620):
+// psi^1 only, first-order upwind in energy with catastrophic attenuation,
+// groups swept from Ng-1 down, in place:
+//   F_g <- max((max(F_g,0)/dt + S_hi/dg * F_{g+1}) / max(denom, eps), 0)
+// with the per-group S_hi/dg and max(denom, eps) precomputed in double in the
+// reference's operation order.  The IDD of the new state (Eq. 24 with psi^2 = 0,
+// integratedDepthDoseLiteKernel, bfpm_solver.cu:523-591) is accumulated on the
+// way as per-block partials; the psi^2 column is 0.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(128) lite_energy_kernel(T* __restrict__ F, const double* __restrict__ lc, double dt,
+                                                          int Ng, long long lanes, const double* __restrict__ dc,
+                                                          int NA, int Ny, int Nz, int trap, double* partials) {
+    constexpr int D = 8;  // groups prefetched ahead of use
+    const long long lane = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const bool ok = lane < lanes;
+    T ring[D];
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        const int e = Ng - 1 - k;
+        ring[k] = (ok && e >= 0) ? F[e * lanes + lane] : T(0);
+    }
+    double w = 1.0;
+    if (trap && ok) {
+        const int pos = static_cast<int>(lane / NA), iy = pos % (Ny + 1), iz = pos / (Ny + 1);
+        if (iy == 0 || iy == Ny) w *= 0.5;
+        if (iz == 0 || iz == Nz) w *= 0.5;
+    }
+    double next = 0.0, acc = 0.0;
+    for (int base = Ng - 1; base >= 0; base -= D)
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        const int ek = base - k;
+        if (ek < 0) break;
+        const double Fg = fmax(static_cast<double>(ring[k]), 0.0);
+        const int ep = ek - D;
+        if (ep >= 0 && ok) ring[k] = F[ep * lanes + lane];
+        const double v = fmax((Fg / dt + __ldg(lc + 2 * ek) * next) / __ldg(lc + 2 * ek + 1), 0.0);
+        const T vs = static_cast<T>(v);
+        if (ok) {
+            F[ek * lanes + lane] = vs;
+            acc += w * __ldg(dc + 2 * ek) * static_cast<double>(vs);
+        }
+        next = static_cast<double>(vs);
+    }
+    __shared__ double red[4];
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    const int wi = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) red[wi] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0;
+        for (int i = 0; i < static_cast<int>(blockDim.x >> 5); ++i) a += red[i];
+        partials[2 * blockIdx.x] = a;
+        partials[2 * blockIdx.x + 1] = 0.0;
+    }
+}
+
+int lite_energy_grid(long long lanes) { return static_cast<int>((lanes + 127) / 128); }
+
+template <typename T>
+cudaError_t launch_lite_energy(T* F, const double* lc, double dt, int Ng, long long lanes, const double* dc, int NA,
+                               int Ny, int Nz, int trap, double* partials, cudaStream_t s) {
+    lite_energy_kernel<T><<<lite_energy_grid(lanes), 128, 0, s>>>(F, lc, dt, Ng, lanes, dc, NA, Ny, Nz, trap, partials);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
 // Lateral transport, Eq. (18) (spatial_transport.cu:23-161, 202-262).
 //
 // One block = one energy group, AC consecutive angles, one tile of output
@@ -616,23 +684,26 @@ __global__ void __launch_bounds__(256) angle_kernel(AngleArgs<T> a) {
 // (or column) of a slice in registers.  The DST-I matrix is symmetric and
 // S[m][N-1-i] = (-1)^m S[m][i], so y = S x needs only the first ceil(N/2)
 // columns applied to x[i] +- x[N-1-i]: N*ceil(N/2) FMAs per row instead of N^2.
-// The half table travels by value as a kernel parameter, so its entries are
-// constant-bank operands of the FMAs (no shared-memory traffic for it).
+// Every entry sin(pi (m+1)(i+1) / (N+1)) is +- sin(pi k / (N+1)) for one
+// k in 1..(N+1)/2, so the whole table is (N+1)/2 values held in registers;
+// which value and which sign each FMA takes is fixed at compile time.
 template <int N, typename T>
-struct SineHalf {
-    T h[N][(N + 1) / 2];
+struct SineTable {
+    T c[(N + 1) / 2];  // c[k-1] = sin(pi k / (N+1))
 };
 
-// Four copies of the half table, one per transform of a slice: separate
-// constant-bank addresses keep the compiler from holding one copy's entries in
-// registers across transforms.
-template <int N, typename T>
-struct SineQuad {
-    SineHalf<N, T> t[4];
-};
+// Entry (m, i) of the DST-I matrix as (k, sign): the argument (m+1)(i+1) is
+// reduced modulo 2(N+1); sin is 0 at 0 and N+1, negative on (N+1, 2(N+1)),
+// and sin(pi b/(N+1)) = sin(pi (N+1-b)/(N+1)).
+__host__ __device__ constexpr int sine_arg(int N, int m, int i) { return ((m + 1) * (i + 1)) % (2 * (N + 1)); }
+__host__ __device__ constexpr int sine_k(int N, int m, int i) {
+    const int a = sine_arg(N, m, i), b = a > N + 1 ? a - (N + 1) : a;
+    return b < N + 1 - b ? b : N + 1 - b;
+}
+__host__ __device__ constexpr bool sine_neg(int N, int m, int i) { return sine_arg(N, m, i) > N + 1; }
 
 template <int N, typename T>
-__device__ __forceinline__ void dst1(const SineHalf<N, T>& S, const T (&x)[N], T (&y)[N]) {
+__device__ __forceinline__ void dst1(const T (&c)[(N + 1) / 2], const T (&x)[N], T (&y)[N]) {
     constexpr int H = N / 2, HC = (N + 1) / 2;
     T p[HC], q[H > 0 ? H : 1];
 #pragma unroll
@@ -644,19 +715,20 @@ __device__ __forceinline__ void dst1(const SineHalf<N, T>& S, const T (&x)[N], T
 #pragma unroll
     for (int m = 0; m < N; ++m) {
         T acc = T(0);
-        if ((m & 1) == 0) {
+        const int n_terms = (m & 1) ? H : HC;
 #pragma unroll
-            for (int i = 0; i < HC; ++i) acc += S.h[m][i] * p[i];
-        } else {
-#pragma unroll
-            for (int i = 0; i < H; ++i) acc += S.h[m][i] * q[i];
+        for (int i = 0; i < n_terms; ++i) {
+            const int k = sine_k(N, m, i);
+            if (k == 0) continue;  // sin(pi) = 0: (m+1)(i+1) a multiple of N+1
+            const T v = (m & 1) ? q[i] : p[i];
+            acc = sine_neg(N, m, i) ? fma(-c[k - 1], v, acc) : fma(c[k - 1], v, acc);
         }
         y[m] = acc;
     }
 }
 
 template <int N, typename T>
-__global__ void __launch_bounds__(256) angle_dst_kernel(AngleArgs<T> a, SineQuad<N, T> S) {
+__global__ void __launch_bounds__(256) angle_dst_kernel(AngleArgs<T> a, SineTable<N, T> S) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int NA = N * N, RS = N + 1;  // padded row stride: conflict-free row and column access
     const int SL = a.slices_per_block;
@@ -673,40 +745,40 @@ __global__ void __launch_bounds__(256) angle_dst_kernel(AngleArgs<T> a, SineQuad
     // of the padded layout, i.e. to e + e / N
     for (int e = threadIdx.x; e < ns * NA; e += blockDim.x) X[e + e / N] = F[e];
     for (int e = threadIdx.x; e < nrows * NA; e += blockDim.x) Fac[e] = a.fac[ek0 * NA + e];
+    T c[(N + 1) / 2];
+#pragma unroll
+    for (int k = 0; k < (N + 1) / 2; ++k) c[k] = S.c[k];
     __syncthreads();
     T x[N], y[N];
-    // ns * N <= blockDim: every row / column has its own thread (no loop, so the
-    // table's constant-bank operands are not hoisted into registers)
-    if (const int row = threadIdx.x; row < ns * N) {  // forward u
-        T* R = X + row * RS;
+    const int line = threadIdx.x;  // ns * N <= blockDim: one row / column per thread
+    if (line < ns * N) {  // forward u
+        T* R = X + line * RS;
 #pragma unroll
         for (int k = 0; k < N; ++k) x[k] = R[k];
-        dst1<N, T>(S.t[0], x, y);
+        dst1<N, T>(c, x, y);
 #pragma unroll
         for (int k = 0; k < N; ++k) R[k] = y[k];
     }
     __syncthreads();
-    if (const int col = threadIdx.x; col < ns * N) {  // forward v, factor, inverse v
-        const int s = col / N, mu = col - s * N;
+    if (line < ns * N) {  // forward v, factor, inverse v
+        const int s = line / N, mu = line - s * N;
         T* C = X + s * N * RS + mu;
 #pragma unroll
         for (int k = 0; k < N; ++k) x[k] = C[k * RS];
-        dst1<N, T>(S.t[1], x, y);
+        dst1<N, T>(c, x, y);
         const T* fac = Fac + (s >= split ? NA : 0) + mu;
 #pragma unroll
         for (int k = 0; k < N; ++k) y[k] *= fac[k * N];
-        dst1<N, T>(S.t[2], y, x);
+        dst1<N, T>(c, y, x);
 #pragma unroll
         for (int k = 0; k < N; ++k) C[k * RS] = x[k];
     }
     __syncthreads();
-    // ns * N <= blockDim: every row / column has its own thread (no loop, so the
-    // table's constant-bank operands are not hoisted into registers)
-    if (const int row = threadIdx.x; row < ns * N) {  // inverse u
-        T* R = X + row * RS;
+    if (line < ns * N) {  // inverse u
+        T* R = X + line * RS;
 #pragma unroll
         for (int k = 0; k < N; ++k) x[k] = R[k];
-        dst1<N, T>(S.t[3], x, y);
+        dst1<N, T>(c, x, y);
 #pragma unroll
         for (int k = 0; k < N; ++k) R[k] = y[k];
     }
@@ -716,13 +788,11 @@ __global__ void __launch_bounds__(256) angle_dst_kernel(AngleArgs<T> a, SineQuad
 
 template <int N, typename T>
 static cudaError_t launch_angle_dst(const AngleArgs<T>& a, cudaStream_t s) {
-    SineQuad<N, T> S;
-    // sine_u lives on the device; the host copy of the half table is built
-    // from the same formula the tables use (angle_diffusion.cu:393-397).
-    for (int m = 0; m < N; ++m)
-        for (int i = 0; i < (N + 1) / 2; ++i)
-            S.t[0].h[m][i] = static_cast<T>(std::sin(3.14159265358979323846 * (m + 1) * (i + 1) / (N + 1)));
-    S.t[1] = S.t[2] = S.t[3] = S.t[0];
+    SineTable<N, T> S;
+    // sine_u lives on the device; the distinct values are built from the same
+    // formula the tables use (angle_diffusion.cu:393-397)
+    for (int k = 1; k <= (N + 1) / 2; ++k)
+        S.c[k - 1] = static_cast<T>(std::sin(3.14159265358979323846 * k / (N + 1)));
     const int SL = std::max(1, std::min(256 / N, a.nyz));  // at most two groups per block
     const size_t smem = (static_cast<size_t>(SL) * N * (N + 1) + 2 * static_cast<size_t>(N) * N) * sizeof(T);
     auto kern = angle_dst_kernel<N, T>;
@@ -791,7 +861,7 @@ __global__ void __launch_bounds__(256) idd_partials_kernel(const T* __restrict__
         double part = 0.0;
         for (int ek = 0; ek < Ng; ++ek) {
             const double x = static_cast<double>(F[ek * lanes + lane]);
-            const double y = static_cast<double>(f[ek * lanes + lane]);
+            const double y = f ? static_cast<double>(f[ek * lanes + lane]) : 0.0;  // f = nullptr: psi^1 only
             part += dc[2 * ek] * x + dc[2 * ek + 1] * y;
             accp += y;
         }
@@ -984,6 +1054,8 @@ cudaError_t launch_convert(const Tin* in, Tout* out, long long n, cudaStream_t s
 
 #define BFPN_INSTANTIATE(T)                                                                                       \
     template cudaError_t launch_energy<T>(const EnergyArgs<T>&, int, cudaStream_t);                               \
+    template cudaError_t launch_lite_energy<T>(T*, const double*, double, int, long long, const double*, int, int,  \
+                                               int, int, double*, cudaStream_t);                                  \
     template cudaError_t launch_transport<T>(const TransportArgs<T>&, int, cudaStream_t);                         \
     template cudaError_t launch_transport_plane<T>(const TransportArgs<T>&, int, cudaStream_t);                   \
     template cudaError_t launch_angle<T>(const AngleArgs<T>&, cudaStream_t);                                      \

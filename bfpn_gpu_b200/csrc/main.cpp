@@ -55,7 +55,7 @@ void printHelp(const char* prog) {
               << "  --nom <value>    Angular v grid points (paper Figure 3 uses 20)\n"
               << "  --precision <fp64|mixed> Device arithmetic (default: fp64)\n"
               << "  --device <n>     CUDA device ordinal (default: 0)\n"
-              << "  --lite-memory    Primary-only low-memory mode (not provided: exits with an error)\n"
+              << "  --lite-memory    Primary-only low-memory mode for large grid development\n"
               << "  --streaming-full Accepted; the state stays device resident\n"
               << "  --primary-only   Skip secondary proton evolution/source\n"
               << "  --energy-model <eq15|legacy> Energy update model (default: eq15)\n"

@@ -84,7 +84,8 @@ BFPnSolver::BFPnSolver(const GridParams& g, const PhysicsParams& p) : grid(g), p
     if (bfpn_footprint_bytes(&cg, &cp, phys.precision, &need) == BFPN_OK) {
         const double one = static_cast<double>(grid.Ny + 1) * (grid.Nz + 1) * grid.Ng * grid.Nmu * grid.Nom *
                            (phys.precision == BFPN_PREC_FP64 ? 8.0 : 4.0) / 1073741824.0;
-        std::cout << "Memory estimate:\n  Mode: full (device resident, "
+        std::cout << "Memory estimate:\n  Mode: " << (phys.lite_memory ? "lite-memory primary-only" : "full")
+                  << " (device resident, "
                   << (phys.precision == BFPN_PREC_FP64 ? "fp64" : "mixed fp32/fp64") << ")\n"
                   << std::fixed << std::setprecision(2) << "  One phase-space array: " << one << " GiB\n"
                   << "  Estimated device footprint: " << need / 1073741824.0 << " GiB" << std::defaultfloat
@@ -126,11 +127,16 @@ void BFPnSolver::solve(double tFinal) {  // bfpm_solver.cu:2166-2267
     std::cout << "Starting BFPn solver..." << std::endl;
     std::cout << "Grid: " << grid.Nx << "x" << grid.Ny << "x" << grid.Nz << ", Energy: " << grid.Ng
               << ", Angle: " << grid.Nmu << "x" << grid.Nom << std::endl;
+    if (phys.lite_memory)  // bfpm_solver.cu:2185-2187
+        std::cout << "Mode: lite-memory primary-only (no secondary, no DG slope, no YZ/angular transport)" << std::endl;
     idd_history_.clear();
     proxy_history_.clear();
     std::vector<double> moments_history;
-    std::vector<double> moments(2 * static_cast<size_t>(grid.Ng));
-    const bool per_step = phys.save_energy_moments || phys.profile_steps;
+    std::vector<double> moment_row(2 * static_cast<size_t>(grid.Ng));
+    // lite mode writes neither energy moments nor spot planes (its loop body
+    // ends after the IDD, bfpm_solver.cu:2191-2210)
+    const bool moments = phys.save_energy_moments && !phys.lite_memory;
+    const bool per_step = moments || phys.profile_steps;
     if (phys.profile_steps) check(bfpn_set_profiling(ctx_, 1), "profiling");
     const auto t0 = std::chrono::steady_clock::now();
     double t = 0.0;
@@ -140,7 +146,7 @@ void BFPnSolver::solve(double tFinal) {  // bfpm_solver.cu:2166-2267
         int chunk = per_step ? 1 : std::min(100 - step % 100, max_steps - step);
         // end a chunk at the first step after which an unsaved spot plane is due
         // (bfpm_solver.cu:2241-2246, depth accumulated the same way)
-        if (!phys.spot_depths.empty()) {
+        if (!phys.spot_depths.empty() && !phys.lite_memory) {
             double tt = t;
             for (int k = 1; k <= chunk; ++k) {
                 tt += grid.dt;
@@ -155,9 +161,9 @@ void BFPnSolver::solve(double tFinal) {  // bfpm_solver.cu:2166-2267
         }
         std::vector<double> idd(chunk), proxy(chunk);
         check(bfpn_step(ctx_, chunk, idd.data(), proxy.data()), "depth step");
-        if (phys.save_energy_moments) {
-            check(bfpn_energy_moments(ctx_, moments.data()), "energy moments");
-            moments_history.insert(moments_history.end(), moments.begin(), moments.end());
+        if (moments) {
+            check(bfpn_energy_moments(ctx_, moment_row.data()), "energy moments");
+            moments_history.insert(moments_history.end(), moment_row.begin(), moment_row.end());
         }
         for (int i = 0; i < chunk; ++i) {
             idd_history_.push_back(idd[i]);
@@ -167,7 +173,7 @@ void BFPnSolver::solve(double tFinal) {  // bfpm_solver.cu:2166-2267
             if (step % 100 == 0)
                 std::cout << "Step " << step << ", t = " << t << "/" << tFinal << ", IDD = " << idd[i] << std::endl;
         }
-        for (size_t i = 0; i < phys.spot_depths.size(); ++i)
+        for (size_t i = 0; i < phys.spot_depths.size() && !phys.lite_memory; ++i)
             if (!spot_saved[i] && t + 0.5 * grid.dt >= phys.spot_depths[i]) {
                 saveSpotPlane(phys.spot_depths[i], t);
                 spot_saved[i] = 1;
@@ -176,7 +182,7 @@ void BFPnSolver::solve(double tFinal) {  // bfpm_solver.cu:2166-2267
     const double seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     saveResults(idd_history_, "idd_output.txt");
     saveResults(proxy_history_, "dose_output.txt");
-    if (phys.save_energy_moments) saveEnergyMoments(moments_history, "energy_moments.txt");
+    if (moments) saveEnergyMoments(moments_history, "energy_moments.txt");
     std::cout << "Solver completed. Paper-style IDD saved to idd_output.txt" << std::endl;
     std::cout << "Diagnostic scalar proxy saved to dose_output.txt" << std::endl;
     if (phys.profile_steps && step > 0) {

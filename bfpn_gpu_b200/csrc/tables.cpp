@@ -423,6 +423,19 @@ std::vector<double> dose_coefficients(const BeamTables& t, const bfpn_phys& p) {
     return c;
 }
 
+std::vector<double> lite_coefficients(const BeamTables& t, double dt) {
+    const double dg = t.d.dg;
+    std::vector<double> c(2 * static_cast<size_t>(t.Ng));
+    for (int ek = 0; ek < t.Ng; ++ek) {
+        const double sig = std::max(t.sigma[ek], 0.0);
+        const double S_lo = std::max(t.S_s[ek], 0.0), S_hi = std::max(t.S_s[ek + 1], 0.0);
+        const double denom = 1.0 / dt + S_lo / dg + sig;
+        c[2 * ek] = S_hi / dg;
+        c[2 * ek + 1] = std::max(denom, kEpsilon);
+    }
+    return c;
+}
+
 std::vector<double> angle_factor(const BeamTables& t, const bfpn_phys& p, double dt) {
     const int Nom = t.Nom, Nmu = t.Nmu, NA = t.NA;
     const double norm = 4.0 / ((Nom + 1.0) * (Nmu + 1.0));

@@ -50,6 +50,11 @@ std::vector<double> energy_coefficients(const BeamTables& t, const bfpn_phys& p,
 // the quadrature du dv dy dz is applied at the end of the reduction.
 std::vector<double> dose_coefficients(const BeamTables& t, const bfpn_phys& p);
 
+// Lite-memory step constants per group (litePrimaryEnergyStepKernel,
+// bfpm_solver.cu:607-619): [2*ek] = max(S_s[ek+1],0) / dg and
+// [2*ek+1] = max(1/dt + max(S_s[ek],0)/dg + max(sigma_c[ek],0), eps).
+std::vector<double> lite_coefficients(const BeamTables& t, double dt);
+
 // Crank-Nicolson DST-I factor [Ng][NA] for step dt (buildDiffusionFactorKernel
 // times the 4/((Nom+1)(Nmu+1)) normalisation).
 std::vector<double> angle_factor(const BeamTables& t, const bfpn_phys& p, double dt);

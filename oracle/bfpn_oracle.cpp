@@ -377,8 +377,35 @@ static bool init_beam(Model& m) {
                        * std::exp(-std::pow((E - m.p.beam_energy) / m.p.sig_E / std::sqrt(2.0), 2));
     }
     for (int s = 0; s < 2; ++s)
-        for (int c = 0; c < 2; ++c) m.st[s][c].assign(m.cells, 0.0);
+        for (int c = 0; c < 2; ++c) m.st[s][c].assign(m.p.flags & BFPN_FLAG_LITE_MEMORY ? 0 : m.cells, 0.0);
     auto& F = m.st[0][0];
+    if (m.p.flags & BFPN_FLAG_LITE_MEMORY) {
+        // initializeLiteDistributionKernel, bfpm_solver.cu:993-1050:
+        // F = initial_scale * f1 * f2 with f1 = exp(-a1 (y^2+z^2)) * angular
+        F.assign(m.cells, 0.0);
+#pragma omp parallel for schedule(static)
+        for (int ek = 0; ek < m.Ng; ++ek)
+            for (int j = 0; j <= m.Nz; ++j)
+                for (int i = 0; i <= m.Ny; ++i)
+                    for (int k = 0; k < m.NA; ++k) {
+                        double y = -0.5 * m.g.Ly + i * m.dy;
+                        double z = -0.5 * m.g.Lz + j * m.dz;
+                        double d1 = std::abs(m.Omend[2 * k]) - c1;
+                        double d2 = std::abs(m.Omend[2 * k + 1]) - c2;
+                        double angular = std::exp(-m.p.a_2 * (d1 * d1 + d2 * d2));
+                        if (discrete) {
+                            bool sel = std::abs(d1) < 0.25 * m.dv && std::abs(d2) < 0.25 * m.du;
+                            angular = sel ? 1.0 / (n1 * n2 * m.du * m.dv) : 0.0;
+                        }
+                        double f1 = std::exp(-m.p.a_1 * (y * y + z * z)) * angular;
+                        double E = (ek + 0.5) * m.dg + 1.0;
+                        double f2 = 1.0 / std::sqrt(2.0 * PI) / m.p.sig_E *
+                                    std::exp(-std::pow((E - m.p.beam_energy) / m.p.sig_E / std::sqrt(2.0), 2));
+                        F[m.idx(ek, j * (m.Ny + 1) + i, k)] = scale * f1 * f2;
+                    }
+        m.steps_done = 0;
+        return true;
+    }
 #pragma omp parallel for schedule(static)
     for (int ek = 0; ek < m.Ng; ++ek)
         for (size_t l = 0; l < m.per_e; ++l) F[ek * m.per_e + l] = m.beam_yza[l] * m.beam_e[ek];
@@ -769,10 +796,69 @@ static void spot_plane(const Model& m, double* plane) {
     }
 }
 
+// litePrimaryEnergyStepKernel, bfpm_solver.cu:593-620 (stepLitePrimary,
+// 3396-3416): psi^1 only, first-order upwind in energy with attenuation.
+static void lite_step(Model& m) {
+    double* F = m.st[0][0].data();
+#pragma omp parallel for schedule(static)
+    for (long long lane = 0; lane < static_cast<long long>(m.per_e); ++lane) {
+        double next_F = 0.0;
+        for (int ek = m.Ng - 1; ek >= 0; --ek) {
+            size_t id = static_cast<size_t>(ek) * m.per_e + lane;
+            double Fg = std::max(F[id], 0.0);
+            double sig = std::max(m.sigma[ek], 0.0);
+            double S_lo = std::max(m.S_s[ek], 0.0);
+            double S_hi = std::max(m.S_s[ek + 1], 0.0);
+            double denom = 1.0 / m.dt + S_lo / m.dg + sig;
+            double F_val = (Fg / m.dt + S_hi / m.dg * next_F) / std::max(denom, EPSILON);
+            F[id] = std::max(F_val, 0.0);
+            next_F = F[id];
+        }
+    }
+}
+
+// integratedDepthDoseLiteKernel, bfpm_solver.cu:523-591
+// (computeIntegratedDepthDoseLite, 3528-3558): psi^1 only.
+static double lite_idd(const Model& m) {
+    const double* F = m.st[0][0].data();
+    const bool trap = m.p.flags & BFPN_FLAG_TRAPEZOIDAL_YZ;
+    const bool cat = m.p.flags & BFPN_FLAG_DOSE_CATASTROPHIC_LOSS;
+    double total = 0.0;
+#pragma omp parallel for schedule(static) reduction(+ : total)
+    for (int ek = 0; ek < m.Ng; ++ek) {
+        double S_mid = 0.5 * (m.S_s[ek] + m.S_s[ek + 1]);
+        double E_mid = 0.5 * (m.en[ek] + m.en[ek + 1]);
+        double part = 0.0;
+        for (int s = 0; s < m.nyz; ++s) {
+            int iy = s % (m.Ny + 1), iz = s / (m.Ny + 1);
+            double w = 1.0;
+            if (trap) {
+                if (iy == 0 || iy == m.Ny) w *= 0.5;
+                if (iz == 0 || iz == m.Nz) w *= 0.5;
+            }
+            for (int a = 0; a < m.NA; ++a) {
+                double Fv = F[m.idx(ek, s, a)];
+                double dose = Fv * S_mid * m.dg;
+                if (cat) dose += Fv * E_mid * std::max(m.sigma[ek], 0.0) * m.dg;
+                part += w * dose / m.p.density;
+            }
+        }
+        total += part;
+    }
+    return total * m.du * m.dv * m.dy * m.dz;
+}
+
 // stepPrimary (bfpm_solver.cu:3238-3311), stepPrimaryEnergyOnly
 // (3313-3333), stepSecondary (3335-3394), and the loop body of solve
 // (2190-2254).
 static void step(Model& m, double* idd_out, double* proxy_out) {
+    if (m.p.flags & BFPN_FLAG_LITE_MEMORY) {  // the lite branch of solve, bfpm_solver.cu:2191-2210
+        lite_step(m);
+        *idd_out = lite_idd(m);
+        *proxy_out = 0.0;
+        m.steps_done++;
+        return;
+    }
     const double h = 0.5 * m.dt;
     const unsigned fl = m.p.flags;
     const bool no_tr = fl & BFPN_FLAG_NO_TRANSPORT, no_an = fl & BFPN_FLAG_NO_ANGLE;
@@ -864,11 +950,16 @@ unsigned long long oracle_cells(void* h) { return static_cast<Model*>(h)->cells;
 
 void oracle_get_state(void* h, int species, int coef, double* out) {
     auto* m = static_cast<Model*>(h);
+    if (m->st[species][coef].size() != m->cells) {  // lite-memory mode holds psi^1 of the primary only
+        std::memset(out, 0, m->cells * sizeof(double));
+        return;
+    }
     std::memcpy(out, m->st[species][coef].data(), m->cells * sizeof(double));
 }
 
 void oracle_set_state(void* h, int species, int coef, const double* in) {
     auto* m = static_cast<Model*>(h);
+    if (m->st[species][coef].size() != m->cells) return;
     std::memcpy(m->st[species][coef].data(), in, m->cells * sizeof(double));
 }
 
@@ -893,7 +984,15 @@ void oracle_source(void* h, double* out) {
     if (out) std::memcpy(out, m->source.data(), m->cells * sizeof(double));
 }
 
-void oracle_idd(void* h, double* idd, double* proxy) { orc::idd(*static_cast<Model*>(h), idd, proxy); }
+void oracle_idd(void* h, double* idd, double* proxy) {
+    auto* m = static_cast<Model*>(h);
+    if (m->p.flags & BFPN_FLAG_LITE_MEMORY) {
+        *idd = orc::lite_idd(*m);
+        *proxy = 0.0;
+        return;
+    }
+    orc::idd(*m, idd, proxy);
+}
 
 void oracle_energy_moments(void* h, double* out) { orc::energy_moments(*static_cast<Model*>(h), out); }
 

@@ -80,3 +80,17 @@ def test_cli_reports_missing_tables(tmp_path):
     r = subprocess.run([CLI, "10", "--time", "0.1", "--data", str(tmp_path / "nowhere"), "--ny", "2", "--nz", "2",
                         "--nmu", "2", "--nom", "2", "--ng", "10"], cwd=tmp_path, capture_output=True, text=True)
     assert r.returncode == 1 and "Error:" in r.stderr
+
+
+def test_cli_lite_memory_matches_oracle(tmp_path):
+    args = ("50 --time 2 --data %s --lg 59 --ng 40 --energy 40 --sigma-e 2 --sigma-yz 0.4 --ny 6 --nz 5 "
+            "--nmu 4 --nom 5 --ly 2 --lz 1.5 --lite-memory --save-energy-moments" % table_dir("synthetic500")).split()
+    out = run_cli(tmp_path, args)
+    assert "Mode: lite-memory primary-only" in out
+    cfg = parse_args(args)
+    mu, sig = read_tables(table_dir("synthetic500"), cfg.ng)
+    idd_o, prox_o = O.Oracle(cfg.grid(), cfg.phys(), mu, sig).step(cfg.max_steps())
+    res = np.loadtxt(tmp_path / "idd_output.txt")
+    assert np.abs(res[:, 1] - idd_o).max() <= 1e-10 * np.abs(idd_o).max()
+    assert not np.any(np.loadtxt(tmp_path / "dose_output.txt")[:, 1])
+    assert not (tmp_path / "energy_moments.txt").exists()  # the lite loop writes no moments

@@ -48,3 +48,17 @@ def test_c1_fixture_matches_current_oracle_prefix():
     o = O.Oracle(cfg.grid(), cfg.phys(), mu, sig)
     idd, proxy = o.step(3)
     assert np.array_equal(idd, ref[:3, 1]) and np.array_equal(proxy, ref[:3, 2])
+
+
+def test_oracle_lite_memory_mode_runs():
+    """Lite-memory restatement: psi^1 only, attenuating, proxy 0."""
+    from bfpn_gpu_b200 import make_config
+    cfg = make_config(nx=100, ny=4, nz=4, nmu=3, nom=3, ng=40, lg=59.0, beam_energy=40.0, sigma_e=2.0,
+                      sigma_yz=0.4, ly=2.0, lz=2.0, lite_memory=True, t_final=2.0)
+    mu, sig = material_tables(cfg, "synthetic500")
+    ora = O.Oracle(cfg.grid(), cfg.phys(), mu, sig)
+    m0 = ora.get_state(0, 0).sum()
+    idd, prox = ora.step(10)
+    assert np.all(idd > 0) and not np.any(prox)
+    assert 0 < ora.get_state(0, 0).sum() < m0
+    assert not np.any(ora.get_state(0, 1)) and not np.any(ora.get_state(1, 0))

@@ -239,6 +239,43 @@ def test_mixed_precision_idd_within_tolerance():
     assert rel_err(i_mix, i_ref) < 1e-3
 
 
+@pytest.mark.parametrize("flags", [{}, {"trapezoidal_yz": True, "discrete_angle_delta": True,
+                                        "normalize_initial_mass": True}])
+def test_lite_memory_steps_fp64(flags):
+    """--lite-memory: psi^1 of the primary only, upwind energy step, lite IDD."""
+    cfg = small_cfg(lite_memory=True, **flags)
+    ctx, ora = build(cfg)
+    n = 15
+    idd_g, prox_g = ctx.step(n)
+    idd_o, prox_o = ora.step(n)
+    assert np.abs(idd_o).max() > 0 and not np.any(prox_o) and not np.any(prox_g)
+    assert rel_err(idd_g, idd_o) < STEP_TOL
+    assert rel_err(ctx.get_state(0, 0), ora.get_state(0, 0)) < STEP_TOL
+    a, b = ctx.idd()
+    assert abs(a - idd_g[-1]) <= 1e-12 * abs(a) and b == 0.0
+    # only psi^1 of the primary exists, and the operators of the full path are not available
+    for call in (lambda: ctx.get_state(0, 1), lambda: ctx.get_state(1, 0), lambda: ctx.energy(0, 0.1),
+                 lambda: ctx.transport(0, 0, 0.1, False), lambda: ctx.angle(0, 0, 0.1),
+                 lambda: ctx.secondary_source(), lambda: ctx.energy_moments(), lambda: ctx.spot_plane()):
+        with pytest.raises(capi.BfpnError):
+            call()
+    big = make_config(ny=20, nz=20, nmu=20, nom=20, ng=500)  # device footprint: one array instead of eight
+    lite = make_config(ny=20, nz=20, nmu=20, nom=20, ng=500, lite_memory=True)
+    assert capi.footprint_bytes(lite.grid(), lite.phys()) < capi.footprint_bytes(big.grid(), big.phys()) / 7
+
+
+def test_lite_memory_mixed_within_tolerance():
+    cfg = small_cfg(lite_memory=True, t_final=8.0)
+    mu, sig = read_tables(table_dir("synthetic500"), cfg.ng)
+    out = []
+    for prec in (capi.PREC_FP64, capi.PREC_MIXED):
+        ctx = Context(cfg.grid(), cfg.phys(), prec)
+        ctx.load_tables(mu, sig)
+        ctx.init_beam()
+        out.append(ctx.step(cfg.max_steps())[0])
+    assert rel_err(out[1], out[0]) < 1e-5
+
+
 def test_errors_are_reported_not_fatal():
     cfg = small_cfg()
     ctx = Context(cfg.grid(), cfg.phys())
