@@ -56,6 +56,17 @@ class Phys(ctypes.Structure):
                 ("material", ctypes.c_int32), ("flags", ctypes.c_uint32)]
 
 
+class Beam(ctypes.Structure):
+    _fields_ = [("grid", Grid), ("phys", Phys), ("precision", ctypes.c_int32), ("nsteps", ctypes.c_int32),
+                ("mu", ctypes.POINTER(ctypes.c_double)), ("mu_rows", ctypes.c_int32),
+                ("sigma_c", ctypes.POINTER(ctypes.c_double)), ("sigma_rows", ctypes.c_int32)]
+
+
+class BeamInfo(ctypes.Structure):
+    _fields_ = [("steps", ctypes.c_int32), ("device", ctypes.c_int32), ("queue_ms", ctypes.c_double),
+                ("run_ms", ctypes.c_double)]
+
+
 # every entry point of include/bfpn_capi.h with its ctypes signature
 _vp = ctypes.c_void_p
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -101,6 +112,15 @@ SIGNATURES = {
     "bfpn_energy_moments": (ctypes.c_int, [_vp, _dp]),
     "bfpn_spot_plane": (ctypes.c_int, [_vp, _dp]),
     "bfpn_idd_noalloc": (ctypes.c_int, [ctypes.POINTER(Grid), _i32, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _vp]),
+    "bfpn_server_create": (ctypes.c_int, [ctypes.POINTER(_i32), _i32, _i32, ctypes.POINTER(_vp)]),
+    "bfpn_server_submit": (ctypes.c_int, [_vp, ctypes.POINTER(Beam), ctypes.POINTER(ctypes.c_uint64)]),
+    "bfpn_server_poll": (_i32, [_vp, ctypes.c_uint64]),
+    "bfpn_server_wait": (ctypes.c_int, [_vp, ctypes.c_uint64, ctypes.c_double, _dp, _dp, _i32,
+                                        ctypes.POINTER(BeamInfo)]),
+    "bfpn_server_destroy": (ctypes.c_int, [_vp]),
+    "bfpn_server_last_error": (ctypes.c_char_p, []),
+    "bfpn_batch_run": (ctypes.c_int, [ctypes.POINTER(Beam), _i32, ctypes.POINTER(_i32), _i32, _i32,
+                                      ctypes.POINTER(_dp), ctypes.POINTER(_dp), ctypes.POINTER(ctypes.c_int)]),
     "bfpn_device_count": (_i32, []),
     "bfpn_device_info": (_i32, [_i32, ctypes.c_char_p, _i32]),
     "bfpn_stream": (_vp, [_vp]),
@@ -170,6 +190,85 @@ def footprint_bytes(grid, phys, precision=PREC_FP64):
     if rc != OK:
         raise BfpnError(rc, lib().bfpn_last_error(None).decode())
     return int(out.value)
+
+
+def _server_error(rc):
+    return BfpnError(rc, lib().bfpn_server_last_error().decode())
+
+
+def make_beam(grid, phys, mu, sigma, nsteps, precision=PREC_FP64):
+    """A bfpn_beam request; the returned object keeps its table arrays alive."""
+    mu = np.ascontiguousarray(mu, dtype=np.float64).reshape(-1, 3)
+    sigma = np.ascontiguousarray(sigma, dtype=np.float64)
+    b = Beam(grid=grid, phys=phys, precision=precision, nsteps=int(nsteps), mu=_ptr(mu), mu_rows=mu.shape[0],
+             sigma_c=_ptr(sigma), sigma_rows=sigma.size)
+    b._keep = (mu, sigma)
+    return b
+
+
+class Server:
+    """bfpn_server_*: a queue of independent beams served by worker threads,
+    each owning one context on one device."""
+
+    def __init__(self, devices=(0,), workers_per_device=1):
+        devs = (_i32 * len(devices))(*devices)
+        h = _vp()
+        rc = lib().bfpn_server_create(devs, len(devices), workers_per_device, ctypes.byref(h))
+        if rc != OK:
+            raise _server_error(rc)
+        self._h = h
+
+    def submit(self, beam):
+        t = ctypes.c_uint64(0)
+        rc = lib().bfpn_server_submit(self._h, ctypes.byref(beam), ctypes.byref(t))
+        if rc != OK:
+            raise _server_error(rc)
+        return t.value
+
+    def poll(self, ticket):
+        return lib().bfpn_server_poll(self._h, ticket)
+
+    def wait(self, ticket, nsteps, timeout=-1.0):
+        """(idd, proxy, info dict) of a finished beam."""
+        idd, prox, info = np.empty(nsteps), np.empty(nsteps), BeamInfo()
+        rc = lib().bfpn_server_wait(self._h, ticket, timeout, _ptr(idd), _ptr(prox), nsteps, ctypes.byref(info))
+        if rc != OK:
+            raise _server_error(rc)
+        return idd, prox, {"steps": info.steps, "device": info.device, "queue_ms": info.queue_ms,
+                           "run_ms": info.run_ms}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().bfpn_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def batch_run(beams, devices=(0,), workers_per_device=2):
+    """bfpn_batch_run: [(idd, proxy)] per beam, raising on the first failure."""
+    n = len(beams)
+    arr = (Beam * n)(*beams)
+    idd = [np.empty(b.nsteps) for b in beams]
+    prox = [np.empty(b.nsteps) for b in beams]
+    ip = (_dp * n)(*[_ptr(a) for a in idd])
+    pp = (_dp * n)(*[_ptr(a) for a in prox])
+    st = (ctypes.c_int * n)()
+    devs = (_i32 * len(devices))(*devices)
+    rc = lib().bfpn_batch_run(arr, n, devs, len(devices), workers_per_device, ip, pp, st)
+    if rc != OK:
+        raise _server_error(rc)
+    return list(zip(idd, prox))
 
 
 def idd_noalloc(grid, precision, trapezoidal_yz, F0, f0, F1, f1, dose_coef, out, device=0, stream=None):

@@ -276,6 +276,58 @@ bfpn_status bfpn_energy_moments(bfpn_ctx* ctx, double* out);
  * angles of the Eq. 24 dose of primary + secondary / density.  nyz doubles. */
 bfpn_status bfpn_spot_plane(bfpn_ctx* ctx, double* plane);
 
+/* ---- multi-beam batching and serving ------------------------------------
+ * The reference runs one beam per process (main.cu:344-348).  These calls
+ * serve many independent beams: a thread-safe queue of requests worked by
+ * threads that each own one context (stream + CUDA graph) on one device, so
+ * several beams run at once per GPU and across GPUs.  A worker keeps its
+ * context between requests of the same shape and only reloads tables and
+ * beam.  Each beam's IDD / proxy history is the same as bfpn_step on a fresh
+ * context would give. */
+typedef struct bfpn_beam {
+    bfpn_grid grid;
+    bfpn_phys phys;
+    int32_t precision;       /* BFPN_PREC_* */
+    int32_t nsteps;          /* depth steps to run (>= 1) */
+    const double* mu;        /* mu_rows x 3, as for bfpn_load_tables (copied at submit) */
+    int32_t mu_rows;
+    const double* sigma_c;   /* sigma_rows values (copied at submit) */
+    int32_t sigma_rows;
+} bfpn_beam;
+
+typedef struct bfpn_beam_info {
+    int32_t steps;           /* steps run (0 on failure) */
+    int32_t device;          /* device that ran it */
+    double queue_ms;         /* submit -> start */
+    double run_ms;           /* start -> finish (context set-up, tables, beam, steps) */
+} bfpn_beam_info;
+
+typedef struct bfpn_server bfpn_server;
+
+/* Start workers_per_device threads on each listed device (NULL / 0 devices:
+ * device 0). */
+bfpn_status bfpn_server_create(const int32_t* devices, int32_t n_devices, int32_t workers_per_device,
+                               bfpn_server** out);
+/* Queue one beam; thread-safe.  *ticket identifies it for poll / wait. */
+bfpn_status bfpn_server_submit(bfpn_server* server, const bfpn_beam* beam, uint64_t* ticket);
+/* 1 finished (success or failure), 0 queued or running, -1 unknown ticket. */
+int32_t bfpn_server_poll(bfpn_server* server, uint64_t ticket);
+/* Wait (timeout_s < 0: no limit; BFPN_TIMEOUT when it runs out, the beam
+ * stays collectable), then copy the histories (capacity >= nsteps; idd /
+ * proxy may be NULL) and release the ticket.  Returns the beam's status. */
+bfpn_status bfpn_server_wait(bfpn_server* server, uint64_t ticket, double timeout_s, double* idd, double* proxy,
+                             int32_t capacity, bfpn_beam_info* info);
+/* Finish queued and running beams, stop the workers, free the server. */
+bfpn_status bfpn_server_destroy(bfpn_server* server);
+/* Message of the last failed server / batch call on this thread. */
+const char* bfpn_server_last_error(void);
+/* Run n beams to completion on a temporary server; idd_out[i] / proxy_out[i]
+ * hold beams[i].nsteps doubles (either array list may be NULL); status_out[i]
+ * (may be NULL) receives each beam's status.  Returns the first failure. */
+bfpn_status bfpn_batch_run(const bfpn_beam* beams, int32_t n, const int32_t* devices, int32_t n_devices,
+                           int32_t workers_per_device, double* const* idd_out, double* const* proxy_out,
+                           bfpn_status* status_out);
+
 /* ---- integrated depth dose without device allocation -------------------
  * No counterpart in the reference: its IDD (computeIntegratedDepthDose +
  * computeScalarDoseProxy, bfpm_solver.cu:3473-3502, 3418-3444) always runs

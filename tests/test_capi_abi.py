@@ -137,3 +137,18 @@ def test_idd_noalloc_checks_arguments_before_any_device_work():
         with pytest.raises(capi.BfpnError) as e:
             capi.idd_noalloc(cfg.grid(), capi.PREC_FP64, False, fake, fake, None, None, fake, fake)
         assert e.value.status == capi.NO_DEVICE
+
+
+def test_server_without_device_fails_cleanly():
+    if capi.lib().bfpn_device_count() > 0:
+        pytest.skip("a CUDA device is present")
+    with pytest.raises(capi.BfpnError) as e:
+        capi.Server()
+    assert e.value.status == capi.NO_DEVICE
+    cfg = make_config(ny=2, nz=2, nmu=2, nom=2, ng=10)
+    mu, sig = read_tables(table_dir("synthetic500"), cfg.ng)
+    with pytest.raises(capi.BfpnError):
+        capi.batch_run([capi.make_beam(cfg.grid(), cfg.phys(), mu, sig, 2)])
+    with pytest.raises(capi.BfpnError) as e:
+        capi.Server(workers_per_device=0)
+    assert e.value.status == capi.INVALID_ARG
