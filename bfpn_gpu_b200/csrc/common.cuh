@@ -39,6 +39,11 @@ enum EnergyCoef {
 
 enum EnergyMode { EMODE_EQ15 = 0, EMODE_EQ15_STRAG = 1, EMODE_LEGACY = 2 };
 
+// 16-byte vector of T for staging loads and stores.
+template <typename T> struct Vec16;
+template <> struct Vec16<float> { using type = float4; static constexpr int W = 4; };
+template <> struct Vec16<double> { using type = double2; static constexpr int W = 2; };
+
 // Arguments of one energy half-step over one species.
 template <typename T>
 struct EnergyArgs {

@@ -506,10 +506,27 @@ __global__ void __launch_bounds__((NP * AC + 31) / 32 * 32) transport_plane_kern
     const T dt = a.dt, hdt = T(0.5) * a.dt;
     const T lo = a.preserve_sign ? -INFINITY : T(0);
 
-    for (int e = threadIdx.x; e < NP * NP * AC; e += blockDim.x) {
-        const int aa = e % AC, p = e / AC;
-        const int z = p / NP, y = p - z * NP;
-        Fs[z * RS + y * AC + aa] = (a0 + aa < NA) ? in[static_cast<size_t>(p) * NA + aa] : T(0);
+    constexpr int NT = (NP * AC + 31) / 32 * 32;  // == blockDim.x
+    if (AC % Vec16<T>::W == 0 && NA % Vec16<T>::W == 0) {
+        // 16-byte loads, several in flight per thread (a0 and NA are multiples of
+        // the vector width, so a vector is wholly inside or wholly past NA)
+        using V = typename Vec16<T>::type;
+        constexpr int W = Vec16<T>::W, NV = NP * NP * AC / W;
+#pragma unroll 4
+        for (int v = threadIdx.x; v < NV; v += NT) {
+            const int e = v * W, aa = e % AC, p = e / AC;
+            const int z = p / NP, y = p - z * NP;
+            V val{};
+            if (a0 + aa < NA) val = *reinterpret_cast<const V*>(in + static_cast<size_t>(p) * NA + aa);
+            *reinterpret_cast<V*>(Fs + z * RS + y * AC + aa) = val;
+        }
+    } else {
+#pragma unroll 4
+        for (int e = threadIdx.x; e < NP * NP * AC; e += NT) {
+            const int aa = e % AC, p = e / AC;
+            const int z = p / NP, y = p - z * NP;
+            Fs[z * RS + y * AC + aa] = (a0 + aa < NA) ? in[static_cast<size_t>(p) * NA + aa] : T(0);
+        }
     }
     __syncthreads();
     const bool act = line < NP;
@@ -743,8 +760,24 @@ __global__ void __launch_bounds__(256) angle_dst_kernel(AngleArgs<T> a, SineTabl
     T* __restrict__ F = a.F + s0 * NA;
     // the block's slices are contiguous: element e of the run goes to row e / N
     // of the padded layout, i.e. to e + e / N
-    for (int e = threadIdx.x; e < ns * NA; e += blockDim.x) X[e + e / N] = F[e];
-    for (int e = threadIdx.x; e < nrows * NA; e += blockDim.x) Fac[e] = a.fac[ek0 * NA + e];
+    constexpr int W = Vec16<T>::W;
+    using V = typename Vec16<T>::type;
+    if (NA % W == 0) {  // the run starts at s0 * NA: 16-byte aligned
+#pragma unroll 4
+        for (int v = threadIdx.x; v < ns * NA / W; v += 256) {
+            const V val = reinterpret_cast<const V*>(F)[v];
+            const T* t = reinterpret_cast<const T*>(&val);
+#pragma unroll
+            for (int k = 0; k < W; ++k) {
+                const int e = v * W + k;
+                X[e + e / N] = t[k];
+            }
+        }
+    } else {
+#pragma unroll 4
+        for (int e = threadIdx.x; e < ns * NA; e += 256) X[e + e / N] = F[e];
+    }
+    for (int e = threadIdx.x; e < nrows * NA; e += 256) Fac[e] = a.fac[ek0 * NA + e];
     T c[(N + 1) / 2];
 #pragma unroll
     for (int k = 0; k < (N + 1) / 2; ++k) c[k] = S.c[k];
@@ -783,7 +816,22 @@ __global__ void __launch_bounds__(256) angle_dst_kernel(AngleArgs<T> a, SineTabl
         for (int k = 0; k < N; ++k) R[k] = y[k];
     }
     __syncthreads();
-    for (int e = threadIdx.x; e < ns * NA; e += blockDim.x) F[e] = X[e + e / N];
+    if (NA % W == 0) {
+#pragma unroll 4
+        for (int v = threadIdx.x; v < ns * NA / W; v += 256) {
+            V val;
+            T* t = reinterpret_cast<T*>(&val);
+#pragma unroll
+            for (int k = 0; k < W; ++k) {
+                const int e = v * W + k;
+                t[k] = X[e + e / N];
+            }
+            reinterpret_cast<V*>(F)[v] = val;
+        }
+    } else {
+#pragma unroll 4
+        for (int e = threadIdx.x; e < ns * NA; e += 256) F[e] = X[e + e / N];
+    }
 }
 
 template <int N, typename T>
