@@ -79,8 +79,9 @@ struct bfpn_ctx {
     int* zero_counter = nullptr;    // scratch counter for one-off IDD reductions
     int* dev_err = nullptr;         // device error word (bounded waits that ran out)
     void* bblob = nullptr;          // split-bf16 angular kernel tiles for the tensor-core source
+    void* ablob = nullptr;          // packed split-bf16 A operand (pipelined tensor-core source)
     bool use_umma = true;
-    int umma_nt = 0, umma_bk = 32, umma_ntiles = 0;
+    int umma_nt = 0, umma_bk = 16, umma_ntiles = 0;
     double* scalar_out = nullptr;   // [2] one-off IDD / proxy
     double* moments = nullptr;      // [Ng][2]
     double* plane = nullptr;        // [nyz] spot dose plane
@@ -269,6 +270,18 @@ bfpn_status dalloc(bfpn_ctx* c, void** out, size_t bytes) {
     return BFPN_OK;
 }
 
+// Frees one buffer from dalloc (no-op for nullptr) and sets the pointer to nullptr.
+void dfree(bfpn_ctx* c, void*& p) {
+    if (!p) return;
+    for (size_t i = 0; i < c->allocs.size(); ++i)
+        if (c->allocs[i].p == p) {
+            cudaFree(p);
+            c->allocs.erase(c->allocs.begin() + static_cast<long>(i));
+            break;
+        }
+    p = nullptr;
+}
+
 void free_all(bfpn_ctx* c) {
     for (auto& p : c->pending) {
         cudaEventDestroy(p.a);
@@ -430,12 +443,12 @@ cudaError_t enq_source(bfpn_ctx* c) {
     a.NA = c->NA;
     a.dg = c->d.dg;
     cudaError_t e;
-    if (sizeof(T) == sizeof(float) && c->use_umma && c->bblob) {
+    if (sizeof(T) == sizeof(float) && c->use_umma && c->bblob && c->ablob) {
         e = prof(c, BFPN_KERNEL_SOURCE_ANGULAR, [&] {
-            return launch_source_angular_umma(as<const float>(c->st[0][0]), as<const float>(c->st[0][1]),
-                                              static_cast<const uint8_t*>(c->bblob), c->groups, c->n_groups,
-                                              as<float>(c->A1), as<float>(c->A2), c->dev_err, c->nyz, c->NA, c->umma_nt,
-                                              c->umma_bk, c->umma_ntiles, c->stream);
+            return launch_source_angular_pipe(as<const float>(c->st[0][0]), as<const float>(c->st[0][1]),
+                                              static_cast<uint8_t*>(c->ablob), static_cast<const uint8_t*>(c->bblob),
+                                              c->groups, c->n_groups, as<float>(c->A1), as<float>(c->A2), c->dev_err,
+                                              c->nyz, c->NA, c->umma_nt, c->umma_bk, c->umma_ntiles, c->stream);
         });
     } else {
         e = prof(c, BFPN_KERNEL_SOURCE_ANGULAR, [&] { return launch_source_angular<T>(a, c->stream); });
@@ -913,11 +926,29 @@ bfpn_status bfpn_load_tables(bfpn_ctx* c, const double* mu, int32_t mu_rows, con
     c->n_groups = static_cast<int>(groups.size());
     if (!groups.empty() && (s = upload_f64(c, c->groups, groups.data(), groups.size() * sizeof(int))) != BFPN_OK)
         return s;
+    // tables of an earlier load (a context reused for another beam): the step
+    // graph captured their addresses, so it goes too
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    if (c->graph_exec) {
+        cudaGraphExecDestroy(c->graph_exec);
+        c->graph_exec = nullptr;
+        c->graph_key = -1;
+    }
+    dfree(c, c->ablob);
+    dfree(c, c->bblob);
     if (c->prec == BFPN_PREC_MIXED && c->A1 && !groups.empty()) {
         // tensor-core source: output tiles of <= 256 columns, multiples of 16
         c->umma_ntiles = (c->NA + 255) / 256;
         c->umma_nt = ((c->NA + c->umma_ntiles - 1) / c->umma_ntiles + 15) / 16 * 16;
         std::vector<uint8_t> blob;
+        // the packed split-bf16 copy of the A operand; without room for it the
+        // source's angular stage stays on the fp32 CUDA-core kernel
+        const size_t pack = umma_pack_bytes(c->n_groups, c->nyz, c->NA, c->umma_bk);
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess && pack + (256u << 20) < free_b) {
+            void* ab = nullptr;
+            if (dalloc(c, &ab, pack) == BFPN_OK) c->ablob = ab;
+        }
         build_umma_blob(T.ker_v.data(), groups.data(), c->n_groups, c->NA, c->umma_nt, c->umma_bk, blob);
         void* d = nullptr;
         if ((s = dalloc(c, &d, blob.size())) != BFPN_OK) return s;
@@ -1035,7 +1066,7 @@ bfpn_status bfpn_energy_eq15(bfpn_ctx* c, int32_t species, double dt, int32_t wi
     if (c->prec == BFPN_PREC_FP64) CUDA_TRY(c, enq_energy<double>(c, species, c->ecoef_op, with_source != 0, nullptr));
     else CUDA_TRY(c, enq_energy<float>(c, species, c->ecoef_op, with_source != 0, nullptr));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
-    return BFPN_OK;
+    return check_device_error(c);
 }
 
 bfpn_status bfpn_transport_eq18(bfpn_ctx* c, int32_t species, int32_t coef, double dt, int32_t preserve_sign) {

@@ -144,11 +144,13 @@ cudaError_t launch_spot_plane(const T* F, const T* f, const T* F1, const T* f1, 
                               int nyz, int NA, double dudv, double* plane, cudaStream_t s);
 
 // Tensor-core (tcgen05) angular contraction of the source, float state
-// (kernels_umma.cu).  bblob from build_umma_blob; err receives a non-zero
-// code if a CTA's bounded wait ran out.
-cudaError_t launch_source_angular_umma(const float* P1, const float* P2, const uint8_t* bblob, const int* groups,
-                                       int n_groups, float* A1, float* A2, int* err, int nyz, int NA, int NT, int BK,
-                                       int n_ntiles, cudaStream_t s);
+// (kernels_umma.cu): pack the A operand into ablob (umma_pack_bytes), then a
+// bulk-copy-fed GEMM; bblob from build_umma_blob with BK = 16; err receives a
+// non-zero code if a CTA's bounded wait ran out.
+cudaError_t launch_source_angular_pipe(const float* P1, const float* P2, uint8_t* ablob, const uint8_t* bblob,
+                                       const int* groups, int n_groups, float* A1, float* A2, int* err, int nyz,
+                                       int NA, int NT, int BK, int n_ntiles, cudaStream_t s);
+size_t umma_pack_bytes(int n_groups, int nyz, int NA, int BK);
 // Host: split-bf16 B tiles of ker_v ([Ng][NA][NA] double) for the listed
 // groups, in the kernel's shared-memory layout.
 void build_umma_blob(const double* ker_v, const int* groups, int n_groups, int NA, int NT, int BK,

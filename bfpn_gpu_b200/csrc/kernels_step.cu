@@ -33,6 +33,41 @@ cudaError_t launch_angle_generic(const AngleArgs<T>& a, cudaStream_t s);
 // ---------------------------------------------------------------------------
 constexpr int kEnergyLanesPerThread = 2;
 
+// One group of the eq15 / legacy recursion for one lane (energyDgCnKernel,
+// energy_solver.cu:88-159): Fg, fg old values of group ek, sg its source,
+// Fn the old psi^1 of group ek-1 (straggling), F_hi_old / f_hi_old the old
+// values of group ek+1 and next_F / next_f its new values.
+template <int MODE>
+__device__ __forceinline__ void energy_lane_update(const double* __restrict__ c, int ek, double Fg, double fg,
+                                                   double sg, double Fn, double F_hi_old, double f_hi_old,
+                                                   double next_F, double next_f, double& Fv, double& fv) {
+    if (MODE == EMODE_LEGACY) {
+        const double idt = __ldg(c + EC_L_IDT), hi = __ldg(c + EC_L_HI), inv = __ldg(c + EC_L_INV_DEN);
+        Fv = (fmax(Fg, 0.0) * idt + hi * next_F + sg) * inv;
+        fv = (fg * idt + hi * next_f) * inv;
+        const double lapc = __ldg(c + EC_L_LAP);
+        if (lapc > 0.0) {
+            const double Flo = (ek > 0) ? Fn : 0.0;
+            Fv += lapc * (fmax(F_hi_old, 0.0) - 2.0 * fmax(Fg, 0.0) + fmax(Flo, 0.0));
+        }
+        Fv = fmax(Fv, 0.0);
+        fv = fmax(fv, 0.0);
+    } else {
+        const double up = F_hi_old - f_hi_old;
+        const double cur = Fg - fg;
+        double common = __ldg(c + EC_C_UP) * up + __ldg(c + EC_C_CUR) * cur + __ldg(c + EC_C_F) * Fg + sg;
+        if (MODE == EMODE_EQ15_STRAG) {
+            const double Flo = (ek > 0) ? Fn : 0.0;
+            common += __ldg(c + EC_S_HI) * F_hi_old + __ldg(c + EC_S_LO) * Flo - __ldg(c + EC_S_G) * Fg;
+        }
+        const double hi_delta = next_F - next_f;
+        const double rhs = __ldg(c + EC_R_F) * fg + __ldg(c + EC_R_UP) * up + __ldg(c + EC_R_CUR) * cur +
+                           __ldg(c + EC_R_FG) * Fg - __ldg(c + EC_A) * common + __ldg(c + EC_R_HI) * hi_delta;
+        fv = rhs * __ldg(c + EC_INV_COE);
+        Fv = __ldg(c + EC_F_FROM_F) * fv + __ldg(c + EC_INV_F) * common + __ldg(c + EC_F_FROM_HI) * hi_delta;
+    }
+}
+
 template <int MODE, typename T, int LPT>
 __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 5 : 4) energy_kernel(EnergyArgs<T> a) {
     constexpr int D = 4;  // groups prefetched ahead of use
@@ -90,32 +125,7 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 5 : 4) energy_kernel(Ene
             // old value of group ek-1 (straggling): the next slot, or the refill of slot 0
             const double Fn = static_cast<double>(rF[(k + 1) % D][j]);
             double Fv, fv;
-            if (MODE == EMODE_LEGACY) {
-                const double idt = __ldg(c + EC_L_IDT), hi = __ldg(c + EC_L_HI), inv = __ldg(c + EC_L_INV_DEN);
-                Fv = (fmax(Fg, 0.0) * idt + hi * next_F[j] + sg) * inv;
-                fv = (fg * idt + hi * next_f[j]) * inv;
-                const double lapc = __ldg(c + EC_L_LAP);
-                if (lapc > 0.0) {
-                    const double Flo = (ek > 0) ? Fn : 0.0;
-                    Fv += lapc * (fmax(F_hi_old[j], 0.0) - 2.0 * fmax(Fg, 0.0) + fmax(Flo, 0.0));
-                }
-                Fv = fmax(Fv, 0.0);
-                fv = fmax(fv, 0.0);
-            } else {
-                const double up = F_hi_old[j] - f_hi_old[j];
-                const double cur = Fg - fg;
-                double common =
-                    __ldg(c + EC_C_UP) * up + __ldg(c + EC_C_CUR) * cur + __ldg(c + EC_C_F) * Fg + sg;
-                if (MODE == EMODE_EQ15_STRAG) {
-                    const double Flo = (ek > 0) ? Fn : 0.0;
-                    common += __ldg(c + EC_S_HI) * F_hi_old[j] + __ldg(c + EC_S_LO) * Flo - __ldg(c + EC_S_G) * Fg;
-                }
-                const double hi_delta = next_F[j] - next_f[j];
-                const double rhs = __ldg(c + EC_R_F) * fg + __ldg(c + EC_R_UP) * up + __ldg(c + EC_R_CUR) * cur +
-                                   __ldg(c + EC_R_FG) * Fg - __ldg(c + EC_A) * common + __ldg(c + EC_R_HI) * hi_delta;
-                fv = rhs * __ldg(c + EC_INV_COE);
-                Fv = __ldg(c + EC_F_FROM_F) * fv + __ldg(c + EC_INV_F) * common + __ldg(c + EC_F_FROM_HI) * hi_delta;
-            }
+            energy_lane_update<MODE>(c, ek, Fg, fg, sg, Fn, F_hi_old[j], f_hi_old[j], next_F[j], next_f[j], Fv, fv);
             const T Fs = static_cast<T>(Fv), fs = static_cast<T>(fv);
             if (ok[j]) {
                 a.F[ek * L + lane[j]] = Fs;

@@ -13,14 +13,14 @@
 // Shared-memory operands use the UMMA K-major no-swizzle layout: 8-row x
 // 16-byte core matrices, rows of a core matrix 16 B apart, core matrices
 // along M/N 128 B apart (SBO) and along K one M/N-extent apart (LBO).  The B
-// tiles are pre-arranged in that layout on the host (tables) and fetched
-// with cp.async.bulk (no multicast); A is converted from the fp32 state by
-// the CTA's threads.  Two pipeline stages: the MMAs of one stage overlap the
-// conversion and copy of the next.  Every mbarrier wait is bounded; on a
-// timeout the CTA records an error code, drains what it issued (bounded),
-// frees its tensor memory and returns.
+// tiles are pre-arranged in that layout on the host (tables); a pack kernel
+// writes the A tiles in it once per source evaluation; both are fetched with
+// cp.async.bulk (no multicast).  Every mbarrier wait is bounded; on a timeout
+// the CTA records an error code, drains what it issued (bounded), frees its
+// tensor memory and returns.
 
 #include "common.cuh"
+#include "async_copy.cuh"
 
 #include <cuda_bf16.h>
 
@@ -33,44 +33,6 @@ namespace {
 
 constexpr int kRows = 128;       // UMMA M: 64 positions x 2 operands
 constexpr int kPos = 64;
-constexpr uint32_t kWaitLimit = 1u << 22;
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
-
-// Bounded parity wait; false when the limit ran out.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
-    for (uint32_t i = 0; i < kWaitLimit; ++i) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.b32 %0, 1, 0, p;\n\t}"
-            : "=r"(done)
-            : "r"(smem_u32(bar)), "r"(phase)
-            : "memory");
-        if (done) return true;
-    }
-    return false;
-}
-
-__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_u32(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
-                 : "memory");
-}
-
 // K-major, no swizzle: start address, LBO (K direction), SBO (M/N direction), version 1.
 __device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
     return static_cast<uint64_t>((addr >> 4) & 0x3FFFu) | (static_cast<uint64_t>((lbo >> 4) & 0x3FFFu) << 16) |
@@ -104,40 +66,100 @@ __host__ __device__ inline size_t umma_kmajor_offset(int row, int k, int rows) {
     return (static_cast<size_t>(k >> 3) * (rows >> 3) + (row >> 3)) * 128 + (row & 7) * 16 + (k & 7) * 2;
 }
 
-struct UmmaSourceArgs {
+// ---------------------------------------------------------------------------
+// Pipelined form.  A pack kernel writes the A operand of every (group,
+// position tile, k chunk) once, already split into bf16 hi / lo and laid out
+// as the UMMA core-matrix tile (rows 0..63 max(P1, 0), rows 64..127 P2), so
+// the GEMM kernel moves both operands with plain bulk copies: one thread keeps
+// kPipe stages of A and B in flight, issues the MMAs of each stage as it lands
+// and refills a stage as soon as the MMAs that read it have completed.  The
+// other threads only wait for the final commit and run the epilogue.
+// ---------------------------------------------------------------------------
+constexpr int kPipe = 4;
+
+struct UmmaPackArgs {
     const float* P1;
     const float* P2;
+    const int* groups;
+    uint8_t* ablob;          // [n_groups][n_mt][nk][hi|lo][128 x BK bf16, core layout]
+    int nyz, NA, nk, n_mt, BK;
+};
+
+// One thread per (row, 8-value k group) of one (group, m tile, k chunk) tile.
+__global__ void __launch_bounds__(256) pack_source_operand_kernel(UmmaPackArgs a) {
+    const int per_tile = kRows * (a.BK / 8);
+    const long long idx = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;  // gridDim.y = groups
+    if (idx >= static_cast<long long>(a.n_mt) * a.nk * per_tile) return;
+    const int gz = blockIdx.y;
+    const int r8 = static_cast<int>(idx % per_tile);
+    const long long tile = idx / per_tile;  // mt * nk + kc
+    const int kc = static_cast<int>(tile % a.nk), mt = static_cast<int>(tile / a.nk);
+    const int row = r8 / (a.BK / 8), c = r8 % (a.BK / 8);
+    const int pos = mt * kPos + (row & (kPos - 1));
+    const bool is_p2 = row >= kPos;
+    const int k0 = kc * a.BK + c * 8;
+    float x[8], r[8];
+    const int g = a.groups[gz];
+    const float* __restrict__ src = (is_p2 ? a.P2 : a.P1) + (static_cast<size_t>(g) * a.nyz + pos) * a.NA;
+    const bool row_ok = pos < a.nyz;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const float v = (row_ok && k0 + q < a.NA) ? __ldg(src + k0 + q) : 0.f;
+        x[q] = is_p2 ? v : fmaxf(v, 0.f);
+        r[q] = x[q] - __bfloat162float(__float2bfloat16_rn(x[q]));
+    }
+    uint4 hi, lo;
+    hi.x = pack_bf16(x[0], x[1]);
+    hi.y = pack_bf16(x[2], x[3]);
+    hi.z = pack_bf16(x[4], x[5]);
+    hi.w = pack_bf16(x[6], x[7]);
+    lo.x = pack_bf16(r[0], r[1]);
+    lo.y = pack_bf16(r[2], r[3]);
+    lo.z = pack_bf16(r[4], r[5]);
+    lo.w = pack_bf16(r[6], r[7]);
+    const size_t a_part = static_cast<size_t>(kRows) * a.BK * 2;
+    uint8_t* base = a.ablob + ((static_cast<size_t>(gz) * a.n_mt + mt) * a.nk + kc) * 2 * a_part;
+    const size_t off = umma_kmajor_offset(row, c * 8, kRows);
+    *reinterpret_cast<uint4*>(base + off) = hi;
+    *reinterpret_cast<uint4*>(base + a_part + off) = lo;
+}
+
+struct UmmaPipeArgs {
+    const uint8_t* ablob;
     const uint8_t* bblob;    // [n_groups][n_ntiles][nk][hi|lo][N_T x BK bf16, core layout]
     const int* groups;
     float* A1;
     float* A2;
-    int* err;                // error word (0 = ok)
-    int nyz, NA, NT, nk, n_ntiles;
+    int* err;
+    int nyz, NA, NT, nk, n_ntiles, n_mt;
 };
 
 template <int BK>
-__global__ void __launch_bounds__(128, 1) source_angular_umma_kernel(UmmaSourceArgs a) {
+__global__ void __launch_bounds__(128, 1) source_angular_umma_pipe_kernel(UmmaPipeArgs a) {
     extern __shared__ __align__(1024) uint8_t smem[];
-    __shared__ __align__(8) uint64_t bar_b[2];
-    __shared__ __align__(8) uint64_t bar_mma[2];
+    __shared__ __align__(8) uint64_t bar_full[kPipe];
+    __shared__ __align__(8) uint64_t bar_mma[kPipe];
     __shared__ uint32_t tmem_base_slot;
+    __shared__ int fail_flag;
 
     const int NT = a.NT;
-    const uint32_t a_part = kRows * BK * 2;       // bytes of one A part (hi or lo)
-    const uint32_t b_part = NT * BK * 2;          // bytes of one B part
+    constexpr uint32_t a_part = kRows * BK * 2;
+    const uint32_t b_part = NT * BK * 2;
     const uint32_t stage_bytes = 2 * a_part + 2 * b_part;
     const int nt = blockIdx.x, mt = blockIdx.y, gz = blockIdx.z;
     const int g = a.groups[gz];
     const int m0 = mt * kPos, n0 = nt * NT;
     const int tid = threadIdx.x, warp = tid >> 5;
     const uint32_t ncols = NT <= 32 ? 32 : NT <= 64 ? 64 : NT <= 128 ? 128 : 256;
+    const int nk = a.nk;
 
     if (tid == 0) {
-        mbar_init(&bar_b[0], 1);
-        mbar_init(&bar_b[1], 1);
-        mbar_init(&bar_mma[0], 1);
-        mbar_init(&bar_mma[1], 1);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        for (int s = 0; s < kPipe; ++s) {
+            mbar_init(&bar_full[s], 1);
+            mbar_init(&bar_mma[s], 1);
+        }
+        mbar_init_fence();
+        fail_flag = 0;
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_slot)),
@@ -150,119 +172,84 @@ __global__ void __launch_bounds__(128, 1) source_angular_umma_kernel(UmmaSourceA
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tmem_base_slot;
 
-    // row of this thread in the A operand
-    const int row = tid;
-    const int pos = m0 + (row & (kPos - 1));
-    const bool is_p2 = row >= kPos;
-    const float* __restrict__ src = (is_p2 ? a.P2 : a.P1) + (static_cast<size_t>(g) * a.nyz + pos) * a.NA;
-    const bool row_ok = pos < a.nyz;
+    const uint8_t* __restrict__ ablob = a.ablob + (static_cast<size_t>(gz) * a.n_mt + mt) * nk * (2 * a_part);
+    const uint8_t* __restrict__ bblob =
+        a.bblob + (static_cast<size_t>(gz) * a.n_ntiles + nt) * nk * static_cast<size_t>(2 * b_part);
     const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(NT >> 3) << 17) |
                            (static_cast<uint32_t>(kRows >> 4) << 24);
-    const uint8_t* __restrict__ blob =
-        a.bblob + (static_cast<size_t>(gz) * a.n_ntiles + nt) * a.nk * static_cast<size_t>(2 * b_part);
 
-    // this thread's row for one stage: BK values, loaded one stage ahead of use
-    const bool vec = (a.NA % 4) == 0;
-    float xa[BK];
-    auto load_row = [&](int k0) {
-        if (vec && row_ok && k0 + BK <= a.NA) {
-#pragma unroll
-            for (int c = 0; c < BK / 4; ++c) {
-                const float4 v = __ldg(reinterpret_cast<const float4*>(src + k0) + c);
-                xa[4 * c] = v.x;
-                xa[4 * c + 1] = v.y;
-                xa[4 * c + 2] = v.z;
-                xa[4 * c + 3] = v.w;
-            }
-        } else {
-#pragma unroll
-            for (int q = 0; q < BK; ++q) xa[q] = (row_ok && k0 + q < a.NA) ? __ldg(src + k0 + q) : 0.f;
-        }
-    };
-    load_row(0);
-
-    bool failed = false;
-    int commits[2] = {0, 0};   // MMA commits per stage (thread 0)
-    int copies[2] = {0, 0};    // B copies issued per stage (thread 0)
-    int copies_seen[2] = {0, 0};
-    for (int it = 0; it < a.nk; ++it) {
-        const int st = it & 1;
-        uint8_t* sA = smem + st * stage_bytes;
-        uint8_t* sB = sA + 2 * a_part;
-        if (it >= 2) {  // the MMAs that read this stage two iterations ago are done
-            const bool ok = mbar_wait(&bar_mma[st], ((it - 2) >> 1) & 1);
-            if (__syncthreads_or(!ok)) {
-                failed = true;
+    if (tid == 0) {
+        int issued[kPipe] = {}, landed[kPipe] = {}, committed[kPipe] = {}, drained[kPipe] = {};
+        auto issue = [&](int it) {
+            const int st = it % kPipe;
+            uint8_t* sA = smem + st * stage_bytes;
+            mbar_expect_tx(&bar_full[st], 2 * a_part + 2 * b_part);
+            bulk_copy_g2s(sA, ablob + static_cast<size_t>(it) * 2 * a_part, 2 * a_part, &bar_full[st]);
+            bulk_copy_g2s(sA + 2 * a_part, bblob + static_cast<size_t>(it) * 2 * b_part, 2 * b_part, &bar_full[st]);
+            ++issued[st];
+        };
+        bool bad = false;
+        for (int it = 0; it < min(kPipe, nk); ++it) issue(it);
+        for (int it = 0; it < nk && !bad; ++it) {
+            const int st = it % kPipe;
+            if (!mbar_wait(&bar_full[st], (it / kPipe) & 1)) {
+                bad = true;
                 break;
             }
-        }
-        if (tid == 0) {
-            mbar_expect_tx(&bar_b[st], 2 * b_part);
-            bulk_copy_g2s(sB, blob + static_cast<size_t>(it) * 2 * b_part, 2 * b_part, &bar_b[st]);
-            ++copies[st];
-        }
-        // A: split the prefetched row into hi / lo bf16, core-matrix layout
+            ++landed[st];
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t aA = smem_u32(smem + st * stage_bytes), aB = aA + 2 * a_part;
+            constexpr uint32_t lboA = (kRows / 8) * 128;
+            const uint32_t lboB = (NT / 8) * 128;
 #pragma unroll
-        for (int c = 0; c < BK / 8; ++c) {
-            float x[8], r[8];
-#pragma unroll
-            for (int q = 0; q < 8; ++q) {
-                x[q] = is_p2 ? xa[c * 8 + q] : fmaxf(xa[c * 8 + q], 0.f);
-                r[q] = x[q] - __bfloat162float(__float2bfloat16_rn(x[q]));
+            for (int j = 0; j < BK / 16; ++j) {
+                const uint64_t ah = umma_desc(aA + j * 2 * lboA, lboA, 128);
+                const uint64_t al = umma_desc(aA + a_part + j * 2 * lboA, lboA, 128);
+                const uint64_t bh = umma_desc(aB + j * 2 * lboB, lboB, 128);
+                const uint64_t bl = umma_desc(aB + b_part + j * 2 * lboB, lboB, 128);
+                umma_bf16(tmem, ah, bh, idesc, (it > 0 || j > 0) ? 1u : 0u);
+                umma_bf16(tmem, ah, bl, idesc, 1u);
+                umma_bf16(tmem, al, bh, idesc, 1u);
             }
-            uint4 hi, lo;
-            hi.x = pack_bf16(x[0], x[1]);
-            hi.y = pack_bf16(x[2], x[3]);
-            hi.z = pack_bf16(x[4], x[5]);
-            hi.w = pack_bf16(x[6], x[7]);
-            lo.x = pack_bf16(r[0], r[1]);
-            lo.y = pack_bf16(r[2], r[3]);
-            lo.z = pack_bf16(r[4], r[5]);
-            lo.w = pack_bf16(r[6], r[7]);
-            const size_t off = umma_kmajor_offset(row, c * 8, kRows);
-            *reinterpret_cast<uint4*>(sA + off) = hi;
-            *reinterpret_cast<uint4*>(sA + a_part + off) = lo;
-        }
-        if (it + 1 < a.nk) load_row((it + 1) * BK);  // in flight while this stage's MMAs run
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-        bool bad = false;
-        if (tid == 0) {
-            if (!mbar_wait(&bar_b[st], (it >> 1) & 1)) {
-                bad = true;
-            } else {
-                ++copies_seen[st];
-                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const uint32_t aA = smem_u32(sA), aB = smem_u32(sB);
-                const uint32_t lboA = (kRows / 8) * 128, lboB = (NT / 8) * 128;
-#pragma unroll
-                for (int j = 0; j < BK / 16; ++j) {
-                    const uint64_t ah = umma_desc(aA + j * 2 * lboA, lboA, 128);
-                    const uint64_t al = umma_desc(aA + a_part + j * 2 * lboA, lboA, 128);
-                    const uint64_t bh = umma_desc(aB + j * 2 * lboB, lboB, 128);
-                    const uint64_t bl = umma_desc(aB + b_part + j * 2 * lboB, lboB, 128);
-                    umma_bf16(tmem, ah, bh, idesc, (it > 0 || j > 0) ? 1u : 0u);
-                    umma_bf16(tmem, ah, bl, idesc, 1u);
-                    umma_bf16(tmem, al, bh, idesc, 1u);
+            umma_commit(&bar_mma[st]);
+            ++committed[st];
+            // refill the stage of the previous iteration once its MMAs are done
+            // (this iteration's MMAs stay queued meanwhile)
+            const int prev = it - 1;
+            if (prev >= 0 && prev + kPipe < nk) {
+                const int ps = prev % kPipe;
+                if (!mbar_wait(&bar_mma[ps], (prev / kPipe) & 1)) {
+                    bad = true;
+                    break;
                 }
-                umma_commit(&bar_mma[st]);
-                ++commits[st];
+                ++drained[ps];
+                issue(prev + kPipe);
             }
         }
-        if (__syncthreads_or(bad)) {
-            failed = true;
-            break;
+        // the last commit covers every MMA issued before it
+        if (!bad && nk > 0) {
+            const int last = nk - 1;
+            if (!mbar_wait(&bar_mma[last % kPipe], (last / kPipe) & 1)) bad = true;
+        }
+        if (bad) {
+            atomicExch(a.err, 1);
+            // drain what was issued: the last commit and any copy not seen to land
+            for (int s = 0; s < kPipe; ++s) {
+                if (committed[s] > drained[s]) mbar_wait(&bar_mma[s], (committed[s] - 1) & 1);
+                if (issued[s] > landed[s]) mbar_wait(&bar_full[s], (issued[s] - 1) & 1);
+            }
+            fail_flag = 1;
         }
     }
-    // wait for the last commit (it covers every MMA issued before it)
-    if (!failed && a.nk > 0) {
-        const int last = a.nk - 1;
-        const bool ok = mbar_wait(&bar_mma[last & 1], (last >> 1) & 1);
-        failed = __syncthreads_or(!ok);
-    }
+    __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (!failed) {
-        float* __restrict__ dst = (is_p2 ? a.A2 : a.A1) + (static_cast<size_t>(g) * a.nyz + pos) * a.NA;
+    if (!fail_flag) {
+        // Epilogue through shared memory (the pipeline buffers are free now):
+        // each thread moves 16-column slices of its accumulator row into a
+        // [128][17]-float tile, then each warp writes whole rows so that every
+        // store instruction covers 16 consecutive outputs of one position.
+        float* tile = reinterpret_cast<float*>(smem);
+        constexpr int TS = 17;  // padded row stride: conflict-free both ways
         const uint32_t lane_base = static_cast<uint32_t>(warp * 32) << 16;
         for (int c0 = 0; c0 < NT; c0 += 16) {
             uint32_t v[16];
@@ -272,21 +259,18 @@ __global__ void __launch_bounds__(128, 1) source_angular_umma_kernel(UmmaSourceA
                   "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
                 : "r"(tmem + lane_base + c0));
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (row_ok) {
 #pragma unroll
-                for (int q = 0; q < 16; ++q) {
-                    const int n = n0 + c0 + q;
-                    if (n < a.NA) dst[n] = __uint_as_float(v[q]);
-                }
+            for (int q = 0; q < 16; ++q) tile[tid * TS + q] = __uint_as_float(v[q]);
+            __syncthreads();
+            // 128 rows x 16 columns: each warp instruction writes 2 rows x 16 columns
+            const int half = (tid & 31) >> 4, col = tid & 15;
+            const int n = n0 + c0 + col;
+            for (int r = warp * 2 + half; r < kRows; r += 8) {
+                const int pos = m0 + (r & (kPos - 1));
+                if (pos < a.nyz && n < a.NA)
+                    ((r >= kPos) ? a.A2 : a.A1)[(static_cast<size_t>(g) * a.nyz + pos) * a.NA + n] = tile[r * TS + col];
             }
-        }
-    } else if (tid == 0) {
-        atomicExch(a.err, 1);
-        // drain what this CTA issued, each wait bounded: the last commit of
-        // each stage, and any copy whose completion was not observed
-        for (int s2 = 0; s2 < 2; ++s2) {
-            if (commits[s2] > 0) mbar_wait(&bar_mma[s2], (commits[s2] - 1) & 1);
-            if (copies[s2] > copies_seen[s2]) mbar_wait(&bar_b[s2], (copies[s2] - 1) & 1);
+            __syncthreads();
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -297,21 +281,35 @@ __global__ void __launch_bounds__(128, 1) source_angular_umma_kernel(UmmaSourceA
     }
 }
 
-size_t umma_source_smem(int NT, int BK) { return 2 * (2 * static_cast<size_t>(kRows) * BK * 2 + 2 * static_cast<size_t>(NT) * BK * 2); }
+size_t umma_pack_bytes(int n_groups, int nyz, int NA, int BK) {
+    const size_t n_mt = (nyz + kPos - 1) / kPos, nk = (NA + BK - 1) / BK;
+    return static_cast<size_t>(n_groups) * n_mt * nk * 2 * kRows * BK * 2;
+}
 
-cudaError_t launch_source_angular_umma(const float* P1, const float* P2, const uint8_t* bblob, const int* groups,
-                                       int n_groups, float* A1, float* A2, int* err, int nyz, int NA, int NT, int BK,
-                                       int n_ntiles, cudaStream_t s) {
+size_t umma_pipe_smem(int NT, int BK) {
+    return static_cast<size_t>(kPipe) * (2 * static_cast<size_t>(kRows) * BK * 2 + 2 * static_cast<size_t>(NT) * BK * 2);
+}
+
+cudaError_t launch_source_angular_pipe(const float* P1, const float* P2, uint8_t* ablob, const uint8_t* bblob,
+                                       const int* groups, int n_groups, float* A1, float* A2, int* err, int nyz,
+                                       int NA, int NT, int BK, int n_ntiles, cudaStream_t s) {
     if (n_groups <= 0) return cudaSuccess;
-    if (BK != 32 || NT % 16 != 0 || NT < 16 || NT > 256) return cudaErrorInvalidValue;
-    UmmaSourceArgs a{P1, P2, bblob, groups, A1, A2, err, nyz, NA, NT, (NA + BK - 1) / BK, n_ntiles};
-    // at most two CTAs per SM when each holds 256 tensor-memory columns (512 per SM)
-    size_t smem = umma_source_smem(NT, BK);
-    if (NT > 128) smem = std::max<size_t>(smem, 80 * 1024);
-    auto kern = source_angular_umma_kernel<32>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (BK != 16 || NT % 16 != 0 || NT < 16 || NT > 256) return cudaErrorInvalidValue;
+    const int n_mt = (nyz + kPos - 1) / kPos, nk = (NA + BK - 1) / BK;
+    UmmaPackArgs p{P1, P2, groups, ablob, nyz, NA, nk, n_mt, BK};
+    const long long per_group = static_cast<long long>(n_mt) * nk * kRows * (BK / 8);
+    if ((per_group + 255) / 256 > 0x7fffffffLL || n_groups > 65535) return cudaErrorInvalidConfiguration;
+    pack_source_operand_kernel<<<dim3(static_cast<unsigned>((per_group + 255) / 256), n_groups), 256, 0, s>>>(p);
+    cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    dim3 grid(n_ntiles, (nyz + kPos - 1) / kPos, n_groups);
+    UmmaPipeArgs a{ablob, bblob, groups, A1, A2, err, nyz, NA, NT, nk, n_ntiles, n_mt};
+    size_t smem = umma_pipe_smem(NT, BK);
+    // at most two CTAs per SM when each holds 256 tensor-memory columns (512 per SM)
+    if (NT > 128) smem = std::max<size_t>(smem, 80 * 1024);
+    auto kern = source_angular_umma_pipe_kernel<16>;
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    dim3 grid(n_ntiles, n_mt, n_groups);
     if (grid.y > 65535 || grid.z > 65535) return cudaErrorInvalidConfiguration;
     kern<<<grid, kRows, smem, s>>>(a);
     return cudaGetLastError();

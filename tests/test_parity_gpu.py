@@ -60,7 +60,9 @@ def assert_states(ctx, ora, tol, which=((0, 0), (0, 1), (1, 0), (1, 1))):
 
 
 @pytest.mark.parametrize("flags", [{}, {"legacy_energy": True}, {"eq15_straggling": True},
-                                   {"legacy_energy": True, "eq15_straggling": True}])
+                                   {"legacy_energy": True, "eq15_straggling": True},
+                                   # 225 lanes: rows not a multiple of 16 bytes -> register-prefetch sweep
+                                   {"ny": 4, "nz": 4, "nmu": 3, "nom": 3, "eq15_straggling": True}])
 def test_energy_operator(flags):
     cfg = small_cfg(**flags)
     ctx, ora = build(cfg)
