@@ -101,6 +101,9 @@ struct bfpn_ctx {
     bool tr_plane_ok = false;   // a compiled whole-plane kernel exists for this plane
     bool tr_plane = false;      // use it
     int tr_plane_ac = 8;
+    bool tr_tile_ok = false;    // the plane needs tiles: the unrolled tiled kernel applies
+    bool tr_tile = false;       // use it
+    int tr_tile_ac = 8;
     int ang_slices = 4;
     int energy_block = 128;
 
@@ -338,6 +341,11 @@ void choose_plane_transport(bfpn_ctx* c) {
     c->tr_plane_ok = transport_plane_supported(c->Ny, c->Nz) &&
                      transport_plane_smem(c->Ny + 1, c->tr_plane_ac, c->elem) <= 200 * 1024;
     c->tr_plane = c->tr_plane_ok;
+    // planes the line-walk kernel would tile: the unrolled tiled kernel instead
+    // (8 float / 4 double angles per block: 78 KB of shared memory, 2 blocks per SM)
+    c->tr_tile_ac = c->elem == 4 ? 8 : 4;
+    c->tr_tile_ok = !c->tr_plane_ok && !c->tr_inplace;
+    c->tr_tile = c->tr_tile_ok;
 }
 
 bool transport_in_place(const bfpn_ctx* c) { return c->tr_plane || c->tr_inplace; }
@@ -405,6 +413,8 @@ cudaError_t enq_transport(bfpn_ctx* c, const void* in, void* out, double dt, boo
     a.preserve_sign = preserve_sign ? 1 : 0;
     if (c->tr_plane)
         return prof(c, BFPN_KERNEL_TRANSPORT, [&] { return launch_transport_plane<T>(a, c->tr_plane_ac, c->stream); });
+    if (c->tr_tile && a.in != a.out)
+        return prof(c, BFPN_KERNEL_TRANSPORT, [&] { return launch_transport_tiles<T>(a, c->tr_tile_ac, c->stream); });
     return prof(c, BFPN_KERNEL_TRANSPORT, [&] { return launch_transport<T>(a, c->tr_ac, c->stream); });
 }
 
@@ -1128,16 +1138,26 @@ bfpn_status bfpn_set_option(bfpn_ctx* c, int32_t option, int32_t value) {
             break;
         case BFPN_OPT_PLANE_TRANSPORT: {
             const bool f32 = c->elem == 4;
-            if (value != 0 && value != 1 && !(f32 ? (value == 8 || value == 16) : (value == 4 || value == 8)))
-                return fail(c, BFPN_INVALID_ARG, "plane transport: 0, 1 or an angle chunk of 8/16 (float), 4/8 (double)");
-            if (value != 0 && !c->tr_plane_ok)
-                return fail(c, BFPN_INVALID_ARG, "no whole-plane transport kernel for this plane size");
-            if (value > 1 && transport_plane_smem(c->Ny + 1, value, c->elem) > 200 * 1024)
-                return fail(c, BFPN_INVALID_ARG, "plane transport chunk needs too much shared memory");
-            if (value == 0 && !c->tr_inplace && !c->tmp)
-                return fail(c, BFPN_INVALID_ARG, "the line-walk kernel needs a buffer this context did not allocate");
-            c->tr_plane = value != 0;
-            if (value > 1) c->tr_plane_ac = value;
+            if (value != 0 && !c->tr_plane_ok && !c->tr_tile_ok)
+                return fail(c, BFPN_INVALID_ARG, "no unrolled transport kernel for this plane size");
+            if (value > 1) {
+                const bool ok = c->tr_plane_ok ? (f32 ? (value == 8 || value == 16) : (value == 4 || value == 8))
+                                               : (f32 ? (value == 4 || value == 8) : (value == 2 || value == 4));
+                if (!ok)
+                    return fail(c, BFPN_INVALID_ARG,
+                                "angle chunk: 8/16 (float) or 4/8 (double) for whole planes, 4/8 (float) or 2/4 "
+                                "(double) for tiled planes");
+                if (c->tr_plane_ok && transport_plane_smem(c->Ny + 1, value, c->elem) > 200 * 1024)
+                    return fail(c, BFPN_INVALID_ARG, "plane transport chunk needs too much shared memory");
+            }
+            if (value != 0 && value != 1 && !(value > 1)) return fail(c, BFPN_INVALID_ARG, "bad option value");
+            if (c->tr_plane_ok) {
+                c->tr_plane = value != 0;
+                if (value > 1) c->tr_plane_ac = value;
+            } else {
+                c->tr_tile = value != 0;
+                if (value > 1) c->tr_tile_ac = value;
+            }
             break;
         }
         default:

@@ -162,6 +162,10 @@ size_t transport_smem(int Ny1, int Nz1, int ty, int tz, int ac, size_t elem);
 // (transport_plane_supported); ang_chunk 8 or 16 (float), 4 or 8 (double).
 template <typename T> cudaError_t launch_transport_plane(const TransportArgs<T>& a, int ang_chunk, cudaStream_t s);
 bool transport_plane_supported(int Ny, int Nz);
+// Any plane, in 27 x 27 output tiles with a 4-cell halo, out of place;
+// ang_chunk 4 or 8 (float), 2 or 4 (double).
+template <typename T> cudaError_t launch_transport_tiles(const TransportArgs<T>& a, int ang_chunk, cudaStream_t s);
+size_t transport_tile_smem(int R, int ac, size_t elem);
 size_t transport_plane_smem(int NP, int ac, size_t elem);
 
 int energy_grid(long long lanes, int block);

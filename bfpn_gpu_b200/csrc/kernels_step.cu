@@ -607,6 +607,170 @@ static cudaError_t launch_plane_np(const TransportArgs<T>& a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// Large planes: the same unrolled walks over R x R regions, R = TT + 8.
+// Block = (group, AC angles, one TT x TT output tile); its region is the tile
+// plus a 4-cell halo, loaded with indices clamped to the plane, so cells
+// outside the plane repeat the edge value -- exactly what the reference's
+// clamped stencil indices read (the slope of a repeated triple is 0).  Every
+// walk treats the region ends as line ends; that is wrong only within 2 cells
+// of a region end that is not a plane edge, and the halo keeps those cells
+// out of what the tile needs.  The predictor at out-of-plane cells is then
+// replaced by its clamped in-plane value (the reference's stage 2 clamps its
+// indices into P as well).  Output goes to a separate array (neighbouring
+// tiles read this tile's input as their halo).
+// ---------------------------------------------------------------------------
+template <typename T, int R, int AC>
+__global__ void __launch_bounds__((R * AC + 31) / 32 * 32) transport_tile_kernel(TransportArgs<T> a, int tiles_y,
+                                                                                  int tiles_z, int n_chunks) {
+    constexpr int TT = R - 8, N = R - 1, RP = R | 1, RS = RP * AC, PL = R * RS;
+    constexpr int NT = (R * AC + 31) / 32 * 32;  // == blockDim.x
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* Fs = reinterpret_cast<T*>(smem_raw);
+    T* Ps = Fs + PL;
+    int b = blockIdx.x;
+    const int tyi = b % tiles_y;
+    b /= tiles_y;
+    const int tzi = b % tiles_z;
+    b /= tiles_z;
+    const int chunk = b % n_chunks, ek = b / n_chunks;
+    const int Ny = a.Ny, Nz = a.Nz, Ny1 = Ny + 1, NA = a.NA, a0 = chunk * AC;
+    const int ry0 = tyi * TT - 4, rz0 = tzi * TT - 4;  // region origin (plane coordinates)
+    const size_t plane = static_cast<size_t>(ek) * Ny1 * (Nz + 1) * NA + a0;
+    const T* __restrict__ in = a.in + plane;
+    T* __restrict__ out = a.out + plane;
+    const int q = threadIdx.x % AC, line = threadIdx.x / AC;
+    const bool qok = a0 + q < NA;
+    const int ang = min(a0 + q, NA - 1);
+    const T wy = a.omega[2 * ang], wz = a.omega[2 * ang + 1];
+    const T wry = wy / a.dy, wrz = wz / a.dz;
+    const bool dny = wy < T(0), dnz = wz < T(0);
+    const T hy = dny ? T(-0.5) : T(0.5), hz = dnz ? T(-0.5) : T(0.5);
+    const int sy = dny ? 1 : 0, sz = dnz ? 1 : 0;
+    const T dt = a.dt, hdt = T(0.5) * a.dt;
+    const T lo = a.preserve_sign ? -INFINITY : T(0);
+
+    if (AC % Vec16<T>::W == 0 && NA % Vec16<T>::W == 0) {
+        using V = typename Vec16<T>::type;
+        constexpr int W = Vec16<T>::W, NV = R * R * AC / W;
+#pragma unroll 4
+        for (int v = threadIdx.x; v < NV; v += NT) {
+            const int e = v * W, aa = e % AC, p = e / AC;
+            const int lz = p / R, ly = p - lz * R;
+            const int gy = min(max(ry0 + ly, 0), Ny), gz = min(max(rz0 + lz, 0), Nz);
+            V val{};
+            if (a0 + aa < NA) val = *reinterpret_cast<const V*>(in + (static_cast<size_t>(gz) * Ny1 + gy) * NA + aa);
+            *reinterpret_cast<V*>(Fs + lz * RS + ly * AC + aa) = val;
+        }
+    } else {
+#pragma unroll 4
+        for (int e = threadIdx.x; e < R * R * AC; e += NT) {
+            const int aa = e % AC, p = e / AC;
+            const int lz = p / R, ly = p - lz * R;
+            const int gy = min(max(ry0 + ly, 0), Ny), gz = min(max(rz0 + lz, 0), Nz);
+            Fs[lz * RS + ly * AC + aa] = (a0 + aa < NA) ? in[(static_cast<size_t>(gz) * Ny1 + gy) * NA + aa] : T(0);
+        }
+    }
+    __syncthreads();
+    const bool act = line < R;
+    // stage 1, y-part of div F (region rows) into Ps
+    if (act) {
+        const T* X = Fs + line * RS + q;
+        T* D = Ps + line * RS + q - sy * AC;
+        walk_plane_line<T, N, AC>(X, wry, hy, [&](int j, T d, T, T) { D[j * AC] = d; });
+        Ps[line * RS + q + sy * N * AC] = T(0);
+    }
+    __syncthreads();
+    // stage 1, z-part (region columns): predictor into Ps, H over F
+    if (act) {
+        T* Xc = Fs + line * AC + q;
+        T* Pc = Ps + line * AC + q;
+        T* Xe = Xc - sz * RS;
+        T* Pe = Pc - sz * RS;
+        walk_plane_line<T, N, RS>(Xc, wrz, hz, [&](int j, T dz, T xj, T xjm1) {
+            const T f = dnz ? xjm1 : xj;
+            const T d = Pe[j * RS] + dz;
+            Pe[j * RS] = max(f - dt * d, lo);
+            Xe[j * RS] = f - hdt * d;
+        });
+        const int cb = sz * N * RS;
+        const T f = Xc[cb], d = Pc[cb];
+        Pc[cb] = max(f - dt * d, lo);
+        Xc[cb] = f - hdt * d;
+    }
+    __syncthreads();
+    // the predictor outside the plane repeats its clamped in-plane value
+    const bool edge = ry0 < 0 || rz0 < 0 || ry0 + R > Ny1 || rz0 + R > Nz + 1;
+    if (edge) {
+        for (int e = threadIdx.x; e < R * R * AC; e += NT) {
+            const int aa = e % AC, p = e / AC;
+            const int lz = p / R, ly = p - lz * R;
+            const int cy = min(max(ry0 + ly, 0), Ny) - ry0, cz = min(max(rz0 + lz, 0), Nz) - rz0;
+            if (cy != ly || cz != lz) Ps[lz * RS + ly * AC + aa] = Ps[cz * RS + cy * AC + aa];
+        }
+        __syncthreads();
+    }
+    // stage 2, y-part of div P on the tile's rows: H - dt/2 d_y P over F
+    if (line < TT) {
+        const int lz = line + 4;
+        const T* X = Ps + lz * RS + q;
+        T* Fe = Fs + lz * RS + q - sy * AC;
+        walk_plane_line<T, N, AC>(X, wry, hy, [&](int j, T d, T, T) { Fe[j * AC] -= hdt * d; });
+    }
+    __syncthreads();
+    // stage 2, z-part on the tile's columns and the corrector, to global
+    const int gy = ry0 + 4 + line;
+    if (line < TT && gy <= Ny) {
+        const int ly = line + 4;
+        const T* X = Ps + ly * AC + q;
+        const T* Fc = Fs + ly * AC + q;
+        const T* Fe = Fc - sz * RS;
+        const size_t zs = static_cast<size_t>(Ny1) * NA;
+        T* o = out + static_cast<size_t>(gy) * NA + q;  // + gz * zs
+        const int gz_lo = rz0 + 4, gz_hi = min(rz0 + 4 + TT, Nz + 1);  // output rows of this tile
+        walk_plane_line<T, N, RS>(X, wrz, hz, [&](int j, T d, T, T) {
+            const int lz = j - sz, gz = rz0 + lz;
+            if (qok && gz >= gz_lo && gz < gz_hi) o[static_cast<size_t>(gz) * zs] = max(Fe[j * RS] - hdt * d, lo);
+        });
+        const int lzb = sz * N, gzb = rz0 + lzb;  // the cell whose z-part is 0
+        if (qok && gzb >= gz_lo && gzb < gz_hi) o[static_cast<size_t>(gzb) * zs] = max(Fc[lzb * RS], lo);
+    }
+}
+
+size_t transport_tile_smem(int R, int ac, size_t elem) {
+    return 2 * static_cast<size_t>(R) * (R | 1) * ac * elem;
+}
+
+constexpr int kTileRegion = 35;  // 27 x 27 output tiles
+
+template <typename T, int AC>
+static cudaError_t launch_tile_ac(const TransportArgs<T>& a, cudaStream_t s) {
+    constexpr int R = kTileRegion, TT = R - 8;
+    const int tiles_y = (a.Ny + 1 + TT - 1) / TT, tiles_z = (a.Nz + 1 + TT - 1) / TT;
+    const int n_chunks = (a.NA + AC - 1) / AC;
+    const size_t smem = transport_tile_smem(R, AC, sizeof(T));
+    auto kern = transport_tile_kernel<T, R, AC>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    const long long blocks = static_cast<long long>(a.Ng) * n_chunks * tiles_y * tiles_z;
+    if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+    kern<<<static_cast<unsigned>(blocks), (R * AC + 31) / 32 * 32, smem, s>>>(a, tiles_y, tiles_z, n_chunks);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_transport_tiles(const TransportArgs<T>& a, int ang_chunk, cudaStream_t s) {
+    if (a.in == a.out) return cudaErrorInvalidValue;  // tiles read neighbours' input as halo
+    if constexpr (sizeof(T) == 4) {
+        if (ang_chunk == 4) return launch_tile_ac<T, 4>(a, s);
+        if (ang_chunk == 8) return launch_tile_ac<T, 8>(a, s);
+    } else {
+        if (ang_chunk == 2) return launch_tile_ac<T, 2>(a, s);
+        if (ang_chunk == 4) return launch_tile_ac<T, 4>(a, s);
+    }
+    return cudaErrorInvalidValue;
+}
+
 // Plane sizes (Ny+1 = Nz+1) with a compiled whole-plane kernel.
 #define BFPN_PLANE_SIZES(X) X(5) X(7) X(9) X(11) X(13) X(15) X(17) X(21) X(25) X(33)
 
@@ -1116,6 +1280,7 @@ cudaError_t launch_convert(const Tin* in, Tout* out, long long n, cudaStream_t s
                                                int, int, double*, cudaStream_t);                                  \
     template cudaError_t launch_transport<T>(const TransportArgs<T>&, int, cudaStream_t);                         \
     template cudaError_t launch_transport_plane<T>(const TransportArgs<T>&, int, cudaStream_t);                   \
+    template cudaError_t launch_transport_tiles<T>(const TransportArgs<T>&, int, cudaStream_t);                   \
     template cudaError_t launch_angle<T>(const AngleArgs<T>&, cudaStream_t);                                      \
     template cudaError_t launch_idd_partials<T>(const T*, const T*, const double*, int, long long, int, int, int,  \
                                                 int, int, double*, int, cudaStream_t);                            \

@@ -241,11 +241,12 @@ int32_t bfpn_source_groups(bfpn_ctx* ctx);
  *   contraction on the tcgen05 tensor cores in mixed precision (split-bf16
  *   operands, fp32 accumulation); 0 uses the fp32 CUDA-core kernel.
  * BFPN_OPT_CUDA_GRAPHS: 1 (default) replays each depth step as a CUDA graph.
- * BFPN_OPT_PLANE_TRANSPORT: 1 (default where compiled: square planes with
- *   Ny = Nz in {4,6,8,10,12,14,16,20,24,32}) runs the transport with the
- *   unrolled whole-plane kernel; 0 uses the general line-walk kernel; 8 or 16
- *   (mixed) / 4 or 8 (FP64) selects the whole-plane kernel with that many
- *   angles per block.  Both kernels compute the same values. */
+ * BFPN_OPT_PLANE_TRANSPORT: 1 (default) runs the transport with the unrolled
+ *   kernels: one block per whole plane for square planes with
+ *   Ny = Nz in {4,6,8,10,12,14,16,20,24,32}, 27 x 27 tiles for planes too large
+ *   for one block; 0 uses the general line-walk kernel; a larger value selects
+ *   the angles per block (whole planes: 8 or 16 mixed, 4 or 8 FP64; tiles: 4 or
+ *   8 mixed, 2 or 4 FP64).  All compute the same values. */
 enum { BFPN_OPT_TENSOR_CORES = 0, BFPN_OPT_CUDA_GRAPHS = 1, BFPN_OPT_PLANE_TRANSPORT = 2 };
 bfpn_status bfpn_set_option(bfpn_ctx* ctx, int32_t option, int32_t value);
 

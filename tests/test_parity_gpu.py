@@ -119,6 +119,41 @@ def test_plane_transport_operator(preserve, n, ang):
         assert_states(ctx, ora, OP_TOL, ((0, 0), (1, 1)))
 
 
+@pytest.mark.parametrize("preserve", [False, True])
+@pytest.mark.parametrize("ny,nz", [(40, 33), (60, 26), (27, 54)])
+def test_tiled_transport_operator(preserve, ny, nz):
+    """Planes too large for one block: the unrolled 27 x 27 tile kernel (whole,
+    partial and one-cell tiles, both angle chunks) and the line-walk tiles,
+    against the oracle."""
+    cfg = small_cfg(ny=ny, nz=nz, nmu=3, nom=2, ng=3, ly=4.0, lz=3.0)
+    ctx, ora = build(cfg)
+    states = seeded_states(ctx, 8)
+    for opt in (1, 2, 0):  # unrolled tiles (4 angles per block), unrolled tiles (2), line walks
+        ctx.set_option(capi.OPT_PLANE_TRANSPORT, opt)
+        set_both(ctx, ora, states)
+        for sp, cf in ((0, 0), (1, 1)):
+            ctx.transport(sp, cf, 0.5 * cfg.dt(), preserve)
+            ora.transport(sp, cf, 0.5 * cfg.dt(), preserve)
+        assert_states(ctx, ora, OP_TOL, ((0, 0), (1, 1)))
+
+
+def test_tiled_transport_mixed_matches_line_walks():
+    cfg = small_cfg(ny=80, nz=80, nmu=4, nom=4, ng=2, ly=16.0, lz=16.0)
+    ctx, _ = build(cfg, precision=capi.PREC_MIXED)
+    states = seeded_states(ctx, 9)
+    out = {}
+    for opt in (1, 4, 0):
+        ctx.set_option(capi.OPT_PLANE_TRANSPORT, opt)
+        for k, arr in enumerate(states):
+            ctx.set_state(k // 2, k % 2, arr)
+        ctx.transport(0, 0, 0.5 * cfg.dt(), False)
+        ctx.transport(0, 1, 0.5 * cfg.dt(), True)
+        out[opt] = (ctx.get_state(0, 0), ctx.get_state(0, 1))
+    for opt in (1, 4):
+        for a, b in zip(out[opt], out[0]):
+            assert rel_err(a, b) < 2e-6
+
+
 def test_plane_transport_mixed_matches_line_walks():
     cfg = small_cfg(ny=20, nz=20, nmu=6, nom=7, ng=5, lz=2.0)
     ctx, _ = build(cfg, precision=capi.PREC_MIXED)
