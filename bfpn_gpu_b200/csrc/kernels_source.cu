@@ -99,6 +99,82 @@ cudaError_t launch_source_angular(const SourceArgs<T>& a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+// Float state: the same contraction on packed fp32x2 FMAs.  Accumulators
+// pair neighbouring output groups of one lane, so one instruction applies the
+// coefficients of outputs (2t, 2t+1) -- one 8-byte piece of a shared-memory
+// row -- to the lane's value held twice.  Products and sums are the scalar
+// kernel's, output by output.
+template <int TE, int LN>
+__global__ void __launch_bounds__(128) source_energy_f2_kernel(SourceArgs<float> a) {
+    constexpr int SC = 32, TP = TE / 2;
+    __shared__ __align__(16) float E1[SC][TE];
+    __shared__ __align__(16) float E2[SC][TE];
+    const int tile = blockIdx.x;
+    const long long per_e = static_cast<long long>(a.nyz) * a.NA;
+    const long long l0 = static_cast<long long>(blockIdx.y) * blockDim.x * LN + threadIdx.x;
+    const int Ng = a.Ng, e0 = tile * TE;
+    const int lo = a.tile_lo[tile], hi = a.tile_hi[tile];
+    float2 q1[TP][LN], q2[TP][LN];
+#pragma unroll
+    for (int t = 0; t < TP; ++t)
+#pragma unroll
+        for (int j = 0; j < LN; ++j) q1[t][j] = q2[t][j] = make_float2(0.f, 0.f);
+    long long lj[LN];
+    bool ok[LN];
+#pragma unroll
+    for (int j = 0; j < LN; ++j) {
+        lj[j] = l0 + static_cast<long long>(j) * blockDim.x;
+        ok[j] = lj[j] < per_e;
+    }
+    for (int s0 = lo; s0 < hi; s0 += SC) {
+        const int n = min(SC, hi - s0);
+        __syncthreads();
+        for (int k = threadIdx.x; k < SC * TE; k += blockDim.x) {
+            const int ss = k / TE, t = k - ss * TE, e = e0 + t;
+            const bool in = ss < n && e < Ng;
+            E1[ss][t] = in ? static_cast<float>(a.e1[static_cast<size_t>(e) * Ng + s0 + ss]) : 0.f;
+            E2[ss][t] = in ? static_cast<float>(a.e2[static_cast<size_t>(e) * Ng + s0 + ss]) : 0.f;
+        }
+        __syncthreads();
+#pragma unroll 2
+        for (int ss = 0; ss < n; ++ss) {
+            const long long row = static_cast<long long>(s0 + ss) * per_e;
+            float2 x1[LN], x2[LN];
+#pragma unroll
+            for (int j = 0; j < LN; ++j) {
+                const float v1 = ok[j] ? a.A1[row + lj[j]] : 0.f, v2 = ok[j] ? a.A2[row + lj[j]] : 0.f;
+                x1[j] = make_float2(v1, v1);
+                x2[j] = make_float2(v2, v2);
+            }
+            const float2* c1 = reinterpret_cast<const float2*>(E1[ss]);
+            const float2* c2 = reinterpret_cast<const float2*>(E2[ss]);
+#pragma unroll
+            for (int t = 0; t < TP; ++t) {
+                const float2 a1 = c1[t], a2 = c2[t];
+#pragma unroll
+                for (int j = 0; j < LN; ++j) {
+                    q1[t][j] = __ffma2_rn(a1, x1[j], q1[t][j]);
+                    q2[t][j] = __ffma2_rn(a2, x2[j], q2[t][j]);
+                }
+            }
+        }
+    }
+    const float dg = static_cast<float>(a.dg), third = 1.f / 3.f;
+#pragma unroll
+    for (int t = 0; t < TP; ++t)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int e = e0 + 2 * t + h;
+            if (e >= Ng) continue;
+#pragma unroll
+            for (int j = 0; j < LN; ++j)
+                if (ok[j]) {
+                    const float s1 = h ? q1[t][j].y : q1[t][j].x, s2 = h ? q2[t][j].y : q2[t][j].x;
+                    a.S[e * per_e + lj[j]] = dg * (s1 + s2 * third);
+                }
+        }
+}
+
 // Energy stage: TE output groups per block and LN lanes per thread.  The
 // source groups of the union band of the TE outputs are streamed once; the
 // band coefficients of a chunk of SC source groups are staged in shared
@@ -177,10 +253,18 @@ cudaError_t launch_source_energy(const SourceArgs<T>& a, int tile_e, cudaStream_
     const long long ly = (per_e + 128 * LN - 1) / (128 * LN);
     if (ly > 65535) return cudaErrorInvalidConfiguration;
     dim3 grid(tiles, static_cast<unsigned>(ly));
-    switch (tile_e) {
-        case 8: source_energy_kernel<T, 8, LN><<<grid, 128, 0, s>>>(a); break;
-        case 16: source_energy_kernel<T, 16, LN><<<grid, 128, 0, s>>>(a); break;
-        default: return cudaErrorInvalidValue;
+    if constexpr (sizeof(T) == 4) {
+        switch (tile_e) {
+            case 8: source_energy_f2_kernel<8, LN><<<grid, 128, 0, s>>>(a); break;
+            case 16: source_energy_f2_kernel<16, LN><<<grid, 128, 0, s>>>(a); break;
+            default: return cudaErrorInvalidValue;
+        }
+    } else {
+        switch (tile_e) {
+            case 8: source_energy_kernel<T, 8, LN><<<grid, 128, 0, s>>>(a); break;
+            case 16: source_energy_kernel<T, 16, LN><<<grid, 128, 0, s>>>(a); break;
+            default: return cudaErrorInvalidValue;
+        }
     }
     return cudaGetLastError();
 }

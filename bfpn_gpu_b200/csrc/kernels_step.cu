@@ -68,9 +68,9 @@ __device__ __forceinline__ void energy_lane_update(const double* __restrict__ c,
     }
 }
 
-template <int MODE, typename T, int LPT>
-__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 5 : 4) energy_kernel(EnergyArgs<T> a) {
-    constexpr int D = 4;  // groups prefetched ahead of use
+template <int MODE, typename T, int LPT, int D = 4, int NTH = 128, int MINB = (sizeof(T) == 4 ? 5 : 4)>
+__global__ void __launch_bounds__(NTH, MINB) energy_kernel(EnergyArgs<T> a) {
+    // D: groups prefetched ahead of use
     const long long L = a.lanes;
     const int Ng = a.Ng;
     long long lane[LPT];
