@@ -176,9 +176,9 @@ def kernel_bytes(cls, cells, elem, n_groups, nyz, NA):
 # the same kernels on this workload with 250 groups (profiles/*_water230_ng250.txt), mixed
 # precision; traffic grows in proportion to the cells, so a full launch is this times cells.
 NCU_DRAM_BYTES_PER_CELL = {
-    "transport": (176.44e6 + 123.78e6) / 44.1e6,
-    "angle": (176.84e6 + 116.88e6) / 44.1e6,
-    "energy": (352.91e6 + 295.51e6) / 44.1e6,
+    "transport": (176.44e6 + 122.67e6) / 44.1e6,
+    "angle": (176.83e6 + 118.22e6) / 44.1e6,
+    "energy": (352.90e6 + 295.08e6) / 44.1e6,
     "source_angular": (286.05e6 + 155.84e6) / 44.1e6,
     "source_energy": (221.78e6 + 146.64e6) / 44.1e6,
 }
