@@ -48,8 +48,9 @@ struct bfpn_ctx {
     void* st[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
     void* tmp = nullptr;       // out-of-place transport target (tiled planes only)
     void* src = nullptr;       // secondary source
-    void* A1 = nullptr;        // angular contractions of the primary
-    void* A2 = nullptr;
+    void* A1 = nullptr;        // angular contractions of the primary (one block of a_bytes; A2 inside it,
+    void* A2 = nullptr;        // or the whole block in the tensor-core operand layout)
+    size_t a_bytes = 0;
     double* ecoef_half = nullptr;   // energy constants for dt/2
     double* ecoef_op = nullptr;     // energy constants for a per-operator dt
     double ecoef_op_dt = -1.0;
@@ -80,6 +81,10 @@ struct bfpn_ctx {
     int* dev_err = nullptr;         // device error word (bounded waits that ran out)
     void* bblob = nullptr;          // split-bf16 angular kernel tiles for the tensor-core source
     void* ablob = nullptr;          // packed split-bf16 A operand (pipelined tensor-core source)
+    void* eblob = nullptr;          // split-bf16 energy coefficient tiles (tensor-core source)
+    int* ework = nullptr;           // energy work items {chunk, column, columns, e group}
+    int* ework_begin = nullptr;     // [e tiles + 1]
+    int e_et = 0, e_emax = 0;
     bool use_umma = true;
     int umma_nt = 0, umma_bk = 16, umma_ntiles = 0;
     double* scalar_out = nullptr;   // [2] one-off IDD / proxy
@@ -198,7 +203,8 @@ uint64_t footprint(const bfpn_grid& g, int prec, bool lite) {
     b += 4 * arr;   // F, f, F1, f1
     b += arr;       // transport target
     b += arr;       // source
-    b += 2 * arr;   // angular contractions
+    b += prec == BFPN_PREC_MIXED ? std::max<uint64_t>(2 * arr, umma_q_bytes(L.per_e, g.Ng))
+                                 : 2 * arr;  // angular contractions
     b += static_cast<uint64_t>(g.Ng) * NA * NA * L.elem;           // ker_v
     b += 2 * static_cast<uint64_t>(g.Ng) * g.Ng * sizeof(double);  // e1, e2
     b += 2 * static_cast<uint64_t>(g.Ng) * NA * L.elem;            // angle factors
@@ -453,16 +459,24 @@ cudaError_t enq_source(bfpn_ctx* c) {
     a.NA = c->NA;
     a.dg = c->d.dg;
     cudaError_t e;
-    if (sizeof(T) == sizeof(float) && c->use_umma && c->bblob && c->ablob) {
+    if (sizeof(T) == sizeof(float) && c->use_umma && c->bblob && c->ablob && c->eblob) {
+        // tensor cores: the angular stage writes the energy stage's split-bf16
+        // operand into the A block, the energy stage reads it
+        uint8_t* q = static_cast<uint8_t*>(c->A1);
         e = prof(c, BFPN_KERNEL_SOURCE_ANGULAR, [&] {
             return launch_source_angular_pipe(as<const float>(c->st[0][0]), as<const float>(c->st[0][1]),
                                               static_cast<uint8_t*>(c->ablob), static_cast<const uint8_t*>(c->bblob),
-                                              c->groups, c->n_groups, as<float>(c->A1), as<float>(c->A2), c->dev_err,
-                                              c->nyz, c->NA, c->umma_nt, c->umma_bk, c->umma_ntiles, c->stream);
+                                              c->groups, c->n_groups, q, c->Ng, c->dev_err, c->nyz, c->NA,
+                                              c->umma_nt, c->umma_bk, c->umma_ntiles, c->stream);
         });
-    } else {
-        e = prof(c, BFPN_KERNEL_SOURCE_ANGULAR, [&] { return launch_source_angular<T>(a, c->stream); });
+        if (e != cudaSuccess) return e;
+        return prof(c, BFPN_KERNEL_SOURCE_ENERGY, [&] {
+            return launch_source_energy_umma(q, static_cast<const uint8_t*>(c->eblob), c->ework, c->ework_begin,
+                                             c->e_et, c->e_emax, as<float>(c->src), c->dev_err, c->per_e, c->Ng,
+                                             c->stream);
+        });
     }
+    e = prof(c, BFPN_KERNEL_SOURCE_ANGULAR, [&] { return launch_source_angular<T>(a, c->stream); });
     if (e != cudaSuccess) return e;
     return prof(c, BFPN_KERNEL_SOURCE_ENERGY, [&] { return launch_source_energy<T>(a, c->tile_e, c->stream); });
 }
@@ -836,8 +850,11 @@ bfpn_status bfpn_create(const bfpn_grid* grid, const bfpn_phys* phys, int precis
     const bool need_secondary = !c->lite && !(phys->flags & (BFPN_FLAG_PRIMARY_ONLY | BFPN_FLAG_ENERGY_ONLY));
     if (need_secondary) {
         ALLOC(c->src, arr);
-        ALLOC(c->A1, arr);
-        ALLOC(c->A2, arr);
+        // A1 and A2 for the CUDA-core source; the same block holds the
+        // tensor-core source's split-bf16 operand
+        c->a_bytes = c->prec == BFPN_PREC_MIXED ? std::max(2 * arr, umma_q_bytes(c->per_e, c->Ng)) : 2 * arr;
+        ALLOC(c->A1, c->a_bytes);
+        c->A2 = static_cast<char*>(c->A1) + arr;
     } else {
         ALLOC(c->src, c->elem);
     }
@@ -871,8 +888,7 @@ bfpn_status bfpn_create(const bfpn_grid* grid, const bfpn_phys* phys, int precis
     ALLOC(c->lite_coef, 2 * static_cast<size_t>(c->Ng) * sizeof(double));
 #undef ALLOC
     if (need_secondary) {
-        if (cudaMemsetAsync(c->A1, 0, arr, c->stream) != cudaSuccess ||
-            cudaMemsetAsync(c->A2, 0, arr, c->stream) != cudaSuccess ||
+        if (cudaMemsetAsync(c->A1, 0, c->a_bytes, c->stream) != cudaSuccess ||
             cudaMemsetAsync(c->src, 0, arr, c->stream) != cudaSuccess) {
             c->err = "memset failed";
             return bail(BFPN_CUDA_ERROR);
@@ -946,6 +962,12 @@ bfpn_status bfpn_load_tables(bfpn_ctx* c, const double* mu, int32_t mu_rows, con
     }
     dfree(c, c->ablob);
     dfree(c, c->bblob);
+    dfree(c, c->eblob);
+    { void* w = c->ework; dfree(c, w); c->ework = nullptr; }
+    { void* w = c->ework_begin; dfree(c, w); c->ework_begin = nullptr; }
+    // rows of groups without an angular kernel are read as zeros; an earlier
+    // beam's tables may have had a kernel there
+    if (c->A1) CUDA_TRY(c, cudaMemsetAsync(c->A1, 0, c->a_bytes, c->stream));
     if (c->prec == BFPN_PREC_MIXED && c->A1 && !groups.empty()) {
         // tensor-core source: output tiles of <= 256 columns, multiples of 16
         c->umma_ntiles = (c->NA + 255) / 256;
@@ -965,6 +987,23 @@ bfpn_status bfpn_load_tables(bfpn_ctx* c, const double* mu, int32_t mu_rows, con
         if ((s = upload_f64(c, d, blob.data(), blob.size())) != BFPN_OK) return s;
         CUDA_TRY(c, cudaStreamSynchronize(c->stream));
         c->bblob = d;
+        // energy stage: banded coefficient tiles and per-output-tile work lists
+        std::vector<uint8_t> eb;
+        std::vector<int> work, begin;
+        build_energy_umma(T.ker_e1.data(), T.ker_e2.data(), T.band_begin.data(), T.band_end.data(), c->Ng, c->d.dg,
+                          eb, work, begin, c->e_emax);
+        c->e_et = static_cast<int>(begin.size()) - 1;
+        void *de = nullptr, *dw = nullptr, *db = nullptr;
+        if ((s = dalloc(c, &de, eb.size())) != BFPN_OK) return s;
+        c->eblob = de;
+        if ((s = upload_f64(c, de, eb.data(), eb.size())) != BFPN_OK) return s;
+        if ((s = dalloc(c, &dw, std::max<size_t>(16, work.size() * sizeof(int)))) != BFPN_OK) return s;
+        c->ework = static_cast<int*>(dw);
+        if (!work.empty() && (s = upload_f64(c, dw, work.data(), work.size() * sizeof(int))) != BFPN_OK) return s;
+        if ((s = dalloc(c, &db, begin.size() * sizeof(int))) != BFPN_OK) return s;
+        c->ework_begin = static_cast<int*>(db);
+        if ((s = upload_f64(c, db, begin.data(), begin.size() * sizeof(int))) != BFPN_OK) return s;
+        CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     }
     const int tiles = (c->Ng + c->tile_e - 1) / c->tile_e;
     std::vector<int> lo(tiles, 0), hi(tiles, 0);
@@ -1131,6 +1170,12 @@ bfpn_status bfpn_set_option(bfpn_ctx* c, int32_t option, int32_t value) {
     if (!c) return BFPN_INVALID_ARG;
     switch (option) {
         case BFPN_OPT_TENSOR_CORES:
+            if (c->use_umma != (value != 0) && c->A1) {
+                // the two source paths keep different layouts in the A block,
+                // and both read the rows the other path wrote as zeros
+                CUDA_TRY(c, cudaMemsetAsync(c->A1, 0, c->a_bytes, c->stream));
+                CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+            }
             c->use_umma = value != 0;
             break;
         case BFPN_OPT_CUDA_GRAPHS:

@@ -147,10 +147,26 @@ cudaError_t launch_spot_plane(const T* F, const T* f, const T* F1, const T* f1, 
 // (kernels_umma.cu): pack the A operand into ablob (umma_pack_bytes), then a
 // bulk-copy-fed GEMM; bblob from build_umma_blob with BK = 16; err receives a
 // non-zero code if a CTA's bounded wait ran out.
+// The epilogue writes A1 / A2 split into bf16 hi / lo into q (umma_q_bytes,
+// the energy stage's operand layout); rows of groups it does not write must
+// be zero.
 cudaError_t launch_source_angular_pipe(const float* P1, const float* P2, uint8_t* ablob, const uint8_t* bblob,
-                                       const int* groups, int n_groups, float* A1, float* A2, int* err, int nyz,
+                                       const int* groups, int n_groups, uint8_t* q, int Ng, int* err, int nyz,
                                        int NA, int NT, int BK, int n_ntiles, cudaStream_t s);
 size_t umma_pack_bytes(int n_groups, int nyz, int NA, int BK);
+size_t umma_q_bytes(long long per_e, int Ng);
+// Tensor-core energy stage: S[e][l] from q with the coefficient tiles and
+// work lists of build_energy_umma (n_et = ceil(Ng / 256) output tiles).
+cudaError_t launch_source_energy_umma(const uint8_t* q, const uint8_t* eblob, const int* work, const int* work_begin,
+                                      int n_et, int emax_cols, float* S, int* err, long long per_e, int Ng,
+                                      cudaStream_t s);
+size_t energy_umma_smem(int emax_cols);
+// Host: split-bf16 tiles of dg e1 and dg e2 / 3 over the bands, work items
+// {chunk, first column, columns, first e group} per 256-group output tile
+// (begin = offsets, in items), and the widest item.
+void build_energy_umma(const double* e1, const double* e2, const int* band_begin, const int* band_end, int Ng,
+                       double dg, std::vector<uint8_t>& blob, std::vector<int>& work, std::vector<int>& begin,
+                       int& emax_cols);
 // Host: split-bf16 B tiles of ker_v ([Ng][NA][NA] double) for the listed
 // groups, in the kernel's shared-memory layout.
 void build_umma_blob(const double* ker_v, const int* groups, int n_groups, int NA, int NT, int BK,

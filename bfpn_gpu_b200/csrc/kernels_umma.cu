@@ -1,23 +1,34 @@
-// Tensor-core (tcgen05 / UMMA) angular contraction of the catastrophic
-// source, mixed precision:
+// Tensor-core (tcgen05 / UMMA) catastrophic source, mixed precision, in two
+// contractions (secondarySourceFromPrimaryKernel, energy_solver.cu:287-333,
+// factorised):
 //
-//   A1[g, pos, out] = sum_in max(P1[g, pos, in], 0) * ker_v[g, in, out]
-//   A2[g, pos, out] = sum_in P2[g, pos, in]         * ker_v[g, in, out]
+//   angular:  A1[s, pos, out] = sum_in max(P1[s, pos, in], 0) * ker_v[s, in, out]
+//             A2[s, pos, out] = sum_in P2[s, pos, in]         * ker_v[s, in, out]
+//   energy:   S[e, l] = sum_{s in band(e)} (dg e1[e, s]) A1[s, l] + (dg e2[e, s] / 3) A2[s, l]
 //
-// One CTA computes a 64-position x N_T-output tile of one source group for
-// both operands at once: UMMA rows 0..63 hold max(P1, 0), rows 64..127 hold
-// P2 of the same positions, and they share the B operand (ker_v).  Operands
-// are split into bf16 hi + lo parts; D += Ah Bh + Ah Bl + Al Bh accumulates
-// in fp32 in tensor memory (relative error ~2^-16 per product).
+// with l = pos * NA + out.  Operands are split into bf16 hi + lo parts;
+// D += Ah Bh + Ah Bl + Al Bh accumulates in fp32 in tensor memory (relative
+// error ~2^-16 per product).
 //
-// Shared-memory operands use the UMMA K-major no-swizzle layout: 8-row x
-// 16-byte core matrices, rows of a core matrix 16 B apart, core matrices
-// along M/N 128 B apart (SBO) and along K one M/N-extent apart (LBO).  The B
-// tiles are pre-arranged in that layout on the host (tables); a pack kernel
-// writes the A tiles in it once per source evaluation; both are fetched with
-// cp.async.bulk (no multicast).  Every mbarrier wait is bounded; on a timeout
-// the CTA records an error code, drains what it issued (bounded), frees its
-// tensor memory and returns.
+// Angular: one CTA computes a 64-position x N_T-output tile of one source
+// group for both operands at once: UMMA rows 0..63 hold max(P1, 0), rows
+// 64..127 P2 of the same positions, sharing the B operand (ker_v).  Operands
+// use the K-major no-swizzle layout (8-row x 16-byte core matrices); the B
+// tiles are arranged on the host, a pack kernel writes the A tiles once per
+// source evaluation.  The epilogue writes A1 / A2 split into bf16 hi / lo in
+// the energy stage's operand layout (below), so the energy stage reads them
+// with plain bulk copies.
+//
+// Energy: one CTA owns 128 lanes (UMMA M, the A operand, MN-major) and up to
+// 256 output groups (the accumulator columns).  For every 16-group chunk of
+// source groups that some output of the tile uses, it multiplies the chunk's
+// 4 x 128 x 16 A tile by the coefficient tile of the outputs whose band meets
+// the chunk (B operand, K-major, N = that output range rounded to 16), so
+// tensor-core work follows the band.
+//
+// All operand moves are cp.async.bulk (no multicast).  Every mbarrier wait is
+// bounded; on a timeout the CTA records an error code, drains what it issued
+// (bounded), frees its tensor memory and returns.
 
 #include "common.cuh"
 #include "async_copy.cuh"
@@ -64,6 +75,25 @@ __device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
 // rows: core matrix (row/8, k/8) of 8 x 8 bf16.
 __host__ __device__ inline size_t umma_kmajor_offset(int row, int k, int rows) {
     return (static_cast<size_t>(k >> 3) * (rows >> 3) + (row >> 3)) * 128 + (row & 7) * 16 + (k & 7) * 2;
+}
+
+// Byte offset of element (plane, s, l) in the energy stage's A operand: lanes
+// in tiles of 128, source groups in rows of 8.  One (lane tile, 8 groups)
+// block is 8 KB: 4 planes (A1 hi, A1 lo, A2 hi, A2 lo) x 2 atoms of 64 lanes
+// x 8 rows (one per group) x 128 B, the 16-byte pieces of row r permuted to
+// j ^ r -- the shared-memory image of an MN-major 128-byte-swizzled UMMA
+// operand, so that a plain bulk copy of 16 groups (16 KB) lands ready to use.
+// nsg = 2 * ceil(Ng / 16) group rows per lane tile.
+__host__ __device__ inline size_t q_offset(int plane, int s, long long l, int nsg) {
+    const long long t = l >> 7;
+    const int li = static_cast<int>(l & 127), sr = s & 7;
+    return ((static_cast<size_t>(t) * nsg + (s >> 3)) * 4 + plane) * 2048 + (li >> 6) * 1024 + sr * 128 +
+           ((((li >> 3) & 7) ^ sr) << 4) + (li & 7) * 2;
+}
+
+size_t umma_q_bytes(long long per_e, int Ng) {
+    const size_t tiles = static_cast<size_t>((per_e + 127) / 128), nsg = 2 * static_cast<size_t>((Ng + 15) / 16);
+    return tiles * nsg * 8192;
 }
 
 // ---------------------------------------------------------------------------
@@ -128,10 +158,9 @@ struct UmmaPipeArgs {
     const uint8_t* ablob;
     const uint8_t* bblob;    // [n_groups][n_ntiles][nk][hi|lo][N_T x BK bf16, core layout]
     const int* groups;
-    float* A1;
-    float* A2;
+    uint8_t* q;              // energy-stage operand (q_offset layout)
     int* err;
-    int nyz, NA, NT, nk, n_ntiles, n_mt;
+    int nyz, NA, NT, nk, n_ntiles, n_mt, nsg;
 };
 
 template <int BK>
@@ -245,11 +274,13 @@ __global__ void __launch_bounds__(128, 1) source_angular_umma_pipe_kernel(UmmaPi
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (!fail_flag) {
         // Epilogue through shared memory (the pipeline buffers are free now):
-        // each thread moves 16-column slices of its accumulator row into a
-        // [128][17]-float tile, then each warp writes whole rows so that every
-        // store instruction covers 16 consecutive outputs of one position.
+        // 16-column slices of the accumulator go to a [128][17]-float tile;
+        // then each thread takes 8 consecutive outputs of one row, splits
+        // them into bf16 hi / lo and writes both into the energy operand
+        // layout.  Two threads share a row, so with 8-aligned lanes one warp
+        // store covers whole 32-byte pieces.
         float* tile = reinterpret_cast<float*>(smem);
-        constexpr int TS = 17;  // padded row stride: conflict-free both ways
+        constexpr int TS = 17;  // padded row stride
         const uint32_t lane_base = static_cast<uint32_t>(warp * 32) << 16;
         for (int c0 = 0; c0 < NT; c0 += 16) {
             uint32_t v[16];
@@ -262,13 +293,35 @@ __global__ void __launch_bounds__(128, 1) source_angular_umma_pipe_kernel(UmmaPi
 #pragma unroll
             for (int q = 0; q < 16; ++q) tile[tid * TS + q] = __uint_as_float(v[q]);
             __syncthreads();
-            // 128 rows x 16 columns: each warp instruction writes 2 rows x 16 columns
-            const int half = (tid & 31) >> 4, col = tid & 15;
-            const int n = n0 + c0 + col;
-            for (int r = warp * 2 + half; r < kRows; r += 8) {
+            for (int task = tid; task < 2 * kRows; task += 128) {
+                const int r = task >> 1, h = task & 1;
                 const int pos = m0 + (r & (kPos - 1));
-                if (pos < a.nyz && n < a.NA)
-                    ((r >= kPos) ? a.A2 : a.A1)[(static_cast<size_t>(g) * a.nyz + pos) * a.NA + n] = tile[r * TS + col];
+                const int n = n0 + c0 + 8 * h;
+                if (pos >= a.nyz || n >= a.NA) continue;
+                const int plane = r >= kPos ? 2 : 0;
+                const long long l = static_cast<long long>(pos) * a.NA + n;
+                const float* x = tile + r * TS + 8 * h;
+                if ((l & 7) == 0 && n + 8 <= a.NA) {
+                    float y[8], z[8];
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) {
+                        y[k] = x[k];
+                        z[k] = y[k] - __bfloat162float(__float2bfloat16_rn(y[k]));
+                    }
+                    const uint4 hi = make_uint4(pack_bf16(y[0], y[1]), pack_bf16(y[2], y[3]), pack_bf16(y[4], y[5]),
+                                                pack_bf16(y[6], y[7]));
+                    const uint4 lo = make_uint4(pack_bf16(z[0], z[1]), pack_bf16(z[2], z[3]), pack_bf16(z[4], z[5]),
+                                                pack_bf16(z[6], z[7]));
+                    *reinterpret_cast<uint4*>(a.q + q_offset(plane, g, l, a.nsg)) = hi;
+                    *reinterpret_cast<uint4*>(a.q + q_offset(plane + 1, g, l, a.nsg)) = lo;
+                } else {
+                    for (int k = 0; k < 8 && n + k < a.NA; ++k) {
+                        const __nv_bfloat16 hb = __float2bfloat16_rn(x[k]);
+                        const __nv_bfloat16 lb = __float2bfloat16_rn(x[k] - __bfloat162float(hb));
+                        *reinterpret_cast<__nv_bfloat16*>(a.q + q_offset(plane, g, l + k, a.nsg)) = hb;
+                        *reinterpret_cast<__nv_bfloat16*>(a.q + q_offset(plane + 1, g, l + k, a.nsg)) = lb;
+                    }
+                }
             }
             __syncthreads();
         }
@@ -291,7 +344,7 @@ size_t umma_pipe_smem(int NT, int BK) {
 }
 
 cudaError_t launch_source_angular_pipe(const float* P1, const float* P2, uint8_t* ablob, const uint8_t* bblob,
-                                       const int* groups, int n_groups, float* A1, float* A2, int* err, int nyz,
+                                       const int* groups, int n_groups, uint8_t* q, int Ng, int* err, int nyz,
                                        int NA, int NT, int BK, int n_ntiles, cudaStream_t s) {
     if (n_groups <= 0) return cudaSuccess;
     if (BK != 16 || NT % 16 != 0 || NT < 16 || NT > 256) return cudaErrorInvalidValue;
@@ -302,7 +355,7 @@ cudaError_t launch_source_angular_pipe(const float* P1, const float* P2, uint8_t
     pack_source_operand_kernel<<<dim3(static_cast<unsigned>((per_group + 255) / 256), n_groups), 256, 0, s>>>(p);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    UmmaPipeArgs a{ablob, bblob, groups, A1, A2, err, nyz, NA, NT, nk, n_ntiles, n_mt};
+    UmmaPipeArgs a{ablob, bblob, groups, q, err, nyz, NA, NT, nk, n_ntiles, n_mt, 2 * ((Ng + 15) / 16)};
     size_t smem = umma_pipe_smem(NT, BK);
     // at most two CTAs per SM when each holds 256 tensor-memory columns (512 per SM)
     if (NT > 128) smem = std::max<size_t>(smem, 80 * 1024);
@@ -313,6 +366,272 @@ cudaError_t launch_source_angular_pipe(const float* P1, const float* P2, uint8_t
     if (grid.y > 65535 || grid.z > 65535) return cudaErrorInvalidConfiguration;
     kern<<<grid, kRows, smem, s>>>(a);
     return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Energy stage.  CTA (lane tile lt, output tile et) owns lanes 128 lt ..
+// 128 lt + 127 (UMMA rows) and output groups 256 et .. 256 et + 255 (tensor
+// memory columns, zeroed first).  Its work list holds, per 16-group source
+// chunk c that some of its outputs use, the output column range [col,
+// col + ncols) whose bands meet the chunk.  Per item one thread lands the
+// chunk's 16 KB A tile (q_offset layout, MN-major, 128-byte swizzle) and the
+// range's coefficient tile (K-major, no swizzle) with two bulk copies and
+// issues 6 MMAs (hi/lo splits of both operands, A1 and A2) into that column
+// range; kPipeE stages in flight.  The epilogue streams each accumulator row
+// (one lane) column by column to S, 128 consecutive lanes per warp store.
+// ---------------------------------------------------------------------------
+constexpr int kEnergyCols = 256;
+constexpr int kMaxStagesE = 4;
+constexpr uint32_t kQStage = 16384;  // 16 groups x 128 lanes x 4 planes x 2 B
+
+struct EnergyUmmaArgs {
+    const uint8_t* q;
+    const uint8_t* eblob;     // [chunk][e group of 8][4 planes][2 k halves][8 rows][16 B]
+    const int4* work;         // {chunk, first column, columns, first e group}
+    const int* work_begin;    // [n_et + 1]
+    float* S;
+    int* err;
+    long long per_e;
+    int Ng, n_et, nsg, n_eg, nst;
+    uint32_t stage_bytes;
+};
+
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return umma_desc(addr, lbo, sbo) | (2ull << 61);
+}
+
+__global__ void __launch_bounds__(128, 1) source_energy_umma_kernel(EnergyUmmaArgs a) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    __shared__ __align__(8) uint64_t bar_full[kMaxStagesE];
+    __shared__ __align__(8) uint64_t bar_mma[kMaxStagesE];
+    __shared__ uint32_t tmem_base_slot;
+    __shared__ int fail_flag;
+
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int et = static_cast<int>(blockIdx.x % a.n_et);
+    const long long lt = blockIdx.x / a.n_et;
+    const int w0 = a.work_begin[et], nw = a.work_begin[et + 1] - w0;
+    const int nst = a.nst;
+    // 128-byte swizzle atoms want 1024-byte aligned stages
+    const uint32_t raw = smem_u32(smem);
+    uint8_t* stages = smem + (((raw + 1023u) & ~1023u) - raw);
+
+    if (tid == 0) {
+        for (int st = 0; st < nst; ++st) {
+            mbar_init(&bar_full[st], 1);
+            mbar_init(&bar_mma[st], 1);
+        }
+        mbar_init_fence();
+        fail_flag = 0;
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_slot)),
+                     "r"(kEnergyCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_base_slot;
+    const uint32_t lane_base = static_cast<uint32_t>(warp * 32) << 16;
+    {  // zero the accumulator: the MMAs of an item only add into its column range
+        const uint32_t z = 0;
+        for (int c0 = 0; c0 < kEnergyCols; c0 += 16)
+            asm volatile(
+                "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1};" ::"r"(
+                    tmem + lane_base + c0),
+                "r"(z)
+                : "memory");
+        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+
+    if (tid == 0 && nw > 0) {
+        int issued[kMaxStagesE] = {}, landed[kMaxStagesE] = {}, committed[kMaxStagesE] = {},
+            drained[kMaxStagesE] = {};
+        const uint8_t* __restrict__ qtile = a.q + static_cast<size_t>(lt) * a.nsg * 8192;
+        auto issue = [&](int it) {
+            const int st = it % nst;
+            const int4 w = a.work[w0 + it];
+            uint8_t* sQ = stages + st * a.stage_bytes;
+            const uint32_t ebytes = static_cast<uint32_t>(w.z) * 128u;  // columns x 4 planes x 16 groups x 2 B
+            mbar_expect_tx(&bar_full[st], kQStage + ebytes);
+            bulk_copy_g2s(sQ, qtile + static_cast<size_t>(2 * w.x) * 8192, kQStage, &bar_full[st]);
+            bulk_copy_g2s(sQ + kQStage, a.eblob + (static_cast<size_t>(w.x) * a.n_eg + w.w) * 1024, ebytes,
+                          &bar_full[st]);
+            ++issued[st];
+        };
+        constexpr uint32_t idesc_base = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) |
+                                        (static_cast<uint32_t>(128 >> 4) << 24);  // f32 += bf16 x bf16, A MN-major
+        bool bad = false;
+        for (int it = 0; it < min(nst, nw); ++it) issue(it);
+        for (int it = 0; it < nw && !bad; ++it) {
+            const int st = it % nst;
+            if (!mbar_wait(&bar_full[st], (it / nst) & 1)) {
+                bad = true;
+                break;
+            }
+            ++landed[st];
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const int4 w = a.work[w0 + it];
+            const uint32_t aQ = smem_u32(stages + st * a.stage_bytes), aE = aQ + kQStage;
+            const uint32_t idesc = idesc_base | (static_cast<uint32_t>(w.z >> 3) << 17);
+            const uint32_t d = tmem + static_cast<uint32_t>(w.y);
+#pragma unroll
+            for (int x = 0; x < 2; ++x) {  // A1 with dg e1, A2 with dg e2 / 3
+                const uint64_t qh = umma_desc_sw128(aQ + (2 * x) * 2048, 1024, 8192);
+                const uint64_t ql = umma_desc_sw128(aQ + (2 * x + 1) * 2048, 1024, 8192);
+                const uint64_t eh = umma_desc(aE + (2 * x) * 256, 128, 1024);
+                const uint64_t el = umma_desc(aE + (2 * x + 1) * 256, 128, 1024);
+                umma_bf16(d, qh, eh, idesc, 1u);
+                umma_bf16(d, ql, eh, idesc, 1u);
+                umma_bf16(d, qh, el, idesc, 1u);
+            }
+            umma_commit(&bar_mma[st]);
+            ++committed[st];
+            const int prev = it - 1;
+            if (prev >= 0 && prev + nst < nw) {
+                const int ps = prev % nst;
+                if (!mbar_wait(&bar_mma[ps], (prev / nst) & 1)) {
+                    bad = true;
+                    break;
+                }
+                ++drained[ps];
+                issue(prev + nst);
+            }
+        }
+        if (!bad) {
+            const int last = nw - 1;
+            if (!mbar_wait(&bar_mma[last % nst], (last / nst) & 1)) bad = true;
+        }
+        if (bad) {
+            atomicExch(a.err, 2);
+            for (int st = 0; st < nst; ++st) {
+                if (committed[st] > drained[st]) mbar_wait(&bar_mma[st], (committed[st] - 1) & 1);
+                if (issued[st] > landed[st]) mbar_wait(&bar_full[st], (issued[st] - 1) & 1);
+            }
+            fail_flag = 1;
+        }
+    }
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (!fail_flag) {
+        const int E0 = et * kEnergyCols;
+        const int ncol = min(kEnergyCols, a.Ng - E0);
+        const long long l = lt * 128 + tid;  // accumulator row tid = lane tid of the tile
+        float* __restrict__ S = a.S + static_cast<size_t>(E0) * a.per_e + l;
+        for (int c0 = 0; c0 < ncol; c0 += 16) {
+            uint32_t v[16];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                  "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+                : "r"(tmem + lane_base + c0));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (l < a.per_e) {
+#pragma unroll
+                for (int j = 0; j < 16; ++j)
+                    if (c0 + j < ncol) S[static_cast<size_t>(c0 + j) * a.per_e] = __uint_as_float(v[j]);
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kEnergyCols)
+                     : "memory");
+    }
+}
+
+// Stages per CTA: as many (up to 4) as keep two CTAs on an SM.
+static int energy_umma_stages(int emax_cols, uint32_t* stage_bytes) {
+    *stage_bytes = kQStage + static_cast<uint32_t>(emax_cols) * 128u;
+    int nst = kMaxStagesE;
+    while (nst > 2 && nst * static_cast<size_t>(*stage_bytes) + 1024 > 110 * 1024) --nst;
+    return nst;
+}
+
+// At least 80 KB, so that no third CTA waits on an SM for tensor memory
+// (two CTAs x 256 columns fill it).
+size_t energy_umma_smem(int emax_cols) {
+    uint32_t sb = 0;
+    const int nst = energy_umma_stages(emax_cols, &sb);
+    return std::max<size_t>(nst * static_cast<size_t>(sb) + 1024, 80 * 1024);
+}
+
+cudaError_t launch_source_energy_umma(const uint8_t* q, const uint8_t* eblob, const int* work, const int* work_begin,
+                                      int n_et, int emax_cols, float* S, int* err, long long per_e, int Ng,
+                                      cudaStream_t s) {
+    if (emax_cols < 0 || emax_cols > kEnergyCols || emax_cols % 16 != 0) return cudaErrorInvalidValue;
+    if (n_et != (Ng + kEnergyCols - 1) / kEnergyCols) return cudaErrorInvalidValue;
+    const long long n_lt = (per_e + 127) / 128;
+    if (n_lt * n_et > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+    EnergyUmmaArgs a;
+    a.q = q;
+    a.eblob = eblob;
+    a.work = reinterpret_cast<const int4*>(work);
+    a.work_begin = work_begin;
+    a.S = S;
+    a.err = err;
+    a.per_e = per_e;
+    a.Ng = Ng;
+    a.n_et = n_et;
+    a.nsg = 2 * ((Ng + 15) / 16);
+    a.n_eg = a.nsg;
+    a.nst = energy_umma_stages(emax_cols, &a.stage_bytes);
+    const size_t smem = energy_umma_smem(emax_cols);
+    cudaError_t e = cudaFuncSetAttribute(source_energy_umma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    source_energy_umma_kernel<<<static_cast<unsigned>(n_lt * n_et), 128, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+// Host: the energy stage's coefficient tiles and work lists.  Tile (chunk c,
+// e group g) = 1 KB: planes dg e1 hi, dg e1 lo, dg e2 / 3 hi, dg e2 / 3 lo,
+// each [2 k halves][8 outputs][8 source groups] bf16 (K-major core matrices).
+void build_energy_umma(const double* e1, const double* e2, const int* band_begin, const int* band_end, int Ng,
+                       double dg, std::vector<uint8_t>& blob, std::vector<int>& work, std::vector<int>& begin,
+                       int& emax_cols) {
+    const int nchunk = (Ng + 15) / 16, n_eg = 2 * nchunk, n_et = (Ng + kEnergyCols - 1) / kEnergyCols;
+    blob.assign(static_cast<size_t>(nchunk) * n_eg * 1024, 0);
+    for (int e = 0; e < Ng; ++e)
+        for (int sg = band_begin[e]; sg < band_end[e]; ++sg) {
+            const double v[2] = {dg * e1[static_cast<size_t>(e) * Ng + sg], dg * e2[static_cast<size_t>(e) * Ng + sg] / 3.0};
+            const int c = sg >> 4, k = sg & 15;
+            for (int x = 0; x < 2; ++x) {
+                const float f = static_cast<float>(v[x]);
+                const __nv_bfloat16 h = __float2bfloat16_rn(f);
+                const __nv_bfloat16 l = __float2bfloat16_rn(f - __bfloat162float(h));
+                const size_t off = ((static_cast<size_t>(c) * n_eg + (e >> 3)) * 4 + 2 * x) * 256 + (k >> 3) * 128 +
+                                   (e & 7) * 16 + (k & 7) * 2;
+                std::memcpy(blob.data() + off, &h, 2);
+                std::memcpy(blob.data() + off + 256, &l, 2);
+            }
+        }
+    work.clear();
+    begin.assign(n_et + 1, 0);
+    emax_cols = 0;
+    for (int et = 0; et < n_et; ++et) {
+        const int E0 = et * kEnergyCols, E1 = std::min(Ng, E0 + kEnergyCols);
+        for (int c = 0; c < nchunk; ++c) {
+            int lo = E1, hi = E0;
+            for (int e = E0; e < E1; ++e)
+                if (band_begin[e] < band_end[e] && band_begin[e] < 16 * c + 16 && band_end[e] > 16 * c) {
+                    lo = std::min(lo, e);
+                    hi = std::max(hi, e + 1);
+                }
+            if (lo >= hi) continue;
+            const int col = (lo - E0) / 16 * 16, ncols = (hi - E0 + 15) / 16 * 16 - col;
+            work.insert(work.end(), {c, col, ncols, (E0 + col) / 8});
+            emax_cols = std::max(emax_cols, ncols);
+        }
+        begin[et + 1] = static_cast<int>(work.size() / 4);
+    }
 }
 
 // Host: B tiles of every used group in the device layout of the kernel above.
