@@ -106,6 +106,8 @@ struct bfpn_ctx {
     bool tr_plane_ok = false;   // a compiled whole-plane kernel exists for this plane
     bool tr_plane = false;      // use it
     int tr_plane_ac = 8;
+    bool tr_pairs_ok = false;   // angle pairs share direction signs (float whole planes)
+    bool tr_pairs = true;       // use the paired kernel where it applies
     bool tr_tile_ok = false;    // the plane needs tiles: the unrolled tiled kernel applies
     bool tr_tile = false;       // use it
     int tr_tile_ac = 8;
@@ -417,6 +419,7 @@ cudaError_t enq_transport(bfpn_ctx* c, const void* in, void* out, double dt, boo
     a.tile_y = c->tr_ty;
     a.tile_z = c->tr_tz;
     a.preserve_sign = preserve_sign ? 1 : 0;
+    a.pairs = (c->elem == 4 && c->tr_pairs && c->tr_pairs_ok) ? 1 : 0;
     if (c->tr_plane)
         return prof(c, BFPN_KERNEL_TRANSPORT, [&] { return launch_transport_plane<T>(a, c->tr_plane_ac, c->stream); });
     if (c->tr_tile && a.in != a.out)
@@ -936,6 +939,7 @@ bfpn_status bfpn_load_tables(bfpn_ctx* c, const double* mu, int32_t mu_rows, con
     const auto lite = lite_coefficients(T, c->d.dt);
     if ((s = upload_f64(c, c->lite_coef, lite.data(), lite.size() * sizeof(double))) != BFPN_OK) return s;
     if ((s = upload_state_table(c, c->omega, T.omega)) != BFPN_OK) return s;
+    c->tr_pairs_ok = transport_pairs_ok(T.omega.data(), c->NA);
     if ((s = upload_state_table(c, c->fac_step, angle_factor(T, c->p, c->d.dt))) != BFPN_OK) return s;
     if ((s = upload_state_table(c, c->sine_u, T.sine_u)) != BFPN_OK) return s;
     if ((s = upload_state_table(c, c->sine_v, T.sine_v)) != BFPN_OK) return s;
@@ -1180,6 +1184,9 @@ bfpn_status bfpn_set_option(bfpn_ctx* c, int32_t option, int32_t value) {
             break;
         case BFPN_OPT_CUDA_GRAPHS:
             c->use_graphs = value != 0 && !c->profiling;
+            break;
+        case BFPN_OPT_PAIRED_ANGLES:
+            c->tr_pairs = value != 0;
             break;
         case BFPN_OPT_PLANE_TRANSPORT: {
             const bool f32 = c->elem == 4;

@@ -71,6 +71,7 @@ struct TransportArgs {
     T dt, dy, dz;
     int tile_y, tile_z;    // output tile (positions)
     int preserve_sign;
+    int pairs = 0;         // float whole planes: two angles per thread (transport_pairs_ok)
 };
 
 // Arguments of one angular-diffusion step (Eq. 19) over one array.
@@ -178,6 +179,9 @@ size_t transport_smem(int Ny1, int Nz1, int ty, int tz, int ac, size_t elem);
 // (transport_plane_supported); ang_chunk 8 or 16 (float), 4 or 8 (double).
 template <typename T> cudaError_t launch_transport_plane(const TransportArgs<T>& a, int ang_chunk, cudaStream_t s);
 bool transport_plane_supported(int Ny, int Nz);
+// True when NA is even and angles (2i, 2i+1) share the signs of omega_y and
+// omega_z ([NA][2] table): the float whole-plane kernel may then pair them.
+bool transport_pairs_ok(const double* omega, int NA);
 // Any plane, in 27 x 27 output tiles with a 4-cell halo, out of place;
 // ang_chunk 4 or 8 (float), 2 or 4 (double).
 template <typename T> cudaError_t launch_transport_tiles(const TransportArgs<T>& a, int ang_chunk, cudaStream_t s);

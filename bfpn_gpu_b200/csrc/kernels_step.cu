@@ -494,6 +494,38 @@ __device__ __forceinline__ void walk_plane_line(const T* X, T wr, T h, const Emi
     emit(N, wr * (xn - gp), xn, xp);  // G(N) = X(N)
 }
 
+// The same walk with its loads issued kPrefetch steps ahead of their use, in
+// program order before the stores of the steps in between (a walk only
+// stores to cells it has already read, so nothing is read stale), and with a
+// second line Y (stride SY) loaded alongside and handed to emit as
+// emit(j, D(j), X(j), X(j-1), Y[j*SY]).
+constexpr int kPrefetch = 4;
+template <typename T, int N, int S, int SY, bool HY, typename Emit>
+__device__ __forceinline__ void walk_plane_line_pf(const T* X, const T* Y, T wr, T h, const Emit& emit) {
+    T x[N + 1], y[N + 1];
+#pragma unroll
+    for (int k = 0; k <= N && k <= kPrefetch + 1; ++k) x[k] = X[k * S];
+    if constexpr (HY) {
+#pragma unroll
+        for (int k = 1; k <= N && k <= kPrefetch; ++k) y[k] = Y[k * SY];
+    }
+    T fwd = x[1] - x[0];
+    T gp = x[0];
+#pragma unroll
+    for (int j = 1; j < N; ++j) {
+        if (j + 1 + kPrefetch <= N) x[j + 1 + kPrefetch] = X[(j + 1 + kPrefetch) * S];
+        if constexpr (HY) {
+            if (j + kPrefetch <= N) y[j + kPrefetch] = Y[(j + kPrefetch) * SY];
+        }
+        const T back = fwd;
+        fwd = x[j + 1] - x[j];
+        const T g = x[j] + h * superbee_diff(back, fwd);
+        emit(j, wr * (g - gp), x[j], x[j - 1], HY ? y[j] : T(0));
+        gp = g;
+    }
+    emit(N, wr * (x[N] - gp), x[N], x[N - 1], HY ? y[N] : T(0));  // G(N) = X(N)
+}
+
 template <typename T, int NP, int AC>
 __global__ void __launch_bounds__((NP * AC + 31) / 32 * 32) transport_plane_kernel(TransportArgs<T> a, int n_chunks) {
     constexpr int N = NP - 1, RP = NP | 1, RS = RP * AC, PL = NP * RS;
@@ -544,7 +576,7 @@ __global__ void __launch_bounds__((NP * AC + 31) / 32 * 32) transport_plane_kern
     if (act) {
         const T* X = Fs + line * RS + q;
         T* D = Ps + line * RS + q - sy * AC;
-        walk_plane_line<T, N, AC>(X, wry, hy, [&](int j, T d, T, T) { D[j * AC] = d; });
+        walk_plane_line_pf<T, N, AC, 0, false>(X, nullptr, wry, hy, [&](int j, T d, T, T, T) { D[j * AC] = d; });
         Ps[line * RS + q + sy * N * AC] = T(0);
     }
     __syncthreads();
@@ -554,9 +586,9 @@ __global__ void __launch_bounds__((NP * AC + 31) / 32 * 32) transport_plane_kern
         T* Pc = Ps + line * AC + q;
         T* Xe = Xc - sz * RS;
         T* Pe = Pc - sz * RS;
-        walk_plane_line<T, N, RS>(Xc, wrz, hz, [&](int j, T dz, T xj, T xjm1) {
+        walk_plane_line_pf<T, N, RS, RS, true>(Xc, Pe, wrz, hz, [&](int j, T dz, T xj, T xjm1, T pj) {
             const T f = dnz ? xjm1 : xj;
-            const T d = Pe[j * RS] + dz;
+            const T d = pj + dz;
             Pe[j * RS] = max(f - dt * d, lo);
             Xe[j * RS] = f - hdt * d;
         });
@@ -570,7 +602,8 @@ __global__ void __launch_bounds__((NP * AC + 31) / 32 * 32) transport_plane_kern
     if (act) {
         const T* X = Ps + line * RS + q;
         T* Fe = Fs + line * RS + q - sy * AC;
-        walk_plane_line<T, N, AC>(X, wry, hy, [&](int j, T d, T, T) { Fe[j * AC] -= hdt * d; });
+        walk_plane_line_pf<T, N, AC, AC, true>(X, Fe, wry, hy,
+                                               [&](int j, T d, T, T, T fj) { Fe[j * AC] = fj - hdt * d; });
     }
     __syncthreads();
     // stage 2, z-part (columns) and the corrector, to global
@@ -581,13 +614,187 @@ __global__ void __launch_bounds__((NP * AC + 31) / 32 * 32) transport_plane_kern
         T* o = out + static_cast<size_t>(line) * NA + q;
         const size_t zs = static_cast<size_t>(NP) * NA;
         T* oe = o - sz * zs;
-        walk_plane_line<T, N, RS>(X, wrz, hz, [&](int j, T d, T, T) {
-            const T v = max(Fe[j * RS] - hdt * d, lo);
+        walk_plane_line_pf<T, N, RS, RS, true>(X, Fe, wrz, hz, [&](int j, T d, T, T, T fj) {
+            const T v = max(fj - hdt * d, lo);
             if (qok) oe[j * zs] = v;
         });
         const int cb = sz * N;
         if (qok) o[cb * zs] = max(Fc[cb * RS], lo);
     }
+}
+
+// ---------------------------------------------------------------------------
+// The same whole-plane kernel with two angles per thread (float state; the
+// two share the signs of omega_y and omega_z, checked on the host).  Sums,
+// products and shared-memory moves work on fp32x2 pairs; the limiter's
+// compares stay per angle.  Each operation is the scalar kernel's, so the
+// results agree with it value for value (up to the sign of zeros).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float2 sub2(float2 x, float2 y) {  // x - y, one rounding
+    return __ffma2_rn(y, make_float2(-1.f, -1.f), x);
+}
+
+// sign(fwd) where |fwd| >= eps, +-0 below: set gives 1.0f / 0.0f, the sign bit of fwd is or-ed in.
+__device__ __forceinline__ float sign_or_zero(float fwd) {
+    float st;
+    asm("set.ge.f32.f32 %0, %1, %2;" : "=f"(st) : "f"(fabsf(fwd)), "f"(static_cast<float>(kEpsilon)));
+    return __int_as_float(__float_as_int(st) | (__float_as_int(fwd) & static_cast<int>(0x80000000u)));
+}
+
+// superbee_diff for a pair: with s = sign_or_zero(fwd), b = s back and
+// |fwd| = s fwd (both exact), and the slope is s m; below eps s = 0 makes
+// b = |fwd| = 0 and so m = 0.
+__device__ __forceinline__ float2 superbee_diff2(float2 back, float2 fwd) {
+    const float2 s = make_float2(sign_or_zero(fwd.x), sign_or_zero(fwd.y));
+    const float2 b = __fmul2_rn(back, s), af = __fmul2_rn(fwd, s);
+    const float2 b2 = __fadd2_rn(b, b), af2 = __fadd2_rn(af, af);
+    float2 m;
+    m.x = fmaxf(0.f, fmaxf(fminf(b2.x, af.x), fminf(b.x, af2.x)));
+    m.y = fmaxf(0.f, fmaxf(fminf(b2.y, af.y), fminf(b.y, af2.y)));
+    return __fmul2_rn(m, s);
+}
+
+template <int N, int S, int SY, bool HY, typename Emit>
+__device__ __forceinline__ void walk_plane_line2(const float2* X, const float2* Y, float2 wr, float2 h,
+                                                 const Emit& emit) {
+    float2 x[N + 1], y[N + 1];
+#pragma unroll
+    for (int k = 0; k <= N && k <= kPrefetch + 1; ++k) x[k] = X[k * S];
+    if constexpr (HY) {
+#pragma unroll
+        for (int k = 1; k <= N && k <= kPrefetch; ++k) y[k] = Y[k * SY];
+    }
+    float2 fwd = sub2(x[1], x[0]);
+    float2 gp = x[0];
+#pragma unroll
+    for (int j = 1; j < N; ++j) {
+        if (j + 1 + kPrefetch <= N) x[j + 1 + kPrefetch] = X[(j + 1 + kPrefetch) * S];
+        if constexpr (HY) {
+            if (j + kPrefetch <= N) y[j + kPrefetch] = Y[(j + kPrefetch) * SY];
+        }
+        const float2 back = fwd;
+        fwd = sub2(x[j + 1], x[j]);
+        const float2 g = __ffma2_rn(h, superbee_diff2(back, fwd), x[j]);
+        emit(j, __fmul2_rn(wr, sub2(g, gp)), x[j], x[j - 1], HY ? y[j] : make_float2(0.f, 0.f));
+        gp = g;
+    }
+    emit(N, __fmul2_rn(wr, sub2(x[N], gp)), x[N], x[N - 1], HY ? y[N] : make_float2(0.f, 0.f));
+}
+
+__device__ __forceinline__ float2 max_lo2(float2 v, float lo) { return make_float2(fmaxf(v.x, lo), fmaxf(v.y, lo)); }
+
+template <int NP, int AC>
+__global__ void __launch_bounds__((NP * AC / 2 + 31) / 32 * 32) transport_plane_f2_kernel(TransportArgs<float> a,
+                                                                                           int n_chunks) {
+    constexpr int N = NP - 1, RP = NP | 1, A2 = AC / 2, RS = RP * A2, PL = NP * RS;  // in float2
+    constexpr int NT = (NP * A2 + 31) / 32 * 32;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2* Fs = reinterpret_cast<float2*>(smem_raw);
+    float2* Ps = Fs + PL;
+    const int chunk = blockIdx.x % n_chunks, ek = blockIdx.x / n_chunks;
+    const int NA = a.NA, a0 = chunk * AC;
+    const size_t plane = static_cast<size_t>(ek) * NP * NP * NA + a0;
+    const float* __restrict__ in = a.in + plane;
+    float* __restrict__ out = a.out + plane;
+    const int q = threadIdx.x % A2, line = threadIdx.x / A2;  // angles a0 + 2q, a0 + 2q + 1
+    const bool ok0 = a0 + 2 * q < NA, ok1 = a0 + 2 * q + 1 < NA;
+    const int g0 = min(a0 + 2 * q, NA - 1), g1 = min(a0 + 2 * q + 1, NA - 1);
+    const float wy0 = a.omega[2 * g0], wz0 = a.omega[2 * g0 + 1];
+    const float wy1 = a.omega[2 * g1], wz1 = a.omega[2 * g1 + 1];
+    const float2 wry = make_float2(wy0 / a.dy, wy1 / a.dy), wrz = make_float2(wz0 / a.dz, wz1 / a.dz);
+    const bool dny = wy0 < 0.f, dnz = wz0 < 0.f;
+    const float2 hy = dny ? make_float2(-0.5f, -0.5f) : make_float2(0.5f, 0.5f);
+    const float2 hz = dnz ? make_float2(-0.5f, -0.5f) : make_float2(0.5f, 0.5f);
+    const int sy = dny ? 1 : 0, sz = dnz ? 1 : 0;
+    const float2 ndt = make_float2(-a.dt, -a.dt), nhdt = make_float2(-0.5f * a.dt, -0.5f * a.dt);
+    const float lo = a.preserve_sign ? -INFINITY : 0.f;
+
+    float* Fsf = reinterpret_cast<float*>(Fs);
+    if (AC % 4 == 0 && NA % 4 == 0) {
+        constexpr int NV = NP * NP * AC / 4;
+#pragma unroll 4
+        for (int v = threadIdx.x; v < NV; v += NT) {
+            const int e = v * 4, aa = e % AC, p = e / AC;
+            const int z = p / NP, y = p - z * NP;
+            float4 val{};
+            if (a0 + aa < NA) val = *reinterpret_cast<const float4*>(in + static_cast<size_t>(p) * NA + aa);
+            *reinterpret_cast<float4*>(Fsf + 2 * (z * RS + y * A2) + aa) = val;
+        }
+    } else {
+#pragma unroll 4
+        for (int e = threadIdx.x; e < NP * NP * AC; e += NT) {
+            const int aa = e % AC, p = e / AC;
+            const int z = p / NP, y = p - z * NP;
+            Fsf[2 * (z * RS + y * A2) + aa] = (a0 + aa < NA) ? in[static_cast<size_t>(p) * NA + aa] : 0.f;
+        }
+    }
+    __syncthreads();
+    const bool act = line < NP;
+    // stage 1, y-part of div F (rows z = line) into Ps
+    if (act) {
+        const float2* X = Fs + line * RS + q;
+        float2* D = Ps + line * RS + q - sy * A2;
+        walk_plane_line2<N, A2, 0, false>(X, nullptr, wry, hy, [&](int j, float2 d, float2, float2, float2) {
+            D[j * A2] = d;
+        });
+        Ps[line * RS + q + sy * N * A2] = make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    // stage 1, z-part (columns y = line): predictor into Ps, H over F
+    if (act) {
+        float2* Xc = Fs + line * A2 + q;
+        float2* Pc = Ps + line * A2 + q;
+        float2* Xe = Xc - sz * RS;
+        float2* Pe = Pc - sz * RS;
+        walk_plane_line2<N, RS, RS, true>(Xc, Pe, wrz, hz, [&](int j, float2 dz, float2 xj, float2 xjm1, float2 pj) {
+            const float2 f = dnz ? xjm1 : xj;
+            const float2 d = __fadd2_rn(pj, dz);
+            Pe[j * RS] = max_lo2(__ffma2_rn(ndt, d, f), lo);
+            Xe[j * RS] = __ffma2_rn(nhdt, d, f);
+        });
+        const int cb = sz * N * RS;
+        const float2 f = Xc[cb], d = Pc[cb];
+        Pc[cb] = max_lo2(__ffma2_rn(ndt, d, f), lo);
+        Xc[cb] = __ffma2_rn(nhdt, d, f);
+    }
+    __syncthreads();
+    // stage 2, y-part of div P (rows): H - dt/2 d_y P over F
+    if (act) {
+        const float2* X = Ps + line * RS + q;
+        float2* Fe = Fs + line * RS + q - sy * A2;
+        walk_plane_line2<N, A2, A2, true>(X, Fe, wry, hy, [&](int j, float2 d, float2, float2, float2 fj) {
+            Fe[j * A2] = __ffma2_rn(nhdt, d, fj);
+        });
+    }
+    __syncthreads();
+    // stage 2, z-part (columns) and the corrector, to global
+    if (act) {
+        const float2* X = Ps + line * A2 + q;
+        const float2* Fc = Fs + line * A2 + q;
+        const float2* Fe = Fc - sz * RS;
+        float* o = out + static_cast<size_t>(line) * NA + 2 * q;
+        const size_t zs = static_cast<size_t>(NP) * NA;
+        float* oe = o - sz * zs;
+        auto put = [&](float* dst, float2 v) {
+            if (ok1) *reinterpret_cast<float2*>(dst) = v;
+            else if (ok0) *dst = v.x;
+        };
+        walk_plane_line2<N, RS, RS, true>(X, Fe, wrz, hz, [&](int j, float2 d, float2, float2, float2 fj) {
+            put(oe + j * zs, max_lo2(__ffma2_rn(nhdt, d, fj), lo));
+        });
+        const int cb = sz * N;
+        put(o + cb * zs, max_lo2(Fc[cb * RS], lo));
+    }
+}
+
+// The packed kernel applies when NA is even (8-byte aligned pairs) and the
+// two angles of every pair share the signs of omega_y and omega_z.
+bool transport_pairs_ok(const double* omega, int NA) {
+    if (NA % 2 != 0) return false;
+    for (int g = 0; g + 1 < NA; g += 2)
+        if ((omega[2 * g] < 0) != (omega[2 * g + 2] < 0) || (omega[2 * g + 1] < 0) != (omega[2 * g + 3] < 0))
+            return false;
+    return true;
 }
 
 size_t transport_plane_smem(int NP, int ac, size_t elem) {
@@ -797,9 +1004,36 @@ static cudaError_t launch_plane_ac(const TransportArgs<T>& a, cudaStream_t s) {
     }
 }
 
+template <int NP, int AC>
+static cudaError_t launch_plane_f2_np(const TransportArgs<float>& a, cudaStream_t s) {
+    const int n_chunks = (a.NA + AC - 1) / AC;
+    const size_t smem = transport_plane_smem(NP, AC, sizeof(float));
+    auto kern = transport_plane_f2_kernel<NP, AC>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    const long long blocks = static_cast<long long>(a.Ng) * n_chunks;
+    if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+    kern<<<static_cast<unsigned>(blocks), (NP * AC / 2 + 31) / 32 * 32, smem, s>>>(a, n_chunks);
+    return cudaGetLastError();
+}
+
+template <int AC>
+static cudaError_t launch_plane_f2_ac(const TransportArgs<float>& a, cudaStream_t s) {
+    if (a.Ny != a.Nz || a.NA % 2 != 0) return cudaErrorNotSupported;
+    switch (a.Ny + 1) {
+#define BFPN_CASE(NP) \
+    case NP: return launch_plane_f2_np<NP, AC>(a, s);
+        BFPN_PLANE_SIZES(BFPN_CASE)
+#undef BFPN_CASE
+        default: return cudaErrorNotSupported;
+    }
+}
+
 template <typename T>
 cudaError_t launch_transport_plane(const TransportArgs<T>& a, int ang_chunk, cudaStream_t s) {
     if constexpr (sizeof(T) == 4) {
+        if (a.pairs && ang_chunk == 8) return launch_plane_f2_ac<8>(a, s);
+        if (a.pairs && ang_chunk == 16) return launch_plane_f2_ac<16>(a, s);
         if (ang_chunk == 8) return launch_plane_ac<T, 8>(a, s);
         if (ang_chunk == 16) return launch_plane_ac<T, 16>(a, s);
     } else {

@@ -237,17 +237,22 @@ int32_t bfpn_kernels_per_step(bfpn_ctx* ctx);
 int32_t bfpn_source_groups(bfpn_ctx* ctx);
 
 /* Run-time options (take effect from the next step; graphs are re-captured).
- * BFPN_OPT_TENSOR_CORES: 1 (default) computes the source's angular
- *   contraction on the tcgen05 tensor cores in mixed precision (split-bf16
- *   operands, fp32 accumulation); 0 uses the fp32 CUDA-core kernel.
+ * BFPN_OPT_TENSOR_CORES: 1 (default) computes the source's angular and
+ *   energy contractions on the tcgen05 tensor cores in mixed precision
+ *   (split-bf16 operands, fp32 accumulation); 0 uses the fp32 CUDA-core
+ *   kernels.
  * BFPN_OPT_CUDA_GRAPHS: 1 (default) replays each depth step as a CUDA graph.
  * BFPN_OPT_PLANE_TRANSPORT: 1 (default) runs the transport with the unrolled
  *   kernels: one block per whole plane for square planes with
  *   Ny = Nz in {4,6,8,10,12,14,16,20,24,32}, 27 x 27 tiles for planes too large
  *   for one block; 0 uses the general line-walk kernel; a larger value selects
  *   the angles per block (whole planes: 8 or 16 mixed, 4 or 8 FP64; tiles: 4 or
- *   8 mixed, 2 or 4 FP64).  All compute the same values. */
-enum { BFPN_OPT_TENSOR_CORES = 0, BFPN_OPT_CUDA_GRAPHS = 1, BFPN_OPT_PLANE_TRANSPORT = 2 };
+ *   8 mixed, 2 or 4 FP64).  All compute the same values.
+ * BFPN_OPT_PAIRED_ANGLES: 1 (default) lets the mixed-precision whole-plane
+ *   transport carry two angles per thread on packed fp32x2 arithmetic when NA
+ *   is even and the angles of each pair (2i, 2i+1) share the signs of their
+ *   direction cosines; 0 keeps one angle per thread.  Same values. */
+enum { BFPN_OPT_TENSOR_CORES = 0, BFPN_OPT_CUDA_GRAPHS = 1, BFPN_OPT_PLANE_TRANSPORT = 2, BFPN_OPT_PAIRED_ANGLES = 3 };
 bfpn_status bfpn_set_option(bfpn_ctx* ctx, int32_t option, int32_t value);
 
 /* bfpn_step_async(nsteps) bracketed by CUDA events on the context stream;

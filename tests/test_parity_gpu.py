@@ -172,6 +172,37 @@ def test_plane_transport_mixed_matches_line_walks():
         ctx.set_option(capi.OPT_PLANE_TRANSPORT, 4)  # 4 angles per block is the FP64 chunk
 
 
+@pytest.mark.parametrize("nom,paired", [(8, True), (6, False)])  # NA 48: pairs share signs; NA 36: pair (2,3) straddles
+def test_paired_plane_transport_equals_single_angle_kernel(nom, paired):
+    """Two angles per thread on packed fp32x2 (mixed whole-plane transport)
+    gives the one-angle kernel's values exactly, including flat regions and
+    differences below the limiter's epsilon; where a pair straddles a sign
+    change of the direction cosines the one-angle kernel runs."""
+    cfg = small_cfg(ny=20, nz=20, nmu=6, nom=nom, ng=5, lz=2.0)
+    ctx, _ = build(cfg, precision=capi.PREC_MIXED)
+    Ng, nyz, NA = ctx.shape
+    states = [a.reshape(Ng, nyz, NA).copy() for a in seeded_states(ctx, 12)]
+    for a in states:
+        a[1, : nyz // 2] = a[1, 0]                    # flat: zero differences
+        a[2] = 3e-11 * np.arange(nyz)[:, None]         # y differences below 1e-10
+        a[3, ::7] = 0.0
+    out = {}
+    for pairs in (1, 0):
+        ctx.set_option(capi.OPT_PAIRED_ANGLES, pairs)
+        for chunk in (16, 8):
+            ctx.set_option(capi.OPT_PLANE_TRANSPORT, chunk)
+            for k, arr in enumerate(states):
+                ctx.set_state(k // 2, k % 2, arr.ravel())
+            ctx.transport(0, 0, 0.5 * cfg.dt(), False)
+            ctx.transport(0, 1, 0.5 * cfg.dt(), True)
+            ctx.transport(1, 1, 0.37 * cfg.dt(), True)
+            out[(pairs, chunk)] = [ctx.get_state(sp, cf) for sp, cf in ((0, 0), (0, 1), (1, 1))]
+    for key, got in out.items():
+        for a, b in zip(got, out[(0, 16)]):
+            assert np.array_equal(a, b), key
+    assert np.abs(out[(0, 16)][1]).max() > 0
+
+
 def test_angle_operator():
     cfg = small_cfg(nmu=7, nom=6)
     ctx, ora = build(cfg)
