@@ -52,6 +52,25 @@ __device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32
                  : "memory");
 }
 
+// Shared -> global bulk copy in the calling thread's bulk group (16-byte
+// aligned addresses, size a multiple of 16).
+__device__ __forceinline__ void bulk_copy_s2g(void* dst, const void* src, uint32_t bytes) {
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_u32(src)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// Until at most N of this thread's committed bulk groups still read shared memory.
+template <int N>
+__device__ __forceinline__ void bulk_wait_read() {
+    asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
+}
+// Until at most N of this thread's committed bulk groups are incomplete.
+template <int N>
+__device__ __forceinline__ void bulk_wait() {
+    asm volatile("cp.async.bulk.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // Orders this thread's earlier generic-proxy shared-memory accesses before
 // later async-proxy ones (bulk copies into a buffer just read).
 __device__ __forceinline__ void fence_proxy_async_smem() {

@@ -439,6 +439,8 @@ cudaError_t enq_angle(bfpn_ctx* c, void* X, const void* fac) {
     a.nyz = c->nyz;
     a.Ng = c->Ng;
     a.slices_per_block = c->ang_slices;
+    a.err = c->dev_err;
+    a.pairs = c->tr_pairs ? 1 : 0;
     return prof(c, BFPN_KERNEL_ANGLE, [&] { return launch_angle<T>(a, c->stream); });
 }
 

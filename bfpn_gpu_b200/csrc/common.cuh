@@ -83,6 +83,8 @@ struct AngleArgs {
     const T* sine_v;       // [Nmu][Nmu]
     int Nom, Nmu, nyz, Ng;
     int slices_per_block;
+    int* err = nullptr;    // device error word: enables the pipelined kernel (bounded waits report here)
+    int pairs = 0;         // float state: two lines per thread in the pipelined kernel
 };
 
 // Arguments of the factorised catastrophic source.

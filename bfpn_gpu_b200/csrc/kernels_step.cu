@@ -7,6 +7,7 @@
 // ang with consecutive threads, so global accesses are coalesced.
 
 #include "common.cuh"
+#include "async_copy.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -1127,6 +1128,11 @@ __host__ __device__ constexpr int sine_k(int N, int m, int i) {
 }
 __host__ __device__ constexpr bool sine_neg(int N, int m, int i) { return sine_arg(N, m, i) > N + 1; }
 
+// A product rounded on its own (never fused into a following add), so that
+// every DST variant rounds the CN factor step the same way.
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+
 template <int N, typename T>
 __device__ __forceinline__ void dst1(const T (&c)[(N + 1) / 2], const T (&x)[N], T (&y)[N]) {
     constexpr int H = N / 2, HC = (N + 1) / 2;
@@ -1209,7 +1215,7 @@ __global__ void __launch_bounds__(256) angle_dst_kernel(AngleArgs<T> a, SineTabl
         dst1<N, T>(c, x, y);
         const T* fac = Fac + (s >= split ? NA : 0) + mu;
 #pragma unroll
-        for (int k = 0; k < N; ++k) y[k] *= fac[k * N];
+        for (int k = 0; k < N; ++k) y[k] = mul_rn(y[k], fac[k * N]);
         dst1<N, T>(c, y, x);
 #pragma unroll
         for (int k = 0; k < N; ++k) C[k * RS] = x[k];
@@ -1242,6 +1248,292 @@ __global__ void __launch_bounds__(256) angle_dst_kernel(AngleArgs<T> a, SineTabl
     }
 }
 
+// Pipelined form of the same transforms: persistent blocks walk their tiles
+// (SL consecutive slices) through a ring of NST shared buffers.  Thread 0
+// lands each tile with a bulk copy NST - 1 tiles ahead of its use and writes
+// each finished tile back with a bulk store, so HBM traffic overlaps the
+// transforms of the tiles in between.  Slices stay unpadded; rows move as
+// 16-byte vectors when N * sizeof(T) allows.  Waits are bounded: on a
+// timeout the block records an error code, drains its copies and stops.
+template <int N, typename T, int NST>
+__global__ void __launch_bounds__(256) angle_dst_pipe_kernel(AngleArgs<T> a, SineTable<N, T> S, long long n_tiles) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t full[NST];
+    __shared__ int go;
+    constexpr int NA = N * N;
+    const int SL = a.slices_per_block, tid = threadIdx.x;
+    const uint32_t stage_bytes = (static_cast<uint32_t>(SL) * NA * sizeof(T) + 127u) / 128u * 128u;
+    const long long total = static_cast<long long>(a.Ng) * a.nyz;
+    auto tile_of = [&](int i) { return static_cast<long long>(blockIdx.x) + static_cast<long long>(i) * gridDim.x; };
+    auto nslices = [&](long long t) { return static_cast<int>(min(static_cast<long long>(SL), total - t * SL)); };
+    auto buf = [&](int st) { return reinterpret_cast<T*>(smem_raw + st * stage_bytes); };
+    int issued[NST] = {}, landed[NST] = {};  // thread 0's bookkeeping
+    auto issue = [&](int i) {
+        const long long t = tile_of(i);
+        const int st = i % NST;
+        const uint32_t bytes = static_cast<uint32_t>(nslices(t)) * NA * sizeof(T);
+        mbar_expect_tx(&full[st], bytes);
+        bulk_copy_g2s(buf(st), a.F + t * SL * NA, bytes, &full[st]);
+        ++issued[st];
+    };
+    if (tid == 0) {
+        for (int st = 0; st < NST; ++st) mbar_init(&full[st], 1);
+        mbar_init_fence();
+        for (int i = 0; i < NST - 1; ++i)
+            if (tile_of(i) < n_tiles) issue(i);
+        go = 1;
+    }
+    T c[(N + 1) / 2];
+#pragma unroll
+    for (int k = 0; k < (N + 1) / 2; ++k) c[k] = S.c[k];
+    __syncthreads();
+    T x[N], y[N];
+    constexpr bool kVecRows = (N * sizeof(T)) % 16 == 0;
+    using V = typename Vec16<T>::type;
+    constexpr int W = Vec16<T>::W;
+    auto load_row = [&](const T* R) {
+        if constexpr (kVecRows) {
+#pragma unroll
+            for (int v = 0; v < N / W; ++v) {
+                const V val = reinterpret_cast<const V*>(R)[v];
+#pragma unroll
+                for (int k = 0; k < W; ++k) x[v * W + k] = reinterpret_cast<const T*>(&val)[k];
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < N; ++k) x[k] = R[k];
+        }
+    };
+    auto store_row = [&](T* R) {
+        if constexpr (kVecRows) {
+#pragma unroll
+            for (int v = 0; v < N / W; ++v) {
+                V val;
+#pragma unroll
+                for (int k = 0; k < W; ++k) reinterpret_cast<T*>(&val)[k] = y[v * W + k];
+                reinterpret_cast<V*>(R)[v] = val;
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < N; ++k) R[k] = y[k];
+        }
+    };
+    for (int i = 0;; ++i) {
+        const long long t = tile_of(i);
+        if (t >= n_tiles) break;
+        const int st = i % NST;
+        if (tid == 0) {
+            if (tile_of(i + NST - 1) < n_tiles) {
+                bulk_wait_read<0>();  // the store of tile i - 1 has left its stage
+                issue(i + NST - 1);
+            }
+            const bool ok = mbar_wait(&full[st], (i / NST) & 1);
+            if (ok) ++landed[st];
+            go = ok ? 1 : 0;
+        }
+        __syncthreads();
+        if (!go) break;
+        T* X = buf(st);
+        const int ns = nslices(t);
+        const int line = tid;
+        if (line < ns * N) {  // forward u
+            load_row(X + line * N);
+            dst1<N, T>(c, x, y);
+            store_row(X + line * N);
+        }
+        __syncthreads();
+        if (line < ns * N) {  // forward v, factor, inverse v
+            const int sl = line / N, mu = line - sl * N;
+            T* C = X + sl * NA + mu;
+#pragma unroll
+            for (int k = 0; k < N; ++k) x[k] = C[k * N];
+            dst1<N, T>(c, x, y);
+            const long long ek = (t * SL + sl) / a.nyz;
+            const T* __restrict__ fac = a.fac + ek * NA + mu;
+#pragma unroll
+            for (int k = 0; k < N; ++k) y[k] = mul_rn(y[k], __ldg(fac + k * N));
+            dst1<N, T>(c, y, x);
+#pragma unroll
+            for (int k = 0; k < N; ++k) C[k * N] = x[k];
+        }
+        __syncthreads();
+        if (line < ns * N) {  // inverse u
+            load_row(X + line * N);
+            dst1<N, T>(c, x, y);
+            store_row(X + line * N);
+        }
+        __syncthreads();
+        if (tid == 0) {
+            fence_proxy_async_smem();
+            bulk_copy_s2g(a.F + t * SL * NA, X, static_cast<uint32_t>(ns) * NA * sizeof(T));
+            bulk_commit();
+        }
+    }
+    if (tid == 0) {
+        if (!go) {
+            atomicExch(a.err, 3);
+            for (int st = 0; st < NST; ++st)
+                if (issued[st] > landed[st]) mbar_wait(&full[st], (issued[st] - 1) & 1);
+        }
+        bulk_wait<0>();
+    }
+}
+
+// DST-I of two lines at once (fp32x2): the scalar dst1's operations, pairwise.
+template <int N>
+__device__ __forceinline__ void dst1_pair(const float (&c)[(N + 1) / 2], const float2 (&x)[N], float2 (&y)[N]) {
+    constexpr int H = N / 2, HC = (N + 1) / 2;
+    float2 p[HC], q[H > 0 ? H : 1];
+#pragma unroll
+    for (int i = 0; i < H; ++i) {
+        p[i] = __fadd2_rn(x[i], x[N - 1 - i]);
+        q[i] = __ffma2_rn(x[N - 1 - i], make_float2(-1.f, -1.f), x[i]);
+    }
+    if (N & 1) p[H] = x[H];
+#pragma unroll
+    for (int m = 0; m < N; ++m) {
+        float2 acc = make_float2(0.f, 0.f);
+        const int n_terms = (m & 1) ? H : HC;
+#pragma unroll
+        for (int i = 0; i < n_terms; ++i) {
+            const int k = sine_k(N, m, i);
+            if (k == 0) continue;
+            const float cc = sine_neg(N, m, i) ? -c[k - 1] : c[k - 1];
+            acc = __ffma2_rn(make_float2(cc, cc), (m & 1) ? q[i] : p[i], acc);
+        }
+        y[m] = acc;
+    }
+}
+
+// The pipelined DST for float state with two lines per thread: rows r and
+// r + R/2 of a tile's R rows, then adjacent columns (mu, mu + 1) of a slice
+// (N even).  128 threads per block, 2 * 128 / N slices per tile.
+template <int N, int NST>
+__global__ void __launch_bounds__(128) angle_dst_pair_kernel(AngleArgs<float> a, SineTable<N, float> S,
+                                                             long long n_tiles) {
+    static_assert(N % 2 == 0, "column pairs need an even N");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t full[NST];
+    __shared__ int go;
+    constexpr int NA = N * N, NH = N / 2;
+    const int SL = a.slices_per_block, tid = threadIdx.x;
+    const uint32_t stage_bytes = (static_cast<uint32_t>(SL) * NA * 4u + 127u) / 128u * 128u;
+    const long long total = static_cast<long long>(a.Ng) * a.nyz;
+    auto tile_of = [&](int i) { return static_cast<long long>(blockIdx.x) + static_cast<long long>(i) * gridDim.x; };
+    auto nslices = [&](long long t) { return static_cast<int>(min(static_cast<long long>(SL), total - t * SL)); };
+    auto buf = [&](int st) { return reinterpret_cast<float*>(smem_raw + st * stage_bytes); };
+    int issued[NST] = {}, landed[NST] = {};
+    auto issue = [&](int i) {
+        const long long t = tile_of(i);
+        const int st = i % NST;
+        const uint32_t bytes = static_cast<uint32_t>(nslices(t)) * NA * 4u;
+        mbar_expect_tx(&full[st], bytes);
+        bulk_copy_g2s(buf(st), a.F + t * SL * NA, bytes, &full[st]);
+        ++issued[st];
+    };
+    if (tid == 0) {
+        for (int st = 0; st < NST; ++st) mbar_init(&full[st], 1);
+        mbar_init_fence();
+        for (int i = 0; i < NST - 1; ++i)
+            if (tile_of(i) < n_tiles) issue(i);
+        go = 1;
+    }
+    float c[(N + 1) / 2];
+#pragma unroll
+    for (int k = 0; k < (N + 1) / 2; ++k) c[k] = S.c[k];
+    __syncthreads();
+    float2 x[N], y[N];
+    constexpr bool kVecRows = (N * 4) % 16 == 0;
+    auto load_rows = [&](const float* A, const float* B) {
+        if constexpr (kVecRows) {
+#pragma unroll
+            for (int v = 0; v < N / 4; ++v) {
+                const float4 u = reinterpret_cast<const float4*>(A)[v], w = reinterpret_cast<const float4*>(B)[v];
+                x[4 * v] = make_float2(u.x, w.x);
+                x[4 * v + 1] = make_float2(u.y, w.y);
+                x[4 * v + 2] = make_float2(u.z, w.z);
+                x[4 * v + 3] = make_float2(u.w, w.w);
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < N; ++k) x[k] = make_float2(A[k], B[k]);
+        }
+    };
+    auto store_rows = [&](float* A, float* B) {
+        if constexpr (kVecRows) {
+#pragma unroll
+            for (int v = 0; v < N / 4; ++v) {
+                reinterpret_cast<float4*>(A)[v] = make_float4(y[4 * v].x, y[4 * v + 1].x, y[4 * v + 2].x, y[4 * v + 3].x);
+                reinterpret_cast<float4*>(B)[v] = make_float4(y[4 * v].y, y[4 * v + 1].y, y[4 * v + 2].y, y[4 * v + 3].y);
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < N; ++k) {
+                A[k] = y[k].x;
+                B[k] = y[k].y;
+            }
+        }
+    };
+    for (int i = 0;; ++i) {
+        const long long t = tile_of(i);
+        if (t >= n_tiles) break;
+        const int st = i % NST;
+        if (tid == 0) {
+            if (tile_of(i + NST - 1) < n_tiles) {
+                bulk_wait_read<0>();  // the store of tile i - 1 has left its stage
+                issue(i + NST - 1);
+            }
+            const bool ok = mbar_wait(&full[st], (i / NST) & 1);
+            if (ok) ++landed[st];
+            go = ok ? 1 : 0;
+        }
+        __syncthreads();
+        if (!go) break;
+        float* X = buf(st);
+        const int ns = nslices(t), half = ns * NH;  // row pairs = column pairs = ns * N / 2
+        if (tid < half) {  // forward u on rows tid and tid + half
+            load_rows(X + tid * N, X + (tid + half) * N);
+            dst1_pair<N>(c, x, y);
+            store_rows(X + tid * N, X + (tid + half) * N);
+        }
+        __syncthreads();
+        if (tid < half) {  // forward v, factor, inverse v on columns (mu, mu + 1)
+            const int sl = tid / NH, mu = 2 * (tid - sl * NH);
+            float2* C = reinterpret_cast<float2*>(X + sl * NA + mu);
+#pragma unroll
+            for (int k = 0; k < N; ++k) x[k] = C[k * NH];
+            dst1_pair<N>(c, x, y);
+            const long long ek = (t * SL + sl) / a.nyz;
+            const float2* __restrict__ fac = reinterpret_cast<const float2*>(a.fac + ek * NA + mu);
+#pragma unroll
+            for (int k = 0; k < N; ++k) y[k] = __fmul2_rn(y[k], __ldg(fac + k * NH));
+            dst1_pair<N>(c, y, x);
+#pragma unroll
+            for (int k = 0; k < N; ++k) C[k * NH] = x[k];
+        }
+        __syncthreads();
+        if (tid < half) {  // inverse u
+            load_rows(X + tid * N, X + (tid + half) * N);
+            dst1_pair<N>(c, x, y);
+            store_rows(X + tid * N, X + (tid + half) * N);
+        }
+        __syncthreads();
+        if (tid == 0) {
+            fence_proxy_async_smem();
+            bulk_copy_s2g(a.F + t * SL * NA, X, static_cast<uint32_t>(ns) * NA * 4u);
+            bulk_commit();
+        }
+    }
+    if (tid == 0) {
+        if (!go) {
+            atomicExch(a.err, 3);
+            for (int st = 0; st < NST; ++st)
+                if (issued[st] > landed[st]) mbar_wait(&full[st], (issued[st] - 1) & 1);
+        }
+        bulk_wait<0>();
+    }
+}
+
 template <int N, typename T>
 static cudaError_t launch_angle_dst(const AngleArgs<T>& a, cudaStream_t s) {
     SineTable<N, T> S;
@@ -1250,16 +1542,57 @@ static cudaError_t launch_angle_dst(const AngleArgs<T>& a, cudaStream_t s) {
     for (int k = 1; k <= (N + 1) / 2; ++k)
         S.c[k - 1] = static_cast<T>(std::sin(3.14159265358979323846 * k / (N + 1)));
     const int SL = std::max(1, std::min(256 / N, a.nyz));  // at most two groups per block
+    const long long total = static_cast<long long>(a.Ng) * a.nyz;
+    const long long n_tiles = (total + SL - 1) / SL;
+    if constexpr (sizeof(T) == 4 && N % 2 == 0 && N >= 4) {
+        if (a.err && a.pairs) {  // two lines per thread, 128 threads: 2 * 128 / N slices per tile
+            constexpr int NST = 3, SLP = 256 / N;
+            const int SL2 = std::max(1, std::min(SLP, a.nyz));
+            const long long tiles2 = (total + SL2 - 1) / SL2;
+            const size_t stage = (static_cast<size_t>(SL2) * N * N * 4 + 127) / 128 * 128;
+            auto pk = angle_dst_pair_kernel<N, NST>;
+            cudaError_t e = cudaFuncSetAttribute(pk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 static_cast<int>(NST * stage));
+            if (e != cudaSuccess) return e;
+            int dev = 0, sms = 0, per_sm = 0;
+            if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+            if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+            if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pk, 128, NST * stage)) != cudaSuccess)
+                return e;
+            AngleArgs<T> b = a;
+            b.slices_per_block = SL2;
+            const long long grid = std::min<long long>(tiles2, static_cast<long long>(sms) * std::max(per_sm, 1));
+            pk<<<static_cast<unsigned>(grid), 128, NST * stage, s>>>(b, S, tiles2);
+            return cudaGetLastError();
+        }
+    }
+    if (a.err && (N * N) % Vec16<T>::W == 0) {
+        // pipelined: 3 (float) / 2 (double) stages of whole tiles in flight per block
+        constexpr int NST = sizeof(T) == 4 ? 3 : 2;
+        const size_t stage = (static_cast<size_t>(SL) * N * N * sizeof(T) + 127) / 128 * 128;
+        auto pk = angle_dst_pipe_kernel<N, T, NST>;
+        cudaError_t e = cudaFuncSetAttribute(pk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             static_cast<int>(NST * stage));
+        if (e != cudaSuccess) return e;
+        int dev = 0, sms = 0, per_sm = 0;
+        if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+        if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pk, 256, NST * stage)) != cudaSuccess)
+            return e;
+        AngleArgs<T> b = a;
+        b.slices_per_block = SL;
+        const long long grid = std::min<long long>(n_tiles, static_cast<long long>(sms) * std::max(per_sm, 1));
+        pk<<<static_cast<unsigned>(grid), 256, NST * stage, s>>>(b, S, n_tiles);
+        return cudaGetLastError();
+    }
     const size_t smem = (static_cast<size_t>(SL) * N * (N + 1) + 2 * static_cast<size_t>(N) * N) * sizeof(T);
     auto kern = angle_dst_kernel<N, T>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return e;
     AngleArgs<T> b = a;
     b.slices_per_block = SL;
-    const long long total = static_cast<long long>(a.Ng) * a.nyz;
-    const long long blocks = (total + SL - 1) / SL;
-    if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
-    kern<<<static_cast<unsigned>(blocks), 256, smem, s>>>(b, S);
+    if (n_tiles > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+    kern<<<static_cast<unsigned>(n_tiles), 256, smem, s>>>(b, S);
     return cudaGetLastError();
 }
 

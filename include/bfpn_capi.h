@@ -248,10 +248,12 @@ int32_t bfpn_source_groups(bfpn_ctx* ctx);
  *   for one block; 0 uses the general line-walk kernel; a larger value selects
  *   the angles per block (whole planes: 8 or 16 mixed, 4 or 8 FP64; tiles: 4 or
  *   8 mixed, 2 or 4 FP64).  All compute the same values.
- * BFPN_OPT_PAIRED_ANGLES: 1 (default) lets the mixed-precision whole-plane
- *   transport carry two angles per thread on packed fp32x2 arithmetic when NA
- *   is even and the angles of each pair (2i, 2i+1) share the signs of their
- *   direction cosines; 0 keeps one angle per thread.  Same values. */
+ * BFPN_OPT_PAIRED_ANGLES: 1 (default) lets mixed-precision kernels carry
+ *   two lines per thread on packed fp32x2 arithmetic: the whole-plane
+ *   transport two angles (when NA is even and the angles of each pair
+ *   (2i, 2i+1) share the signs of their direction cosines), the angular DST
+ *   two rows / columns of a slice (even Nom = Nmu); 0 keeps one line per
+ *   thread.  Same values. */
 enum { BFPN_OPT_TENSOR_CORES = 0, BFPN_OPT_CUDA_GRAPHS = 1, BFPN_OPT_PLANE_TRANSPORT = 2, BFPN_OPT_PAIRED_ANGLES = 3 };
 bfpn_status bfpn_set_option(bfpn_ctx* ctx, int32_t option, int32_t value);
 

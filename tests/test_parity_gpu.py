@@ -203,6 +203,26 @@ def test_paired_plane_transport_equals_single_angle_kernel(nom, paired):
     assert np.abs(out[(0, 16)][1]).max() > 0
 
 
+@pytest.mark.parametrize("n", [8, 20, 7])
+def test_paired_dst_equals_one_line_per_thread(n):
+    """Mixed-precision angular step: the two-lines-per-thread DST (fp32x2)
+    gives the one-line kernel's values exactly (odd N has no pairs)."""
+    cfg = small_cfg(ny=5, nz=6, nmu=n, nom=n, ng=7)
+    ctx, _ = build(cfg, precision=capi.PREC_MIXED)
+    states = seeded_states(ctx, 13)
+    out = {}
+    for pairs in (1, 0):
+        ctx.set_option(capi.OPT_PAIRED_ANGLES, pairs)
+        for k, arr in enumerate(states):
+            ctx.set_state(k // 2, k % 2, arr)
+        ctx.angle(0, 0, cfg.dt())
+        ctx.angle(1, 1, 0.3 * cfg.dt())
+        out[pairs] = (ctx.get_state(0, 0), ctx.get_state(1, 1))
+    for a, b in zip(out[1], out[0]):
+        assert np.array_equal(a, b)
+    assert not np.array_equal(out[0][0], states[0].astype(np.float32))
+
+
 def test_angle_operator():
     cfg = small_cfg(nmu=7, nom=6)
     ctx, ora = build(cfg)
