@@ -1546,7 +1546,7 @@ static cudaError_t launch_angle_dst(const AngleArgs<T>& a, cudaStream_t s) {
     const long long n_tiles = (total + SL - 1) / SL;
     if constexpr (sizeof(T) == 4 && N % 2 == 0 && N >= 4) {
         if (a.err && a.pairs) {  // two lines per thread, 128 threads: 2 * 128 / N slices per tile
-            constexpr int NST = 3, SLP = 256 / N;
+            constexpr int NST = 2, SLP = 256 / N;  // 2 stages: 5 blocks per SM at N = 20
             const int SL2 = std::max(1, std::min(SLP, a.nyz));
             const long long tiles2 = (total + SL2 - 1) / SL2;
             const size_t stage = (static_cast<size_t>(SL2) * N * N * 4 + 127) / 128 * 128;
@@ -1567,8 +1567,8 @@ static cudaError_t launch_angle_dst(const AngleArgs<T>& a, cudaStream_t s) {
         }
     }
     if (a.err && (N * N) % Vec16<T>::W == 0) {
-        // pipelined: 3 (float) / 2 (double) stages of whole tiles in flight per block
-        constexpr int NST = sizeof(T) == 4 ? 3 : 2;
+        // pipelined: 2 stages of whole tiles per block (more blocks per SM beat deeper rings)
+        constexpr int NST = 2;
         const size_t stage = (static_cast<size_t>(SL) * N * N * sizeof(T) + 127) / 128 * 128;
         auto pk = angle_dst_pipe_kernel<N, T, NST>;
         cudaError_t e = cudaFuncSetAttribute(pk, cudaFuncAttributeMaxDynamicSharedMemorySize,
