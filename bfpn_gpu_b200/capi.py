@@ -34,7 +34,7 @@ FLAG_DOSE_CATASTROPHIC_LOSS = 1 << 11
 FLAG_CALIBRATE_CROSS_SECTIONS = 1 << 12
 FLAG_LITE_MEMORY = 1 << 13
 # run-time options
-OPT_TENSOR_CORES, OPT_CUDA_GRAPHS, OPT_PLANE_TRANSPORT, OPT_PAIRED_ANGLES = 0, 1, 2, 3
+OPT_TENSOR_CORES, OPT_CUDA_GRAPHS, OPT_PLANE_TRANSPORT, OPT_PAIRED_ANGLES, OPT_CLUSTER_TRANSPORT = 0, 1, 2, 3, 4
 # kernel classes of the profile
 KERNEL_CLASSES = ["energy", "transport", "angle", "source_angular", "source_energy", "idd"]
 # tables

@@ -108,6 +108,8 @@ struct bfpn_ctx {
     int tr_plane_ac = 8;
     bool tr_pairs_ok = false;   // angle pairs share direction signs (float whole planes)
     bool tr_pairs = true;       // use the paired kernel where it applies
+    bool tr_cluster_ok = false; // a cluster kernel is compiled for this plane (float state)
+    int tr_cluster = 1;         // 0 off, 1 planes without a whole-plane kernel, 2 every supported plane
     bool tr_tile_ok = false;    // the plane needs tiles: the unrolled tiled kernel applies
     bool tr_tile = false;       // use it
     int tr_tile_ac = 8;
@@ -354,9 +356,16 @@ void choose_plane_transport(bfpn_ctx* c) {
     c->tr_tile_ac = c->elem == 4 ? 8 : 4;
     c->tr_tile_ok = !c->tr_plane_ok && !c->tr_inplace;
     c->tr_tile = c->tr_tile_ok;
+    c->tr_cluster_ok = c->elem == 4 && transport_cluster_supported(c->Ny, c->Nz);
 }
 
-bool transport_in_place(const bfpn_ctx* c) { return c->tr_plane || c->tr_inplace; }
+// The cluster kernel runs this context's transport (it needs paired angles).
+bool cluster_transport(const bfpn_ctx* c) {
+    if (!c->tr_cluster_ok || !c->tr_pairs || !c->tr_pairs_ok) return false;
+    return c->tr_cluster == 2 || (c->tr_cluster == 1 && !c->tr_plane);
+}
+
+bool transport_in_place(const bfpn_ctx* c) { return c->tr_plane || c->tr_inplace || cluster_transport(c); }
 
 template <typename T>
 bfpn_status upload_as(bfpn_ctx* c, void* dst, const double* host, size_t n) {
@@ -420,6 +429,10 @@ cudaError_t enq_transport(bfpn_ctx* c, const void* in, void* out, double dt, boo
     a.tile_z = c->tr_tz;
     a.preserve_sign = preserve_sign ? 1 : 0;
     a.pairs = (c->elem == 4 && c->tr_pairs && c->tr_pairs_ok) ? 1 : 0;
+    if constexpr (sizeof(T) == 4) {
+        if (cluster_transport(c))
+            return prof(c, BFPN_KERNEL_TRANSPORT, [&] { return launch_transport_cluster(a, c->stream); });
+    }
     if (c->tr_plane)
         return prof(c, BFPN_KERNEL_TRANSPORT, [&] { return launch_transport_plane<T>(a, c->tr_plane_ac, c->stream); });
     if (c->tr_tile && a.in != a.out)
@@ -1189,6 +1202,12 @@ bfpn_status bfpn_set_option(bfpn_ctx* c, int32_t option, int32_t value) {
             break;
         case BFPN_OPT_PAIRED_ANGLES:
             c->tr_pairs = value != 0;
+            break;
+        case BFPN_OPT_CLUSTER_TRANSPORT:
+            if (value < 0 || value > 2) return fail(c, BFPN_INVALID_ARG, "cluster transport: 0, 1 or 2");
+            if (value == 2 && !c->tr_cluster_ok)
+                return fail(c, BFPN_INVALID_ARG, "no cluster transport kernel for this plane size / precision");
+            c->tr_cluster = value;
             break;
         case BFPN_OPT_PLANE_TRANSPORT: {
             const bool f32 = c->elem == 4;

@@ -184,6 +184,11 @@ bool transport_plane_supported(int Ny, int Nz);
 // True when NA is even and angles (2i, 2i+1) share the signs of omega_y and
 // omega_z ([NA][2] table): the float whole-plane kernel may then pair them.
 bool transport_pairs_ok(const double* omega, int NA);
+// Float state, paired angles, square planes of the compiled sizes
+// (transport_cluster_supported): one thread-block cluster per (group,
+// 8-angle chunk) plane, in place.
+cudaError_t launch_transport_cluster(const TransportArgs<float>& a, cudaStream_t s);
+bool transport_cluster_supported(int Ny, int Nz);
 // Any plane, in 27 x 27 output tiles with a 4-cell halo, out of place;
 // ang_chunk 4 or 8 (float), 2 or 4 (double).
 template <typename T> cudaError_t launch_transport_tiles(const TransportArgs<T>& a, int ang_chunk, cudaStream_t s);

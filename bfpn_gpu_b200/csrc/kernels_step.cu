@@ -9,6 +9,8 @@
 #include "common.cuh"
 #include "async_copy.cuh"
 
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -788,6 +790,242 @@ __global__ void __launch_bounds__((NP * AC / 2 + 31) / 32 * 32) transport_plane_
     }
 }
 
+// ---------------------------------------------------------------------------
+// Planes too large for one block (float state, paired angles): a cluster of
+// CL CTAs holds one (group, 2*A2-angle chunk) plane, CTA r the z rows
+// [r NP / CL, (r+1) NP / CL) of both shared planes (F, then H; the y-part of
+// div F, then the predictor P).  No cell is computed twice.  Row walks are
+// local: a row is cut into YS segments, each walked by its own thread from
+// its cells plus 2 either side.  Column walks take their band plus 2 rows
+// either side: in stage 1 those rows come from the input in HBM, in stage 2
+// from the neighbouring CTAs' predictor rows (distributed shared memory),
+// behind a cluster barrier whose arrive follows each CTA's stage 1 and whose
+// wait precedes its stage 2.  Cells beyond the plane repeat the edge value
+// (the reference's clamped indices), which also yields D = 0 at the boundary
+// face.  Per cell the arithmetic is the whole-plane kernel's.
+// ---------------------------------------------------------------------------
+template <int NP, int CL, int A2>
+struct ClusterPlane {
+    static constexpr int N = NP - 1;
+    static constexpr int BZ = (NP + CL - 1) / CL;         // rows of the largest band
+    static constexpr int YS = (NP + BZ - 1) / BZ;         // row segments
+    static constexpr int YT = (BZ * A2 + 31) / 32 * 32;   // threads per row segment
+    static constexpr int NT = (NP * A2 > YS * YT ? (NP * A2 + 31) / 32 * 32 : YS * YT);
+    static constexpr int RS = NP * A2;                    // row stride (float2)
+    static constexpr size_t smem = 2ull * BZ * RS * sizeof(float2);
+};
+
+// One line of faces: D(j) = wr (G(j) - G(j-1)), G(j) = x_j + h sb(x_j - x_{j-1},
+// x_{j+1} - x_j), over values x_k = get(k), k = 0 .. L-1, standing for
+// X(first - 2) .. X(first + L - 3); emit(i, d, X(first + i - 1), X(first + i))
+// for face first + i, i = 0 .. L-4.  get(k) is called kPrefetch steps ahead of
+// its use, in program order before the emits in between (which only store to
+// cells already read).
+template <int L, typename Get, typename Emit>
+__device__ __forceinline__ void walk_get2(const Get& get, float2 wr, float2 h, const Emit& emit) {
+    float2 x[L];
+#pragma unroll
+    for (int k = 0; k < L && k < kPrefetch + 3; ++k) x[k] = get(k);
+    float2 back = sub2(x[1], x[0]);
+    float2 fwd = sub2(x[2], x[1]);
+    float2 gp = __ffma2_rn(h, superbee_diff2(back, fwd), x[1]);  // G(first - 1)
+#pragma unroll
+    for (int i = 0; i + 4 <= L; ++i) {
+        if (i + 3 + kPrefetch < L) x[i + 3 + kPrefetch] = get(i + 3 + kPrefetch);
+        back = fwd;
+        fwd = sub2(x[i + 3], x[i + 2]);
+        const float2 g = __ffma2_rn(h, superbee_diff2(back, fwd), x[i + 2]);
+        emit(i, __fmul2_rn(wr, sub2(g, gp)), x[i + 1], x[i + 2]);
+        gp = g;
+    }
+}
+
+// Row segment [C0, C1) of a row at X (stride A2): faces C0 .. C1, cell = face - s.
+template <int N, int C0, int C1, int A2, typename Emit>
+__device__ __forceinline__ void walk_row_segment(const float2* X, float2 wr, float2 h, int s, const Emit& emit) {
+    constexpr int L = C1 - C0 + 4;
+    walk_get2<L>([&](int k) { return X[min(max(C0 - 2 + k, 0), N) * A2]; }, wr, h,
+                 [&](int i, float2 d, float2, float2) {
+                     const int cell = C0 + i - s;
+                     if (cell >= C0 && cell < C1) emit(cell, d);
+                 });
+}
+
+template <int N, int YS, int K, int A2, typename Emit>
+__device__ __forceinline__ void walk_row_dispatch(int seg, const float2* X, float2 wr, float2 h, int s,
+                                                  const Emit& emit) {
+    if constexpr (K < YS) {
+        if (seg == K) {
+            walk_row_segment<N, K * (N + 1) / YS, (K + 1) * (N + 1) / YS, A2>(X, wr, h, s, emit);
+            return;
+        }
+        walk_row_dispatch<N, YS, K + 1, A2>(seg, X, wr, h, s, emit);
+    }
+}
+
+// Column over a band of B rows at Xb (stride RS) with 2 rows either side in
+// registers: faces z0 .. z0 + B, cell (band row) = face - z0 - s; emit gets
+// the X value of the cell as its third argument.
+template <int B, int RS, typename Emit>
+__device__ __forceinline__ void walk_band_column(const float2* Xb, const float2 (&below)[2], const float2 (&above)[2],
+                                                 float2 wr, float2 h, int s, const Emit& emit) {
+    walk_get2<B + 4>(
+        [&](int k) { return k < 2 ? below[k] : (k < B + 2 ? Xb[(k - 2) * RS] : above[k - B - 2]); }, wr, h,
+        [&](int i, float2 d, float2 xm, float2 x0) {
+            const int cell = i - s;
+            if (cell >= 0 && cell < B) emit(cell, d, s ? xm : x0);
+        });
+}
+
+template <int NP, int CL, int A2>
+__global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(ClusterPlane<NP, CL, A2>::NT)
+    transport_cluster_kernel(TransportArgs<float> a, int n_chunks) {
+    using S = ClusterPlane<NP, CL, A2>;
+    constexpr int N = S::N, BZ = S::BZ, RS = S::RS, AC = 2 * A2;
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float2* Fs = reinterpret_cast<float2*>(smem_raw);
+    float2* Ps = Fs + BZ * RS;
+    const int rank = static_cast<int>(cluster.block_rank());
+    const int plane_id = blockIdx.x / CL;
+    const int chunk = plane_id % n_chunks, ek = plane_id / n_chunks;
+    const int z0 = rank * NP / CL, z1 = (rank + 1) * NP / CL, B = z1 - z0;
+    const int NA = a.NA, a0 = chunk * AC;
+    const size_t zs = static_cast<size_t>(NP) * NA;  // one z row in the state
+    const float* in = a.in + static_cast<size_t>(ek) * NP * zs + a0;
+    float* out = a.out + static_cast<size_t>(ek) * NP * zs + a0;
+    const int tid = threadIdx.x;
+
+    // column items: (column cy, pair cq); row items: (segment, band row rz, pair rq)
+    const int cq = tid % A2, cy = tid / A2;
+    const int seg = tid / S::YT, rr = tid % S::YT, rq = rr % A2, rz = rr / A2;
+    auto pair_setup = [&](int q, float2& wry, float2& wrz, float2& hy, float2& hz, int& sy, int& sz, bool& ok0,
+                          bool& ok1) {
+        ok0 = a0 + 2 * q < NA;
+        ok1 = a0 + 2 * q + 1 < NA;
+        const int g0 = min(a0 + 2 * q, NA - 1), g1 = min(a0 + 2 * q + 1, NA - 1);
+        const float wy0 = a.omega[2 * g0], wz0 = a.omega[2 * g0 + 1];
+        const float wy1 = a.omega[2 * g1], wz1 = a.omega[2 * g1 + 1];
+        wry = make_float2(wy0 / a.dy, wy1 / a.dy);
+        wrz = make_float2(wz0 / a.dz, wz1 / a.dz);
+        hy = wy0 < 0.f ? make_float2(-0.5f, -0.5f) : make_float2(0.5f, 0.5f);
+        hz = wz0 < 0.f ? make_float2(-0.5f, -0.5f) : make_float2(0.5f, 0.5f);
+        sy = wy0 < 0.f ? 1 : 0;
+        sz = wz0 < 0.f ? 1 : 0;
+    };
+    const float2 ndt = make_float2(-a.dt, -a.dt), nhdt = make_float2(-0.5f * a.dt, -0.5f * a.dt);
+    const float lo = a.preserve_sign ? -INFINITY : 0.f;
+    const bool col_item = cy < NP;
+    const bool row_item = seg < S::YS && rz < B;
+
+    // stage 0: the band of F; column items also take F 2 rows either side (clamped to the plane)
+    float* Fsf = reinterpret_cast<float*>(Fs);
+    if (NA % 4 == 0) {
+        for (int v = tid; v < B * NP * (AC / 4); v += S::NT) {
+            const int hp = v % (AC / 4), p = v / (AC / 4);
+            float4 val{};
+            if (a0 + 4 * hp < NA)
+                val = *reinterpret_cast<const float4*>(in + static_cast<size_t>(z0 * NP + p) * NA + 4 * hp);
+            *reinterpret_cast<float4*>(Fsf + p * (2 * A2) + 4 * hp) = val;
+        }
+    } else {
+        for (int v = tid; v < B * NP * A2; v += S::NT) {
+            const int q = v % A2, p = v / A2;
+            float2 val{};
+            if (a0 + 2 * q < NA)
+                val = *reinterpret_cast<const float2*>(in + static_cast<size_t>(z0 * NP + p) * NA + 2 * q);
+            Fs[p * A2 + q] = val;
+        }
+    }
+    float2 fb[2] = {}, fa[2] = {};
+    if (col_item && a0 + 2 * cq < NA) {
+        const float* col = in + static_cast<size_t>(cy) * NA + 2 * cq;
+        fb[0] = *reinterpret_cast<const float2*>(col + max(z0 - 2, 0) * zs);
+        fb[1] = *reinterpret_cast<const float2*>(col + max(z0 - 1, 0) * zs);
+        fa[0] = *reinterpret_cast<const float2*>(col + min(z1, N) * zs);
+        fa[1] = *reinterpret_cast<const float2*>(col + min(z1 + 1, N) * zs);
+    }
+    __syncthreads();
+    // stage 1, y-part of div F (rows) into Ps
+    if (row_item) {
+        float2 wry, wrz, hy, hz;
+        int sy, sz;
+        bool ok0, ok1;
+        pair_setup(rq, wry, wrz, hy, hz, sy, sz, ok0, ok1);
+        float2* D = Ps + rz * RS + rq;
+        walk_row_dispatch<N, S::YS, 0, A2>(seg, Fs + rz * RS + rq, wry, hy, sy,
+                                           [&](int cell, float2 d) { D[cell * A2] = d; });
+    }
+    __syncthreads();
+    // stage 1, z-part (columns): predictor into Ps, H over F
+    if (col_item) {
+        float2 wry, wrz, hy, hz;
+        int sy, sz;
+        bool ok0, ok1;
+        pair_setup(cq, wry, wrz, hy, hz, sy, sz, ok0, ok1);
+        float2* Pc = Ps + cy * A2 + cq;
+        float2* Xc = Fs + cy * A2 + cq;
+        auto emit = [&](int cell, float2 dz, float2 f) {
+            const float2 d = __fadd2_rn(Pc[cell * RS], dz);
+            Pc[cell * RS] = max_lo2(__ffma2_rn(ndt, d, f), lo);
+            Xc[cell * RS] = __ffma2_rn(nhdt, d, f);
+        };
+        if (B == BZ) walk_band_column<BZ, RS>(Xc, fb, fa, wrz, hz, sz, emit);
+        else walk_band_column<BZ - 1, RS>(Xc, fb, fa, wrz, hz, sz, emit);
+    }
+    cluster.barrier_arrive();  // this CTA's predictor rows are final
+    __syncthreads();
+    // stage 2, y-part of div P (rows): H - dt/2 d_y P over F
+    if (row_item) {
+        float2 wry, wrz, hy, hz;
+        int sy, sz;
+        bool ok0, ok1;
+        pair_setup(rq, wry, wrz, hy, hz, sy, sz, ok0, ok1);
+        float2* Fe = Fs + rz * RS + rq;
+        walk_row_dispatch<N, S::YS, 0, A2>(
+            seg, Ps + rz * RS + rq, wry, hy, sy,
+            [&](int cell, float2 d) { Fe[cell * A2] = __ffma2_rn(nhdt, d, Fe[cell * A2]); });
+    }
+    __syncthreads();
+    cluster.barrier_wait();  // the neighbours' predictor rows are final
+    // stage 2, z-part (columns) and the corrector, to HBM
+    if (col_item) {
+        float2 wry, wrz, hy, hz;
+        int sy, sz;
+        bool ok0, ok1;
+        pair_setup(cq, wry, wrz, hy, hz, sy, sz, ok0, ok1);
+        const int off = cy * A2 + cq;
+        float2 pb[2], pa[2];
+        if (rank > 0) {
+            const int Bm = z0 - (rank - 1) * NP / CL;  // rows of the band below
+            const float2* rem = cluster.map_shared_rank(Ps, rank - 1);
+            pb[0] = rem[(Bm - 2) * RS + off];
+            pb[1] = rem[(Bm - 1) * RS + off];
+        } else {
+            pb[0] = pb[1] = Ps[off];
+        }
+        if (rank < CL - 1) {
+            const float2* rem = cluster.map_shared_rank(Ps, rank + 1);
+            pa[0] = rem[off];
+            pa[1] = rem[RS + off];
+        } else {
+            pa[0] = pa[1] = Ps[(B - 1) * RS + off];
+        }
+        const float2* Fc = Fs + off;
+        float* o = out + static_cast<size_t>(z0) * zs + static_cast<size_t>(cy) * NA + 2 * cq;
+        auto emit = [&](int cell, float2 d, float2) {
+            const float2 v = max_lo2(__ffma2_rn(nhdt, d, Fc[cell * RS]), lo);
+            float* dst = o + cell * zs;
+            if (ok1) *reinterpret_cast<float2*>(dst) = v;
+            else if (ok0) *dst = v.x;
+        };
+        if (B == BZ) walk_band_column<BZ, RS>(Ps + off, pb, pa, wrz, hz, sz, emit);
+        else walk_band_column<BZ - 1, RS>(Ps + off, pb, pa, wrz, hz, sz, emit);
+    }
+    cluster.sync();  // no CTA leaves while a neighbour still reads its rows
+}
+
 // The packed kernel applies when NA is even (8-byte aligned pairs) and the
 // two angles of every pair share the signs of omega_y and omega_z.
 bool transport_pairs_ok(const double* omega, int NA) {
@@ -977,6 +1215,46 @@ cudaError_t launch_transport_tiles(const TransportArgs<T>& a, int ang_chunk, cud
         if (ang_chunk == 4) return launch_tile_ac<T, 4>(a, s);
     }
     return cudaErrorInvalidValue;
+}
+
+// Plane sizes (Ny+1 = Nz+1) and cluster sizes of the compiled cluster kernel
+// (8 angles per plane chunk; bands of NP / CL rows).
+#define BFPN_CLUSTER_PLANES(X) X(21, 2) X(41, 2) X(49, 4) X(65, 4) X(81, 4) X(97, 8) X(129, 8)
+
+bool transport_cluster_supported(int Ny, int Nz) {
+    if (Ny != Nz) return false;
+    switch (Ny + 1) {
+#define BFPN_CASE(NP, CL) case NP:
+        BFPN_CLUSTER_PLANES(BFPN_CASE)
+#undef BFPN_CASE
+        return true;
+        default: return false;
+    }
+}
+
+template <int NP, int CL>
+static cudaError_t launch_cluster_np(const TransportArgs<float>& a, cudaStream_t s) {
+    constexpr int A2 = 4, AC = 2 * A2;
+    using S = ClusterPlane<NP, CL, A2>;
+    const int n_chunks = (a.NA + AC - 1) / AC;
+    auto kern = transport_cluster_kernel<NP, CL, A2>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::smem));
+    if (e != cudaSuccess) return e;
+    const long long blocks = static_cast<long long>(a.Ng) * n_chunks * CL;
+    if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+    kern<<<static_cast<unsigned>(blocks), S::NT, S::smem, s>>>(a, n_chunks);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_transport_cluster(const TransportArgs<float>& a, cudaStream_t s) {
+    if (a.Ny != a.Nz || a.NA % 2 != 0 || !a.pairs) return cudaErrorNotSupported;
+    switch (a.Ny + 1) {
+#define BFPN_CASE(NP, CL) \
+    case NP: return launch_cluster_np<NP, CL>(a, s);
+        BFPN_CLUSTER_PLANES(BFPN_CASE)
+#undef BFPN_CASE
+        default: return cudaErrorNotSupported;
+    }
 }
 
 // Plane sizes (Ny+1 = Nz+1) with a compiled whole-plane kernel.

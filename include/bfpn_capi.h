@@ -253,8 +253,21 @@ int32_t bfpn_source_groups(bfpn_ctx* ctx);
  *   transport two angles (when NA is even and the angles of each pair
  *   (2i, 2i+1) share the signs of their direction cosines), the angular DST
  *   two rows / columns of a slice (even Nom = Nmu); 0 keeps one line per
- *   thread.  Same values. */
-enum { BFPN_OPT_TENSOR_CORES = 0, BFPN_OPT_CUDA_GRAPHS = 1, BFPN_OPT_PLANE_TRANSPORT = 2, BFPN_OPT_PAIRED_ANGLES = 3 };
+ *   thread.  Same values.
+ * BFPN_OPT_CLUSTER_TRANSPORT: 1 (default) runs the mixed-precision transport
+ *   of square planes with Ny = Nz in {40,48,64,80,96,128} (paired angles) on
+ *   thread-block clusters: 2 to 8 CTAs hold one plane in their shared memory
+ *   and exchange edge rows through distributed shared memory, in place;
+ *   2 also uses it for Ny = Nz = 20 (in place of the whole-plane kernel);
+ *   0 leaves those planes to the tiled kernel.  Values agree with the other
+ *   kernels to float rounding. */
+enum {
+    BFPN_OPT_TENSOR_CORES = 0,
+    BFPN_OPT_CUDA_GRAPHS = 1,
+    BFPN_OPT_PLANE_TRANSPORT = 2,
+    BFPN_OPT_PAIRED_ANGLES = 3,
+    BFPN_OPT_CLUSTER_TRANSPORT = 4
+};
 bfpn_status bfpn_set_option(bfpn_ctx* ctx, int32_t option, int32_t value);
 
 /* bfpn_step_async(nsteps) bracketed by CUDA events on the context stream;

@@ -223,6 +223,45 @@ def test_paired_dst_equals_one_line_per_thread(n):
     assert not np.array_equal(out[0][0], states[0].astype(np.float32))
 
 
+def _transport_states(ctx, cfg, seed, opts):
+    states = seeded_states(ctx, seed)
+    for k, v in opts.items():
+        ctx.set_option(k, v)
+    for k, arr in enumerate(states):
+        ctx.set_state(k // 2, k % 2, arr)
+    ctx.transport(0, 0, 0.5 * cfg.dt(), False)
+    ctx.transport(0, 1, 0.5 * cfg.dt(), True)
+    ctx.transport(1, 0, 0.31 * cfg.dt(), False)
+    return [ctx.get_state(sp, cf) for sp, cf in ((0, 0), (0, 1), (1, 0))]
+
+
+def test_cluster_transport_matches_whole_plane_kernel():
+    """Thread-block-cluster transport (2 CTAs holding one 21 x 21 plane, edge
+    rows over distributed shared memory) against the whole-plane kernel."""
+    cfg = small_cfg(ny=20, nz=20, nmu=6, nom=8, ng=5, lz=2.0)
+    ctx, _ = build(cfg, precision=capi.PREC_MIXED)
+    a = _transport_states(ctx, cfg, 21, {capi.OPT_CLUSTER_TRANSPORT: 2})
+    b = _transport_states(ctx, cfg, 21, {capi.OPT_CLUSTER_TRANSPORT: 0})
+    for x, y in zip(a, b):
+        assert rel_err(x, y) < 1e-6
+
+
+@pytest.mark.parametrize("n", [40, 48, 80])
+def test_cluster_transport_matches_tiled_kernel(n):
+    """Large planes: the cluster kernel (2 or 4 CTAs per plane) against the
+    tiled kernel (27 x 27 tiles with recomputed halos) and the line walks."""
+    cfg = small_cfg(ny=n, nz=n, nmu=4, nom=4, ng=2, ly=16.0, lz=16.0)
+    ctx, _ = build(cfg, precision=capi.PREC_MIXED)
+    a = _transport_states(ctx, cfg, 22, {capi.OPT_CLUSTER_TRANSPORT: 1})
+    b = _transport_states(ctx, cfg, 22, {capi.OPT_CLUSTER_TRANSPORT: 0})
+    c = _transport_states(ctx, cfg, 22, {capi.OPT_CLUSTER_TRANSPORT: 0, capi.OPT_PLANE_TRANSPORT: 0})
+    for x, y, z in zip(a, b, c):
+        assert rel_err(x, y) < 1e-6
+        assert rel_err(x, z) < 2e-6
+    with pytest.raises(capi.BfpnError):
+        ctx.set_option(capi.OPT_CLUSTER_TRANSPORT, 3)
+
+
 def test_angle_operator():
     cfg = small_cfg(nmu=7, nom=6)
     ctx, ora = build(cfg)
