@@ -176,11 +176,11 @@ def kernel_bytes(cls, cells, elem, n_groups, nyz, NA):
 # the same kernels on this workload with 250 groups (profiles/*_water230_ng250.txt), mixed
 # precision; traffic grows in proportion to the cells, so a full launch is this times cells.
 NCU_DRAM_BYTES_PER_CELL = {
-    "transport": (176.44e6 + 122.67e6) / 44.1e6,
-    "angle": (176.83e6 + 118.22e6) / 44.1e6,
-    "energy": (352.90e6 + 295.08e6) / 44.1e6,
-    "source_angular": (286.05e6 + 155.84e6) / 44.1e6,
-    "source_energy": (221.78e6 + 146.64e6) / 44.1e6,
+    "transport": (176.52e6 + 122.73e6) / 44.1e6,
+    "angle": (176.85e6 + 119.49e6) / 44.1e6,
+    "energy": (352.90e6 + 295.12e6) / 44.1e6,
+    "source_angular": (190.52e6 + 153.69e6 + 284.85e6 + 154.88e6) / 44.1e6,  # pack + GEMM
+    "source_energy": (249.24e6 + 132.63e6) / 44.1e6,
 }
 
 
