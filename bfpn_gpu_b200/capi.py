@@ -33,8 +33,10 @@ FLAG_TRAPEZOIDAL_YZ = 1 << 10
 FLAG_DOSE_CATASTROPHIC_LOSS = 1 << 11
 FLAG_CALIBRATE_CROSS_SECTIONS = 1 << 12
 FLAG_LITE_MEMORY = 1 << 13
+FLAG_STREAMING_FULL = 1 << 14
 # run-time options
-OPT_TENSOR_CORES, OPT_CUDA_GRAPHS, OPT_PLANE_TRANSPORT, OPT_PAIRED_ANGLES, OPT_CLUSTER_TRANSPORT = 0, 1, 2, 3, 4
+(OPT_TENSOR_CORES, OPT_CUDA_GRAPHS, OPT_PLANE_TRANSPORT, OPT_PAIRED_ANGLES, OPT_CLUSTER_TRANSPORT, OPT_LANE_CHUNK,
+ OPT_ENERGY_CHUNK) = range(7)
 # kernel classes of the profile
 KERNEL_CLASSES = ["energy", "transport", "angle", "source_angular", "source_energy", "idd"]
 # tables

@@ -53,6 +53,8 @@ class RunConfig:
     energy_density: float = 1.0
     lite_memory: bool = False
     streaming_full: bool = False
+    lane_chunk: int = 262144
+    energy_chunk: int = 128
     primary_only: bool = False
     legacy_energy: bool = False
     eq15_straggling: bool = False
@@ -93,7 +95,8 @@ class RunConfig:
                           (self.trapezoidal_yz, capi.FLAG_TRAPEZOIDAL_YZ),
                           (self.dose_catastrophic_loss, capi.FLAG_DOSE_CATASTROPHIC_LOSS),
                           (self.calibrate_cross_sections, capi.FLAG_CALIBRATE_CROSS_SECTIONS),
-                          (self.lite_memory, capi.FLAG_LITE_MEMORY)):
+                          (self.lite_memory, capi.FLAG_LITE_MEMORY),
+                          (self.streaming_full, capi.FLAG_STREAMING_FULL)):
             if cond:
                 f |= bit
         return f
@@ -204,8 +207,12 @@ def parse_args(argv):
             c.calibrate_cross_sections = True
         elif a == "--sigma-yz" and has:
             c.sigma_yz = float(nxt())
-        elif a in ("--lane-chunk", "--energy-chunk", "--stream-dir") and has:
-            nxt()  # streaming-mode tuning; the state is HBM resident here
+        elif a == "--lane-chunk" and has:
+            c.lane_chunk = int(nxt())
+        elif a == "--energy-chunk" and has:
+            c.energy_chunk = int(nxt())
+        elif a == "--stream-dir" and has:
+            nxt()  # the reference's backing-file directory; the out-of-core state is in pinned host memory
         elif a == "--idd-stride" and has:
             c.idd_stride = max(1, int(nxt()))
         elif a == "--spot-depths" and has:

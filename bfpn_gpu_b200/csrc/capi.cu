@@ -91,6 +91,15 @@ struct bfpn_ctx {
     double* moments = nullptr;      // [Ng][2]
     double* plane = nullptr;        // [nyz] spot dose plane
     bool lite = false;              // lite-memory mode: psi^1 of the primary only
+    // out-of-core mode: st[][] are pinned host arrays; device chunk buffers
+    bool ooc = false;
+    int ooc_lane_req = 262144, ooc_group_req = 128;  // requested chunk sizes (lanes, groups)
+    int lc_pos = 0, lc = 0, n_lc = 0, ecg = 0;        // positions / lanes per lane chunk, lane chunks, groups per group chunk
+    bool ooc_ready = false;
+    void* dl[4] = {nullptr, nullptr, nullptr, nullptr};  // lane chunk: the species' psi^1, psi^2; the primary's for the source
+    void* dgc = nullptr;                                 // group chunk
+    void* ooc_part = nullptr;                            // IDD partials of every lane chunk, both species
+    std::vector<void*> host_allocs;
     double* lite_coef = nullptr;    // [Ng][2] lite step constants
 
     BeamTables tables;
@@ -307,6 +316,8 @@ void free_all(bfpn_ctx* c) {
     c->graph_exec = nullptr;
     for (auto& b : c->allocs) cudaFree(b.p);
     c->allocs.clear();
+    for (void* p : c->host_allocs) cudaFreeHost(p);
+    c->host_allocs.clear();
 }
 
 // Transport launch shape: a whole (Ny+1) x (Nz+1) plane per block when it
@@ -412,8 +423,9 @@ cudaError_t enq_energy(bfpn_ctx* c, int species, const double* coef, bool with_s
     return prof(c, BFPN_KERNEL_ENERGY, [&] { return launch_energy<T>(a, c->energy_block, c->stream); });
 }
 
+// ng >= 0: the arrays hold ng groups (a chunk of the out-of-core mode).
 template <typename T>
-cudaError_t enq_transport(bfpn_ctx* c, const void* in, void* out, double dt, bool preserve_sign) {
+cudaError_t enq_transport(bfpn_ctx* c, const void* in, void* out, double dt, bool preserve_sign, int ng = -1) {
     TransportArgs<T> a;
     a.in = as<const T>(const_cast<void*>(in));
     a.out = as<T>(out);
@@ -421,7 +433,7 @@ cudaError_t enq_transport(bfpn_ctx* c, const void* in, void* out, double dt, boo
     a.Ny = c->Ny;
     a.Nz = c->Nz;
     a.NA = c->NA;
-    a.Ng = c->Ng;
+    a.Ng = ng >= 0 ? ng : c->Ng;
     a.dt = static_cast<T>(dt);
     a.dy = static_cast<T>(c->d.dy);
     a.dz = static_cast<T>(c->d.dz);
@@ -441,7 +453,7 @@ cudaError_t enq_transport(bfpn_ctx* c, const void* in, void* out, double dt, boo
 }
 
 template <typename T>
-cudaError_t enq_angle(bfpn_ctx* c, void* X, const void* fac) {
+cudaError_t enq_angle(bfpn_ctx* c, void* X, const void* fac, int ng = -1) {
     AngleArgs<T> a;
     a.F = as<T>(X);
     a.fac = as<const T>(const_cast<void*>(fac));
@@ -450,53 +462,62 @@ cudaError_t enq_angle(bfpn_ctx* c, void* X, const void* fac) {
     a.Nom = c->Nom;
     a.Nmu = c->Nmu;
     a.nyz = c->nyz;
-    a.Ng = c->Ng;
+    a.Ng = ng >= 0 ? ng : c->Ng;
     a.slices_per_block = c->ang_slices;
     a.err = c->dev_err;
     a.pairs = c->tr_pairs ? 1 : 0;
     return prof(c, BFPN_KERNEL_ANGLE, [&] { return launch_angle<T>(a, c->stream); });
 }
 
+// The source from primary arrays P1, P2 of nyz positions (row stride
+// nyz * NA) into S; A1 / A2 (and the tensor-core operand) in the context's
+// A block, sized for those positions.
 template <typename T>
-cudaError_t enq_source(bfpn_ctx* c) {
+cudaError_t enq_source_on(bfpn_ctx* c, const void* P1, const void* P2, void* S, int nyz) {
     SourceArgs<T> a;
-    a.P1 = as<const T>(c->st[0][0]);
-    a.P2 = as<const T>(c->st[0][1]);
+    a.P1 = as<const T>(const_cast<void*>(P1));
+    a.P2 = as<const T>(const_cast<void*>(P2));
     a.ker_v = as<const T>(c->ker_v);
     a.groups = c->groups;
     a.n_groups = c->n_groups;
     a.A1 = as<T>(c->A1);
     a.A2 = as<T>(c->A2);
-    a.S = as<T>(c->src);
+    a.S = as<T>(S);
     a.e1 = c->e1;
     a.e2 = c->e2;
     a.tile_lo = c->tile_lo;
     a.tile_hi = c->tile_hi;
     a.Ng = c->Ng;
-    a.nyz = c->nyz;
+    a.nyz = nyz;
     a.NA = c->NA;
     a.dg = c->d.dg;
+    const long long per_e = static_cast<long long>(nyz) * c->NA;
     cudaError_t e;
     if (sizeof(T) == sizeof(float) && c->use_umma && c->bblob && c->ablob && c->eblob) {
         // tensor cores: the angular stage writes the energy stage's split-bf16
         // operand into the A block, the energy stage reads it
         uint8_t* q = static_cast<uint8_t*>(c->A1);
         e = prof(c, BFPN_KERNEL_SOURCE_ANGULAR, [&] {
-            return launch_source_angular_pipe(as<const float>(c->st[0][0]), as<const float>(c->st[0][1]),
+            return launch_source_angular_pipe(as<const float>(const_cast<void*>(P1)),
+                                              as<const float>(const_cast<void*>(P2)),
                                               static_cast<uint8_t*>(c->ablob), static_cast<const uint8_t*>(c->bblob),
-                                              c->groups, c->n_groups, q, c->Ng, c->dev_err, c->nyz, c->NA,
+                                              c->groups, c->n_groups, q, c->Ng, c->dev_err, nyz, c->NA,
                                               c->umma_nt, c->umma_bk, c->umma_ntiles, c->stream);
         });
         if (e != cudaSuccess) return e;
         return prof(c, BFPN_KERNEL_SOURCE_ENERGY, [&] {
             return launch_source_energy_umma(q, static_cast<const uint8_t*>(c->eblob), c->ework, c->ework_begin,
-                                             c->e_et, c->e_emax, as<float>(c->src), c->dev_err, c->per_e, c->Ng,
-                                             c->stream);
+                                             c->e_et, c->e_emax, as<float>(S), c->dev_err, per_e, c->Ng, c->stream);
         });
     }
     e = prof(c, BFPN_KERNEL_SOURCE_ANGULAR, [&] { return launch_source_angular<T>(a, c->stream); });
     if (e != cudaSuccess) return e;
     return prof(c, BFPN_KERNEL_SOURCE_ENERGY, [&] { return launch_source_energy<T>(a, c->tile_e, c->stream); });
+}
+
+template <typename T>
+cudaError_t enq_source(bfpn_ctx* c) {
+    return enq_source_on<T>(c, c->st[0][0], c->st[0][1], c->src, c->nyz);
 }
 
 // transport half-step, angle full step, transport half-step on one array
@@ -592,6 +613,180 @@ cudaError_t enq_step_any(bfpn_ctx* c, bool first, bool secondary_zero) {
                                      : enq_step<float>(c, first, secondary_zero);
 }
 
+// ---------------------------------------------------------------------------
+// Out-of-core mode (BFPN_FLAG_STREAMING_FULL; the reference's
+// solveStreamingFull, bfpm_solver.cu:3113-3236, with its backing files
+// replaced by pinned host memory).  The operators split two ways: the energy
+// sweep and the source are local to a lane (position, angle), so they run on
+// lane chunks -- every group of lc_pos whole positions, moved with 2D copies
+// (rows of lc lanes on the device; a partial last chunk is zero-padded, and
+// zeros stay zero and add nothing to the IDD); transport and angular
+// diffusion are local to a group, so they run on group chunks of ecg
+// contiguous groups.  A depth step is the in-core step's operator sequence,
+// each operator one streamed pass; the kernels are the in-core ones.  The
+// secondary's source is rebuilt for each lane chunk from the primary in both
+// of its energy passes (the primary does not change in between).
+// ---------------------------------------------------------------------------
+bfpn_status ensure_ooc(bfpn_ctx* c) {
+    const int lc_pos = std::max(1, std::min(c->nyz, c->ooc_lane_req / c->NA));
+    const int ecg = std::max(1, std::min(c->Ng, c->ooc_group_req));
+    if (c->ooc_ready && lc_pos == c->lc_pos && ecg == c->ecg) return BFPN_OK;
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    for (void*& p : c->dl) dfree(c, p);
+    dfree(c, c->dgc);
+    dfree(c, c->tmp);
+    dfree(c, c->src);
+    dfree(c, c->A1);
+    c->A2 = nullptr;
+    dfree(c, c->ablob);
+    dfree(c, c->ooc_part);
+    c->ooc_ready = false;
+    c->lc_pos = lc_pos;
+    c->lc = lc_pos * c->NA;
+    c->n_lc = (c->nyz + lc_pos - 1) / lc_pos;
+    c->ecg = ecg;
+    const size_t lane_arr = static_cast<size_t>(c->Ng) * c->lc * c->elem;
+    const size_t group_arr = static_cast<size_t>(ecg) * c->per_e * c->elem;
+    const bool secondary = !(c->p.flags & (BFPN_FLAG_PRIMARY_ONLY | BFPN_FLAG_ENERGY_ONLY));
+    bfpn_status s;
+    for (int k = 0; k < (secondary ? 4 : 2); ++k)
+        if ((s = dalloc(c, &c->dl[k], lane_arr)) != BFPN_OK) return s;
+    if ((s = dalloc(c, &c->dgc, group_arr)) != BFPN_OK) return s;
+    if (!c->tr_inplace && (s = dalloc(c, &c->tmp, group_arr)) != BFPN_OK) return s;
+    if (secondary) {
+        if ((s = dalloc(c, &c->src, lane_arr)) != BFPN_OK) return s;
+        c->a_bytes = c->prec == BFPN_PREC_MIXED ? std::max(2 * lane_arr, umma_q_bytes(c->lc, c->Ng)) : 2 * lane_arr;
+        if ((s = dalloc(c, &c->A1, c->a_bytes)) != BFPN_OK) return s;
+        c->A2 = static_cast<char*>(c->A1) + lane_arr;
+        CUDA_TRY(c, cudaMemsetAsync(c->A1, 0, c->a_bytes, c->stream));
+        if (c->prec == BFPN_PREC_MIXED && c->bblob && c->n_groups > 0) {
+            void* ab = nullptr;
+            if (dalloc(c, &ab, umma_pack_bytes(c->n_groups, lc_pos, c->NA, c->umma_bk)) == BFPN_OK) c->ablob = ab;
+            else cudaGetLastError();  // without it the source stays on the CUDA-core kernels
+        }
+    }
+    const size_t part = 4 * static_cast<size_t>(c->n_lc) * energy_grid(c->lc, c->energy_block);
+    if ((s = dalloc(c, &c->ooc_part, part * sizeof(double))) != BFPN_OK) return s;
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    c->ooc_ready = true;
+    return BFPN_OK;
+}
+
+// Lane chunk k of host array H to / from device rows of lc lanes.
+cudaError_t ooc_lane_copy(bfpn_ctx* c, void* H, void* D, int k, bool to_device) {
+    const size_t e = c->elem, pitch_h = static_cast<size_t>(c->per_e) * e, pitch_d = static_cast<size_t>(c->lc) * e;
+    const long long p0 = static_cast<long long>(k) * c->lc_pos;
+    const size_t lanes = static_cast<size_t>(std::min<long long>(c->lc_pos, c->nyz - p0)) * c->NA;
+    char* h = static_cast<char*>(H) + p0 * c->NA * e;
+    cudaError_t r;
+    if (!to_device) return cudaMemcpy2DAsync(h, pitch_h, D, pitch_d, lanes * e, c->Ng, cudaMemcpyDeviceToHost, c->stream);
+    r = cudaMemcpy2DAsync(D, pitch_d, h, pitch_h, lanes * e, c->Ng, cudaMemcpyHostToDevice, c->stream);
+    if (r == cudaSuccess && lanes < static_cast<size_t>(c->lc))
+        r = cudaMemset2DAsync(static_cast<char*>(D) + lanes * e, pitch_d, 0, (c->lc - lanes) * e, c->Ng, c->stream);
+    return r;
+}
+
+// One energy half-step of a species over every lane chunk; with partials,
+// energy_grid(lc) partial pairs per chunk, chunk after chunk (*count in total).
+template <typename T>
+cudaError_t ooc_energy_pass(bfpn_ctx* c, int species, bool with_source, double* partials, int* count) {
+    const int gpc = energy_grid(c->lc, c->energy_block);
+    cudaError_t e;
+    for (int k = 0; k < c->n_lc; ++k) {
+        if ((e = ooc_lane_copy(c, c->st[species][0], c->dl[0], k, true)) != cudaSuccess) return e;
+        if ((e = ooc_lane_copy(c, c->st[species][1], c->dl[1], k, true)) != cudaSuccess) return e;
+        if (with_source) {
+            if ((e = ooc_lane_copy(c, c->st[0][0], c->dl[2], k, true)) != cudaSuccess) return e;
+            if ((e = ooc_lane_copy(c, c->st[0][1], c->dl[3], k, true)) != cudaSuccess) return e;
+            if ((e = enq_source_on<T>(c, c->dl[2], c->dl[3], c->src, c->lc_pos)) != cudaSuccess) return e;
+        }
+        EnergyArgs<T> a;
+        a.F = as<T>(c->dl[0]);
+        a.f = as<T>(c->dl[1]);
+        a.src = with_source ? as<const T>(c->src) : nullptr;
+        a.coef = c->ecoef_half;
+        a.Ng = c->Ng;
+        a.lanes = c->lc;
+        a.lane0 = static_cast<long long>(k) * c->lc;
+        if (c->p.flags & BFPN_FLAG_LEGACY_ENERGY) a.mode = EMODE_LEGACY;
+        else if (c->p.flags & BFPN_FLAG_EQ15_STRAGGLING) a.mode = EMODE_EQ15_STRAG;
+        else a.mode = EMODE_EQ15;
+        a.partials = partials ? partials + 2 * static_cast<size_t>(k) * gpc : nullptr;
+        a.dose_coef = c->dose_coef;
+        a.NA = c->NA;
+        a.Ny = c->Ny;
+        a.Nz = c->Nz;
+        a.trapezoidal = (c->p.flags & BFPN_FLAG_TRAPEZOIDAL_YZ) ? 1 : 0;
+        if ((e = prof(c, BFPN_KERNEL_ENERGY, [&] { return launch_energy<T>(a, c->energy_block, c->stream); })) !=
+            cudaSuccess)
+            return e;
+        if ((e = ooc_lane_copy(c, c->st[species][0], c->dl[0], k, false)) != cudaSuccess) return e;
+        if ((e = ooc_lane_copy(c, c->st[species][1], c->dl[1], k, false)) != cudaSuccess) return e;
+    }
+    if (count) *count = c->n_lc * gpc;
+    return cudaSuccess;
+}
+
+// Transport half-step, angle step, transport half-step on one array, group chunk by group chunk.
+template <typename T>
+cudaError_t ooc_tat_pass(bfpn_ctx* c, int species, int coef, bool do_tr, bool do_an, bool preserve) {
+    const double h = 0.5 * c->d.dt;
+    char* X = static_cast<char*>(c->st[species][coef]);
+    const size_t row = static_cast<size_t>(c->per_e) * c->elem;
+    cudaError_t e;
+    for (int e0 = 0; e0 < c->Ng; e0 += c->ecg) {
+        const int g = std::min(c->ecg, c->Ng - e0);
+        const void* fac = static_cast<const char*>(c->fac_step) + static_cast<size_t>(e0) * c->NA * c->elem;
+        if ((e = cudaMemcpyAsync(c->dgc, X + e0 * row, g * row, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess)
+            return e;
+        if (do_tr) {
+            void* Y = transport_in_place(c) ? c->dgc : c->tmp;
+            if ((e = enq_transport<T>(c, c->dgc, Y, h, preserve, g)) != cudaSuccess) return e;
+            if (do_an && (e = enq_angle<T>(c, Y, fac, g)) != cudaSuccess) return e;
+            if ((e = enq_transport<T>(c, Y, c->dgc, h, preserve, g)) != cudaSuccess) return e;
+        } else if (do_an) {
+            if ((e = enq_angle<T>(c, c->dgc, fac, g)) != cudaSuccess) return e;
+        }
+        if ((e = cudaMemcpyAsync(X + e0 * row, c->dgc, g * row, cudaMemcpyDeviceToHost, c->stream)) != cudaSuccess)
+            return e;
+    }
+    return cudaSuccess;
+}
+
+// One depth step: enq_step's operator sequence, streamed.
+template <typename T>
+cudaError_t ooc_step(bfpn_ctx* c, bool first, bool secondary_zero) {
+    const unsigned fl = c->p.flags;
+    const bool energy_only = fl & BFPN_FLAG_ENERGY_ONLY;
+    const bool do_tr = !(fl & BFPN_FLAG_NO_TRANSPORT), do_an = !(fl & BFPN_FLAG_NO_ANGLE);
+    const size_t half = 2 * static_cast<size_t>(c->n_lc) * energy_grid(c->lc, c->energy_block);
+    double* partP = static_cast<double*>(c->ooc_part);
+    double* partS = partP + half;
+    int nP = 0, nS = 0;
+    cudaError_t e;
+    if ((e = ooc_energy_pass<T>(c, 0, false, nullptr, nullptr)) != cudaSuccess) return e;
+    if (!energy_only) {
+        const bool clip_F = !(fl & BFPN_FLAG_NO_SPATIAL_CLIPPING);
+        if ((e = ooc_tat_pass<T>(c, 0, 0, do_tr, do_an, !clip_F)) != cudaSuccess) return e;
+        if ((e = ooc_tat_pass<T>(c, 0, 1, do_tr, do_an, true)) != cudaSuccess) return e;
+    }
+    if ((e = ooc_energy_pass<T>(c, 0, false, partP, &nP)) != cudaSuccess) return e;
+    const bool secondary = !energy_only && !(fl & BFPN_FLAG_PRIMARY_ONLY) && !first;
+    if (secondary) {
+        if ((e = ooc_energy_pass<T>(c, 1, true, nullptr, nullptr)) != cudaSuccess) return e;
+        if ((e = ooc_tat_pass<T>(c, 1, 0, true, true, false)) != cudaSuccess) return e;
+        if ((e = ooc_tat_pass<T>(c, 1, 1, true, true, true)) != cudaSuccess) return e;
+        if ((e = ooc_energy_pass<T>(c, 1, true, partS, &nS)) != cudaSuccess) return e;
+    } else if (!secondary_zero) {
+        return cudaErrorNotSupported;  // an uploaded secondary that this step does not advance
+    }
+    const double w = c->d.du * c->d.dv * c->d.dy * c->d.dz;
+    return prof(c, BFPN_KERNEL_IDD, [&] {
+        return launch_finalize_idd(partP, nP, partS, nS, w, c->d.dg, c->hist_idd, c->hist_proxy, c->counter,
+                                   c->hist_cap, 1, c->stream);
+    });
+}
+
 bfpn_status ensure_history(bfpn_ctx* c, int needed) {
     if (needed <= c->hist_cap) return BFPN_OK;
     int cap = c->hist_cap;
@@ -620,6 +815,23 @@ bfpn_status run_steps(bfpn_ctx* c, int nsteps) {
     if (nsteps < 0) return fail(c, BFPN_INVALID_ARG, "nsteps < 0");
     bfpn_status s = ensure_history(c, c->steps_done + nsteps);
     if (s != BFPN_OK) return s;
+    if (c->ooc) {  // streamed steps, launched eagerly
+        if ((s = ensure_ooc(c)) != BFPN_OK) return s;
+        for (int i = 0; i < nsteps; ++i) {
+            const bool first = c->steps_done == 0;
+            const long long before = c->launches;
+            const cudaError_t e = c->prec == BFPN_PREC_FP64 ? ooc_step<double>(c, first, c->secondary_zero)
+                                                            : ooc_step<float>(c, first, c->secondary_zero);
+            if (e == cudaErrorNotSupported)
+                return fail(c, BFPN_INVALID_ARG,
+                            "out-of-core mode: an uploaded secondary state that a step does not advance");
+            CUDA_TRY(c, e);
+            c->kernels_per_step = static_cast<int>(c->launches - before);
+            if (!first && !(c->p.flags & (BFPN_FLAG_ENERGY_ONLY | BFPN_FLAG_PRIMARY_ONLY))) c->secondary_zero = false;
+            c->steps_done++;
+        }
+        return BFPN_OK;
+    }
     for (int i = 0; i < nsteps; ++i) {
         const bool first = c->steps_done == 0;
         const bool secondary_stepping =
@@ -780,6 +992,16 @@ bfpn_status bfpn_footprint_bytes(const bfpn_grid* grid, const bfpn_phys* phys, i
     if (!valid_grid(*grid, why)) return fail(nullptr, BFPN_INVALID_ARG, why);
     if (precision != BFPN_PREC_FP64 && precision != BFPN_PREC_MIXED)
         return fail(nullptr, BFPN_INVALID_ARG, "unknown precision");
+    if (phys && (phys->flags & BFPN_FLAG_STREAMING_FULL)) {  // device bytes at the default chunk sizes
+        const size_t elem = precision == BFPN_PREC_FP64 ? 8 : 4;
+        const long long nyz = static_cast<long long>(grid->Ny + 1) * (grid->Nz + 1), NA = grid->Nmu * grid->Nom;
+        const long long lc = std::max<long long>(1, std::min<long long>(nyz, 262144 / NA)) * NA;
+        const size_t lane_arr = static_cast<size_t>(grid->Ng) * lc * elem;
+        const size_t group_arr = static_cast<size_t>(std::min(grid->Ng, 128)) * nyz * NA * elem;
+        *bytes = 8 * lane_arr + 2 * group_arr + static_cast<size_t>(grid->Ng) * NA * NA * elem +
+                 2 * static_cast<size_t>(grid->Ng) * grid->Ng * sizeof(double) + (64u << 20);
+        return BFPN_OK;
+    }
     *bytes = footprint(*grid, precision, phys && (phys->flags & BFPN_FLAG_LITE_MEMORY));
     return BFPN_OK;
 }
@@ -793,6 +1015,8 @@ bfpn_status bfpn_create(const bfpn_grid* grid, const bfpn_phys* phys, int precis
         return fail(nullptr, BFPN_INVALID_ARG, "unknown precision");
     if (!(phys->density > 0) || !(phys->energy_density > 0) || !(phys->sig_E > 0))
         return fail(nullptr, BFPN_INVALID_ARG, "density and sigma_E must be positive");
+    if ((phys->flags & BFPN_FLAG_STREAMING_FULL) && (phys->flags & BFPN_FLAG_LITE_MEMORY))
+        return fail(nullptr, BFPN_INVALID_ARG, "--lite-memory and --streaming-full are mutually exclusive");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         cudaGetLastError();
@@ -802,6 +1026,7 @@ bfpn_status bfpn_create(const bfpn_grid* grid, const bfpn_phys* phys, int precis
 
     auto* c = new bfpn_ctx();
     c->g = *grid;
+    c->ooc = (phys->flags & BFPN_FLAG_STREAMING_FULL) != 0;
     c->p = *phys;
     c->prec = precision;
     c->device = device;
@@ -833,7 +1058,7 @@ bfpn_status bfpn_create(const bfpn_grid* grid, const bfpn_phys* phys, int precis
     }
     {
         size_t free_b = 0, total_b = 0;
-        if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
+        if (!c->ooc && cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
             const uint64_t need = footprint(*grid, precision, (phys->flags & BFPN_FLAG_LITE_MEMORY) != 0);
             if (need > free_b) {
                 char msg[256];
@@ -862,11 +1087,23 @@ bfpn_status bfpn_create(const bfpn_grid* grid, const bfpn_phys* phys, int precis
     dst = static_cast<std::remove_reference_t<decltype(dst)>>(v);
     c->lite = (phys->flags & BFPN_FLAG_LITE_MEMORY) != 0;
     for (int sp = 0; sp < 2; ++sp)
-        for (int cf = 0; cf < 2; ++cf)
-            if (!c->lite || (sp == 0 && cf == 0)) { ALLOC(c->st[sp][cf], arr); }
-    if (!c->tr_inplace && !c->lite) { ALLOC(c->tmp, arr); }
+        for (int cf = 0; cf < 2; ++cf) {
+            if (c->ooc) {
+                void* h = nullptr;
+                if (cudaHostAlloc(&h, arr, cudaHostAllocDefault) != cudaSuccess) {
+                    cudaGetLastError();
+                    c->err = "cannot allocate the pinned host state (" + std::to_string(arr) + " bytes per array)";
+                    return bail(BFPN_OOM);
+                }
+                c->host_allocs.push_back(h);
+                c->st[sp][cf] = h;
+            } else if (!c->lite || (sp == 0 && cf == 0)) {
+                ALLOC(c->st[sp][cf], arr);
+            }
+        }
+    if (!c->tr_inplace && !c->lite && !c->ooc) { ALLOC(c->tmp, arr); }
     const bool need_secondary = !c->lite && !(phys->flags & (BFPN_FLAG_PRIMARY_ONLY | BFPN_FLAG_ENERGY_ONLY));
-    if (need_secondary) {
+    if (need_secondary && !c->ooc) {
         ALLOC(c->src, arr);
         // A1 and A2 for the CUDA-core source; the same block holds the
         // tensor-core source's split-bf16 operand
@@ -905,7 +1142,7 @@ bfpn_status bfpn_create(const bfpn_grid* grid, const bfpn_phys* phys, int precis
     ALLOC(c->plane, static_cast<size_t>(c->nyz) * sizeof(double));
     ALLOC(c->lite_coef, 2 * static_cast<size_t>(c->Ng) * sizeof(double));
 #undef ALLOC
-    if (need_secondary) {
+    if (need_secondary && !c->ooc) {
         if (cudaMemsetAsync(c->A1, 0, c->a_bytes, c->stream) != cudaSuccess ||
             cudaMemsetAsync(c->src, 0, arr, c->stream) != cudaSuccess) {
             c->err = "memset failed";
@@ -987,7 +1224,8 @@ bfpn_status bfpn_load_tables(bfpn_ctx* c, const double* mu, int32_t mu_rows, con
     // rows of groups without an angular kernel are read as zeros; an earlier
     // beam's tables may have had a kernel there
     if (c->A1) CUDA_TRY(c, cudaMemsetAsync(c->A1, 0, c->a_bytes, c->stream));
-    if (c->prec == BFPN_PREC_MIXED && c->A1 && !groups.empty()) {
+    c->ooc_ready = false;  // the chunk buffers depend on the source groups
+    if (c->prec == BFPN_PREC_MIXED && (c->A1 || (c->ooc && c->ker_v)) && !groups.empty()) {
         // tensor-core source: output tiles of <= 256 columns, multiples of 16
         c->umma_ntiles = (c->NA + 255) / 256;
         c->umma_nt = ((c->NA + c->umma_ntiles - 1) / c->umma_ntiles + 15) / 16 * 16;
@@ -996,7 +1234,7 @@ bfpn_status bfpn_load_tables(bfpn_ctx* c, const double* mu, int32_t mu_rows, con
         // source's angular stage stays on the fp32 CUDA-core kernel
         const size_t pack = umma_pack_bytes(c->n_groups, c->nyz, c->NA, c->umma_bk);
         size_t free_b = 0, total_b = 0;
-        if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess && pack + (256u << 20) < free_b) {
+        if (!c->ooc && cudaMemGetInfo(&free_b, &total_b) == cudaSuccess && pack + (256u << 20) < free_b) {
             void* ab = nullptr;
             if (dalloc(c, &ab, pack) == BFPN_OK) c->ablob = ab;
         }
@@ -1055,6 +1293,29 @@ bfpn_status bfpn_init_beam(bfpn_ctx* c) {
     bfpn_status s = set_device(c);
     if (s != BFPN_OK) return s;
     const size_t arr = static_cast<size_t>(c->cells) * c->elem;
+    if (c->ooc) {  // group chunk by group chunk into the host array
+        if ((s = ensure_ooc(c)) != BFPN_OK) return s;
+        const size_t row = static_cast<size_t>(c->per_e) * c->elem;
+        for (int e0 = 0; e0 < c->Ng; e0 += c->ecg) {
+            const int g = std::min(c->ecg, c->Ng - e0);
+            if (c->prec == BFPN_PREC_FP64)
+                CUDA_TRY(c, launch_init_beam<double>(as<double>(c->dgc), c->beam_yza, c->beam_e + e0, c->per_e, g,
+                                                     c->stream));
+            else
+                CUDA_TRY(c, launch_init_beam<float>(as<float>(c->dgc), c->beam_yza, c->beam_e + e0, c->per_e, g,
+                                                    c->stream));
+            CUDA_TRY(c, cudaMemcpyAsync(static_cast<char*>(c->st[0][0]) + e0 * row, c->dgc, g * row,
+                                        cudaMemcpyDeviceToHost, c->stream));
+        }
+        CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+        for (void* X : {c->st[0][1], c->st[1][0], c->st[1][1]}) std::memset(X, 0, arr);
+        CUDA_TRY(c, cudaMemsetAsync(c->counter, 0, sizeof(int), c->stream));
+        CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+        c->beam_ready = true;
+        c->steps_done = 0;
+        c->secondary_zero = true;
+        return BFPN_OK;
+    }
     if (c->prec == BFPN_PREC_FP64) {
         CUDA_TRY(c, launch_init_beam<double>(as<double>(c->st[0][0]), c->beam_yza, c->beam_e, c->per_e, c->Ng, c->stream));
     } else {
@@ -1119,6 +1380,7 @@ void* bfpn_stream(bfpn_ctx* c) { return c ? static_cast<void*>(c->stream) : null
 
 bfpn_status bfpn_energy_eq15(bfpn_ctx* c, int32_t species, double dt, int32_t with_source) {
     if (!c) return BFPN_INVALID_ARG;
+    if (c->ooc) return fail(c, BFPN_INVALID_ARG, "needs a device-resident state (not available in the out-of-core mode)");
     if (!c->tables_loaded) return fail(c, BFPN_NOT_READY, "tables not loaded");
     if (species < 0 || species > 1 || !(dt > 0)) return fail(c, BFPN_INVALID_ARG, "bad species or dt");
     if (c->lite) return fail(c, BFPN_INVALID_ARG, "not available in lite-memory mode (psi^1 of the primary only)");
@@ -1139,6 +1401,7 @@ bfpn_status bfpn_energy_eq15(bfpn_ctx* c, int32_t species, double dt, int32_t wi
 
 bfpn_status bfpn_transport_eq18(bfpn_ctx* c, int32_t species, int32_t coef, double dt, int32_t preserve_sign) {
     if (!c) return BFPN_INVALID_ARG;
+    if (c->ooc) return fail(c, BFPN_INVALID_ARG, "needs a device-resident state (not available in the out-of-core mode)");
     if (!c->tables_loaded) return fail(c, BFPN_NOT_READY, "tables not loaded");
     if (species < 0 || species > 1 || coef < 0 || coef > 1 || !(dt > 0))
         return fail(c, BFPN_INVALID_ARG, "bad species, coef or dt");
@@ -1157,6 +1420,7 @@ bfpn_status bfpn_transport_eq18(bfpn_ctx* c, int32_t species, int32_t coef, doub
 
 bfpn_status bfpn_angle_eq19(bfpn_ctx* c, int32_t species, int32_t coef, double dt) {
     if (!c) return BFPN_INVALID_ARG;
+    if (c->ooc) return fail(c, BFPN_INVALID_ARG, "needs a device-resident state (not available in the out-of-core mode)");
     if (!c->tables_loaded) return fail(c, BFPN_NOT_READY, "tables not loaded");
     if (species < 0 || species > 1 || coef < 0 || coef > 1 || !(dt > 0))
         return fail(c, BFPN_INVALID_ARG, "bad species, coef or dt");
@@ -1175,6 +1439,7 @@ bfpn_status bfpn_angle_eq19(bfpn_ctx* c, int32_t species, int32_t coef, double d
 
 bfpn_status bfpn_secondary_source(bfpn_ctx* c) {
     if (!c) return BFPN_INVALID_ARG;
+    if (c->ooc) return fail(c, BFPN_INVALID_ARG, "needs a device-resident state (not available in the out-of-core mode)");
     if (!c->tables_loaded) return fail(c, BFPN_NOT_READY, "tables not loaded");
     if (!c->A1) return fail(c, BFPN_INVALID_ARG, "context has no secondary species (primary-only or energy-only)");
     bfpn_status s = set_device(c);
@@ -1202,6 +1467,11 @@ bfpn_status bfpn_set_option(bfpn_ctx* c, int32_t option, int32_t value) {
             break;
         case BFPN_OPT_PAIRED_ANGLES:
             c->tr_pairs = value != 0;
+            break;
+        case BFPN_OPT_LANE_CHUNK:
+        case BFPN_OPT_ENERGY_CHUNK:
+            if (value < 1) return fail(c, BFPN_INVALID_ARG, "chunk sizes must be positive");
+            (option == BFPN_OPT_LANE_CHUNK ? c->ooc_lane_req : c->ooc_group_req) = value;
             break;
         case BFPN_OPT_CLUSTER_TRANSPORT:
             if (value < 0 || value > 2) return fail(c, BFPN_INVALID_ARG, "cluster transport: 0, 1 or 2");
@@ -1246,6 +1516,7 @@ bfpn_status bfpn_set_option(bfpn_ctx* c, int32_t option, int32_t value) {
 
 bfpn_status bfpn_idd(bfpn_ctx* c, double* idd, double* proxy) {
     if (!c) return BFPN_INVALID_ARG;
+    if (c->ooc) return fail(c, BFPN_INVALID_ARG, "needs a device-resident state (not available in the out-of-core mode)");
     if (!c->tables_loaded) return fail(c, BFPN_NOT_READY, "tables not loaded");
     bfpn_status s = set_device(c);
     if (s != BFPN_OK) return s;
@@ -1300,8 +1571,17 @@ bfpn_status bfpn_state_upload(bfpn_ctx* c, int32_t species, int32_t coef, const 
         return fail(c, BFPN_INVALID_ARG, "lite-memory mode holds only psi^1 of the primary (species 0, coef 0)");
     bfpn_status s = set_device(c);
     if (s != BFPN_OK) return s;
-    s = c->prec == BFPN_PREC_FP64 ? upload_as<double>(c, c->st[species][coef], host, c->cells)
-                                  : upload_as<float>(c, c->st[species][coef], host, c->cells);
+    if (c->ooc) {  // the state is host memory: convert in place
+        CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+        if (c->prec == BFPN_PREC_FP64) std::memcpy(c->st[species][coef], host, c->cells * sizeof(double));
+        else {
+            float* d = static_cast<float*>(c->st[species][coef]);
+            for (long long i = 0; i < c->cells; ++i) d[i] = static_cast<float>(host[i]);
+        }
+    } else {
+        s = c->prec == BFPN_PREC_FP64 ? upload_as<double>(c, c->st[species][coef], host, c->cells)
+                                      : upload_as<float>(c, c->st[species][coef], host, c->cells);
+    }
     if (s != BFPN_OK) return s;
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     if (species == 1) c->secondary_zero = false;
@@ -1316,12 +1596,22 @@ bfpn_status bfpn_state_download(bfpn_ctx* c, int32_t species, int32_t coef, doub
         return fail(c, BFPN_INVALID_ARG, "lite-memory mode holds only psi^1 of the primary (species 0, coef 0)");
     bfpn_status s = set_device(c);
     if (s != BFPN_OK) return s;
+    if (c->ooc) {
+        CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+        if (c->prec == BFPN_PREC_FP64) std::memcpy(host, c->st[species][coef], c->cells * sizeof(double));
+        else {
+            const float* d = static_cast<const float*>(c->st[species][coef]);
+            for (long long i = 0; i < c->cells; ++i) host[i] = static_cast<double>(d[i]);
+        }
+        return BFPN_OK;
+    }
     return c->prec == BFPN_PREC_FP64 ? download_as<double>(c, c->st[species][coef], host, c->cells)
                                      : download_as<float>(c, c->st[species][coef], host, c->cells);
 }
 
 bfpn_status bfpn_source_download(bfpn_ctx* c, double* host) {
     if (!c || !host) return BFPN_INVALID_ARG;
+    if (c->ooc) return fail(c, BFPN_INVALID_ARG, "needs a device-resident state (not available in the out-of-core mode)");
     if (!c->A1) return fail(c, BFPN_INVALID_ARG, "context has no secondary species");
     bfpn_status s = set_device(c);
     if (s != BFPN_OK) return s;
@@ -1410,6 +1700,7 @@ bfpn_status bfpn_setup_summary(bfpn_ctx* c, bfpn_setup_info* out) {
 
 bfpn_status bfpn_energy_moments(bfpn_ctx* c, double* out) {
     if (!c || !out) return BFPN_INVALID_ARG;
+    if (c->ooc) return fail(c, BFPN_INVALID_ARG, "needs a device-resident state (not available in the out-of-core mode)");
     if (c->lite) return fail(c, BFPN_INVALID_ARG, "not available in lite-memory mode (psi^1 of the primary only)");
     bfpn_status s = set_device(c);
     if (s != BFPN_OK) return s;
@@ -1428,6 +1719,7 @@ bfpn_status bfpn_energy_moments(bfpn_ctx* c, double* out) {
 
 bfpn_status bfpn_spot_plane(bfpn_ctx* c, double* plane) {
     if (!c || !plane) return BFPN_INVALID_ARG;
+    if (c->ooc) return fail(c, BFPN_INVALID_ARG, "needs a device-resident state (not available in the out-of-core mode)");
     if (c->lite) return fail(c, BFPN_INVALID_ARG, "not available in lite-memory mode (psi^1 of the primary only)");
     if (!c->tables_loaded) return fail(c, BFPN_NOT_READY, "tables not loaded");
     bfpn_status s = set_device(c);

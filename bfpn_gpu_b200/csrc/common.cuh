@@ -59,6 +59,7 @@ struct EnergyArgs {
     const double* dose_coef;  // [Ng][2]: weight of psi^1 and psi^2
     int NA, Ny, Nz;
     int trapezoidal;
+    long long lane0 = 0;   // state lane of lane 0 (a chunk of whole positions; trapezoidal weights)
 };
 
 // Arguments of one transport half-step (Eq. 18) over one array.

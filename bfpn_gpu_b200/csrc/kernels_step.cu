@@ -102,7 +102,7 @@ __global__ void __launch_bounds__(NTH, MINB) energy_kernel(EnergyArgs<T> a) {
         F_hi_old[j] = f_hi_old[j] = next_F[j] = next_f[j] = 0.0;
         w_pos[j] = 1.0;
         if (a.partials && a.trapezoidal && ok[j]) {
-            const int pos = static_cast<int>(lane[j] / a.NA);
+            const int pos = static_cast<int>((lane[j] + a.lane0) / a.NA);
             const int iy = pos % (a.Ny + 1), iz = pos / (a.Ny + 1);
             if (iy == 0 || iy == a.Ny) w_pos[j] *= 0.5;
             if (iz == 0 || iz == a.Nz) w_pos[j] *= 0.5;

@@ -56,7 +56,7 @@ void printHelp(const char* prog) {
               << "  --precision <fp64|mixed> Device arithmetic (default: fp64)\n"
               << "  --device <n>     CUDA device ordinal (default: 0)\n"
               << "  --lite-memory    Primary-only low-memory mode for large grid development\n"
-              << "  --streaming-full Accepted; the state stays device resident\n"
+              << "  --streaming-full Out-of-core mode: the state in pinned host memory, streamed through the GPU in chunks\n"
               << "  --primary-only   Skip secondary proton evolution/source\n"
               << "  --energy-model <eq15|legacy> Energy update model (default: eq15)\n"
               << "  --eq15-straggling Enable Eq.15 straggling/SIPG terms\n"
@@ -74,7 +74,10 @@ void printHelp(const char* prog) {
               << "  --no-cross-section-calibration Use fitted sigma_c directly (default)\n"
               << "  --legacy-cross-section-calibration Apply the legacy empirical sigma_c correction\n"
               << "  --sigma-yz <cm>  Initial transverse Gaussian sigma (default: 0.1)\n"
-              << "  --idd-stride <n> Accepted (streaming-mode option; IDD is computed every step)\n"
+              << "  --lane-chunk <n> Streaming mode: lanes per energy-sweep chunk (default: 262144)\n"
+              << "  --energy-chunk <n> Streaming mode: groups per transport/angle chunk (default: 128)\n"
+              << "  --stream-dir <path> Accepted (the streamed state is in pinned host memory)\n"
+              << "  --idd-stride <n> Streaming mode: write the IDD every n steps (default: 1)\n"
               << "  --spot-depths <x,...> Save YZ dose planes near requested depths\n"
               << "  --spot-prefix <path> Prefix for spot plane files (default: spot)\n"
               << "  --print-config   Print the parsed run as JSON and exit\n"

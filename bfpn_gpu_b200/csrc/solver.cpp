@@ -63,6 +63,7 @@ bfpn_phys toCPhys(const PhysicsParams& p) {
     if (p.dose_catastrophic_loss) f |= BFPN_FLAG_DOSE_CATASTROPHIC_LOSS;
     if (p.calibrate_cross_sections) f |= BFPN_FLAG_CALIBRATE_CROSS_SECTIONS;
     if (p.lite_memory) f |= BFPN_FLAG_LITE_MEMORY;
+    if (p.streaming_full) f |= BFPN_FLAG_STREAMING_FULL;
     c.flags = f;
     return c;
 }
@@ -76,16 +77,18 @@ void BFPnSolver::check(bfpn_status s, const char* what) {
 
 BFPnSolver::BFPnSolver(const GridParams& g, const PhysicsParams& p) : grid(g), phys(p) {
     grid.computeDeltas();
-    if (phys.streaming_full)
-        std::cout << "Note: --streaming-full keeps the whole state resident in device memory here" << std::endl;
+    if (phys.streaming_full && (phys.save_energy_moments || !phys.spot_depths.empty()))
+        throw std::runtime_error(
+            "--save-energy-moments and --spot-depths need the device-resident state; run them without --streaming-full");
     const bfpn_grid cg = toCGrid(grid);
     const bfpn_phys cp = toCPhys(phys);
     uint64_t need = 0;
     if (bfpn_footprint_bytes(&cg, &cp, phys.precision, &need) == BFPN_OK) {
         const double one = static_cast<double>(grid.Ny + 1) * (grid.Nz + 1) * grid.Ng * grid.Nmu * grid.Nom *
                            (phys.precision == BFPN_PREC_FP64 ? 8.0 : 4.0) / 1073741824.0;
-        std::cout << "Memory estimate:\n  Mode: " << (phys.lite_memory ? "lite-memory primary-only" : "full")
-                  << " (device resident, "
+        std::cout << "Memory estimate:\n  Mode: "
+                  << (phys.lite_memory ? "lite-memory primary-only" : phys.streaming_full ? "streaming-full" : "full")
+                  << (phys.streaming_full ? " (pinned host state, device chunks, " : " (device resident, ")
                   << (phys.precision == BFPN_PREC_FP64 ? "fp64" : "mixed fp32/fp64") << ")\n"
                   << std::fixed << std::setprecision(2) << "  One phase-space array: " << one << " GiB\n"
                   << "  Estimated device footprint: " << need / 1073741824.0 << " GiB" << std::defaultfloat
@@ -96,6 +99,10 @@ BFPnSolver::BFPnSolver(const GridParams& g, const PhysicsParams& p) : grid(g), p
         std::ostringstream msg;
         msg << bfpn_last_error(nullptr);
         throw std::runtime_error(msg.str());
+    }
+    if (phys.streaming_full) {
+        check(bfpn_set_option(ctx_, BFPN_OPT_LANE_CHUNK, phys.streaming_lane_chunk), "lane chunk");
+        check(bfpn_set_option(ctx_, BFPN_OPT_ENERGY_CHUNK, phys.streaming_energy_chunk), "energy chunk");
     }
 }
 
@@ -129,6 +136,12 @@ void BFPnSolver::solve(double tFinal) {  // bfpm_solver.cu:2166-2267
               << ", Angle: " << grid.Nmu << "x" << grid.Nom << std::endl;
     if (phys.lite_memory)  // bfpm_solver.cu:2185-2187
         std::cout << "Mode: lite-memory primary-only (no secondary, no DG slope, no YZ/angular transport)" << std::endl;
+    const int n_angle = grid.Nmu * grid.Nom, nyz = (grid.Ny + 1) * (grid.Nz + 1);
+    if (phys.streaming_full)  // bfpm_solver.cu:3134-3140
+        std::cout << "Mode: streaming-full out-of-core, lane chunk "
+                  << std::max(1, std::min(nyz, phys.streaming_lane_chunk / n_angle)) * n_angle << " (requested "
+                  << phys.streaming_lane_chunk << "), energy chunk " << std::max(1, phys.streaming_energy_chunk)
+                  << ", IDD stride " << std::max(1, phys.idd_stride) << std::endl;
     idd_history_.clear();
     proxy_history_.clear();
     std::vector<double> moments_history;
@@ -180,8 +193,22 @@ void BFPnSolver::solve(double tFinal) {  // bfpm_solver.cu:2166-2267
             }
     }
     const double seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-    saveResults(idd_history_, "idd_output.txt");
-    saveResults(proxy_history_, "dose_output.txt");
+    if (phys.streaming_full) {
+        // the reference's streaming files: a row every idd_stride steps and the
+        // last, the scalar proxy written as 0 (bfpm_solver.cu:3144, 3206-3209)
+        const int stride = std::max(1, phys.idd_stride);
+        std::ofstream fi("idd_output.txt"), fp("dose_output.txt");
+        fi << std::setprecision(17) << "# x_cm value\n";
+        fp << std::setprecision(17) << "# x_cm value\n";
+        for (size_t i = 0; i < idd_history_.size(); ++i)
+            if ((i + 1) % stride == 0 || i + 1 == idd_history_.size()) {
+                fi << (i + 1) * grid.dt << " " << idd_history_[i] << "\n";
+                fp << (i + 1) * grid.dt << " " << 0.0 << "\n";
+            }
+    } else {
+        saveResults(idd_history_, "idd_output.txt");
+        saveResults(proxy_history_, "dose_output.txt");
+    }
     if (moments) saveEnergyMoments(moments_history, "energy_moments.txt");
     std::cout << "Solver completed. Paper-style IDD saved to idd_output.txt" << std::endl;
     std::cout << "Diagnostic scalar proxy saved to dose_output.txt" << std::endl;

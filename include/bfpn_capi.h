@@ -69,7 +69,16 @@ enum {
     BFPN_FLAG_TRAPEZOIDAL_YZ = 1u << 10,
     BFPN_FLAG_DOSE_CATASTROPHIC_LOSS = 1u << 11,
     BFPN_FLAG_CALIBRATE_CROSS_SECTIONS = 1u << 12,
-    BFPN_FLAG_LITE_MEMORY = 1u << 13
+    BFPN_FLAG_LITE_MEMORY = 1u << 13,
+    /* --streaming-full (solveStreamingFull, bfpm_solver.cu:3113-3236): the four
+     * state arrays live in pinned host memory instead of HBM and each depth
+     * step streams them through the GPU -- lane chunks (every group of a set of
+     * whole positions) for the energy sweeps and the source, group chunks for
+     * transport and angular diffusion; chunk sizes BFPN_OPT_LANE_CHUNK /
+     * BFPN_OPT_ENERGY_CHUNK.  For grids whose state does not fit in HBM.  The
+     * per-operator entry points, the one-off IDD, energy moments and spot
+     * planes need a resident state and report BFPN_INVALID_ARG. */
+    BFPN_FLAG_STREAMING_FULL = 1u << 14
 };
 
 typedef struct bfpn_phys {
@@ -260,13 +269,19 @@ int32_t bfpn_source_groups(bfpn_ctx* ctx);
  *   and exchange edge rows through distributed shared memory, in place;
  *   2 also uses it for Ny = Nz = 20 (in place of the whole-plane kernel);
  *   0 leaves those planes to the tiled kernel.  Values agree with the other
- *   kernels to float rounding. */
+ *   kernels to float rounding.
+ * BFPN_OPT_LANE_CHUNK / BFPN_OPT_ENERGY_CHUNK (out-of-core mode only): lanes
+ *   per lane chunk (rounded down to whole positions, at least one; default
+ *   262,144, the reference's --lane-chunk) and groups per group chunk (default
+ *   128, --energy-chunk); the device buffers are sized on the next step. */
 enum {
     BFPN_OPT_TENSOR_CORES = 0,
     BFPN_OPT_CUDA_GRAPHS = 1,
     BFPN_OPT_PLANE_TRANSPORT = 2,
     BFPN_OPT_PAIRED_ANGLES = 3,
-    BFPN_OPT_CLUSTER_TRANSPORT = 4
+    BFPN_OPT_CLUSTER_TRANSPORT = 4,
+    BFPN_OPT_LANE_CHUNK = 5,
+    BFPN_OPT_ENERGY_CHUNK = 6
 };
 bfpn_status bfpn_set_option(bfpn_ctx* ctx, int32_t option, int32_t value);
 

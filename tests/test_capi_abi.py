@@ -152,3 +152,12 @@ def test_server_without_device_fails_cleanly():
     with pytest.raises(capi.BfpnError) as e:
         capi.Server(workers_per_device=0)
     assert e.value.status == capi.INVALID_ARG
+
+
+def test_streaming_and_lite_memory_are_exclusive():
+    from bfpn_gpu_b200 import make_config
+    cfg = make_config(ny=4, nz=4, nmu=2, nom=2, ng=10, lite_memory=True)
+    import dataclasses
+    bad = dataclasses.replace(cfg, streaming_full=True)
+    with pytest.raises(capi.BfpnError, match="mutually exclusive"):
+        capi.Context(bad.grid(), bad.phys(), capi.PREC_FP64)
