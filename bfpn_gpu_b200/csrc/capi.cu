@@ -96,8 +96,10 @@ struct bfpn_ctx {
     int ooc_lane_req = 262144, ooc_group_req = 128;  // requested chunk sizes (lanes, groups)
     int lc_pos = 0, lc = 0, n_lc = 0, ecg = 0;        // positions / lanes per lane chunk, lane chunks, groups per group chunk
     bool ooc_ready = false;
-    void* dl[4] = {nullptr, nullptr, nullptr, nullptr};  // lane chunk: the species' psi^1, psi^2; the primary's for the source
-    void* dgc = nullptr;                                 // group chunk
+    void* dl[2][4] = {};    // two slots of a lane chunk: the species' psi^1, psi^2; the primary's for the source
+    void* dgc[2] = {};      // two slots of a group chunk
+    cudaStream_t s_in = nullptr, s_out = nullptr;        // host-to-device / device-to-host copies
+    cudaEvent_t ev_in[2] = {}, ev_comp[2] = {}, ev_out[2] = {}, ev_pass = nullptr;
     void* ooc_part = nullptr;                            // IDD partials of every lane chunk, both species
     std::vector<void*> host_allocs;
     double* lite_coef = nullptr;    // [Ng][2] lite step constants
@@ -632,8 +634,21 @@ bfpn_status ensure_ooc(bfpn_ctx* c) {
     const int ecg = std::max(1, std::min(c->Ng, c->ooc_group_req));
     if (c->ooc_ready && lc_pos == c->lc_pos && ecg == c->ecg) return BFPN_OK;
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
-    for (void*& p : c->dl) dfree(c, p);
-    dfree(c, c->dgc);
+    if (!c->s_in) {
+        CUDA_TRY(c, cudaStreamCreateWithFlags(&c->s_in, cudaStreamNonBlocking));
+        CUDA_TRY(c, cudaStreamCreateWithFlags(&c->s_out, cudaStreamNonBlocking));
+        for (int k = 0; k < 2; ++k) {
+            CUDA_TRY(c, cudaEventCreateWithFlags(&c->ev_in[k], cudaEventDisableTiming));
+            CUDA_TRY(c, cudaEventCreateWithFlags(&c->ev_comp[k], cudaEventDisableTiming));
+            CUDA_TRY(c, cudaEventCreateWithFlags(&c->ev_out[k], cudaEventDisableTiming));
+        }
+        CUDA_TRY(c, cudaEventCreateWithFlags(&c->ev_pass, cudaEventDisableTiming));
+    }
+    CUDA_TRY(c, cudaStreamSynchronize(c->s_in));
+    CUDA_TRY(c, cudaStreamSynchronize(c->s_out));
+    for (auto& slot : c->dl)
+        for (void*& p : slot) dfree(c, p);
+    for (void*& p : c->dgc) dfree(c, p);
     dfree(c, c->tmp);
     dfree(c, c->src);
     dfree(c, c->A1);
@@ -649,9 +664,11 @@ bfpn_status ensure_ooc(bfpn_ctx* c) {
     const size_t group_arr = static_cast<size_t>(ecg) * c->per_e * c->elem;
     const bool secondary = !(c->p.flags & (BFPN_FLAG_PRIMARY_ONLY | BFPN_FLAG_ENERGY_ONLY));
     bfpn_status s;
-    for (int k = 0; k < (secondary ? 4 : 2); ++k)
-        if ((s = dalloc(c, &c->dl[k], lane_arr)) != BFPN_OK) return s;
-    if ((s = dalloc(c, &c->dgc, group_arr)) != BFPN_OK) return s;
+    for (auto& slot : c->dl)
+        for (int k = 0; k < (secondary ? 4 : 2); ++k)
+            if ((s = dalloc(c, &slot[k], lane_arr)) != BFPN_OK) return s;
+    for (void*& p : c->dgc)
+        if ((s = dalloc(c, &p, group_arr)) != BFPN_OK) return s;
     if (!c->tr_inplace && (s = dalloc(c, &c->tmp, group_arr)) != BFPN_OK) return s;
     if (secondary) {
         if ((s = dalloc(c, &c->src, lane_arr)) != BFPN_OK) return s;
@@ -673,17 +690,26 @@ bfpn_status ensure_ooc(bfpn_ctx* c) {
 }
 
 // Lane chunk k of host array H to / from device rows of lc lanes.
-cudaError_t ooc_lane_copy(bfpn_ctx* c, void* H, void* D, int k, bool to_device) {
+cudaError_t ooc_lane_copy(bfpn_ctx* c, void* H, void* D, int k, bool to_device, cudaStream_t st) {
     const size_t e = c->elem, pitch_h = static_cast<size_t>(c->per_e) * e, pitch_d = static_cast<size_t>(c->lc) * e;
     const long long p0 = static_cast<long long>(k) * c->lc_pos;
     const size_t lanes = static_cast<size_t>(std::min<long long>(c->lc_pos, c->nyz - p0)) * c->NA;
     char* h = static_cast<char*>(H) + p0 * c->NA * e;
     cudaError_t r;
-    if (!to_device) return cudaMemcpy2DAsync(h, pitch_h, D, pitch_d, lanes * e, c->Ng, cudaMemcpyDeviceToHost, c->stream);
-    r = cudaMemcpy2DAsync(D, pitch_d, h, pitch_h, lanes * e, c->Ng, cudaMemcpyHostToDevice, c->stream);
+    if (!to_device) return cudaMemcpy2DAsync(h, pitch_h, D, pitch_d, lanes * e, c->Ng, cudaMemcpyDeviceToHost, st);
+    r = cudaMemcpy2DAsync(D, pitch_d, h, pitch_h, lanes * e, c->Ng, cudaMemcpyHostToDevice, st);
     if (r == cudaSuccess && lanes < static_cast<size_t>(c->lc))
-        r = cudaMemset2DAsync(static_cast<char*>(D) + lanes * e, pitch_d, 0, (c->lc - lanes) * e, c->Ng, c->stream);
+        r = cudaMemset2DAsync(static_cast<char*>(D) + lanes * e, pitch_d, 0, (c->lc - lanes) * e, c->Ng, st);
     return r;
+}
+
+// The next pass reads host arrays this pass writes: both the copy-in and the
+// compute stream wait for every copy out of this pass.
+cudaError_t ooc_pass_end(bfpn_ctx* c) {
+    cudaError_t e = cudaEventRecord(c->ev_pass, c->s_out);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(c->s_in, c->ev_pass, 0);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(c->stream, c->ev_pass, 0);
+    return e;
 }
 
 // One energy half-step of a species over every lane chunk; with partials,
@@ -693,16 +719,22 @@ cudaError_t ooc_energy_pass(bfpn_ctx* c, int species, bool with_source, double* 
     const int gpc = energy_grid(c->lc, c->energy_block);
     cudaError_t e;
     for (int k = 0; k < c->n_lc; ++k) {
-        if ((e = ooc_lane_copy(c, c->st[species][0], c->dl[0], k, true)) != cudaSuccess) return e;
-        if ((e = ooc_lane_copy(c, c->st[species][1], c->dl[1], k, true)) != cudaSuccess) return e;
+        const int sl = k & 1;
+        void* const* B = c->dl[sl];
+        // in: once the copies out of this slot's previous chunk are done
+        if ((e = cudaStreamWaitEvent(c->s_in, c->ev_out[sl], 0)) != cudaSuccess) return e;
+        if ((e = ooc_lane_copy(c, c->st[species][0], B[0], k, true, c->s_in)) != cudaSuccess) return e;
+        if ((e = ooc_lane_copy(c, c->st[species][1], B[1], k, true, c->s_in)) != cudaSuccess) return e;
         if (with_source) {
-            if ((e = ooc_lane_copy(c, c->st[0][0], c->dl[2], k, true)) != cudaSuccess) return e;
-            if ((e = ooc_lane_copy(c, c->st[0][1], c->dl[3], k, true)) != cudaSuccess) return e;
-            if ((e = enq_source_on<T>(c, c->dl[2], c->dl[3], c->src, c->lc_pos)) != cudaSuccess) return e;
+            if ((e = ooc_lane_copy(c, c->st[0][0], B[2], k, true, c->s_in)) != cudaSuccess) return e;
+            if ((e = ooc_lane_copy(c, c->st[0][1], B[3], k, true, c->s_in)) != cudaSuccess) return e;
         }
+        if ((e = cudaEventRecord(c->ev_in[sl], c->s_in)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(c->stream, c->ev_in[sl], 0)) != cudaSuccess) return e;
+        if (with_source && (e = enq_source_on<T>(c, B[2], B[3], c->src, c->lc_pos)) != cudaSuccess) return e;
         EnergyArgs<T> a;
-        a.F = as<T>(c->dl[0]);
-        a.f = as<T>(c->dl[1]);
+        a.F = as<T>(B[0]);
+        a.f = as<T>(B[1]);
         a.src = with_source ? as<const T>(c->src) : nullptr;
         a.coef = c->ecoef_half;
         a.Ng = c->Ng;
@@ -720,11 +752,15 @@ cudaError_t ooc_energy_pass(bfpn_ctx* c, int species, bool with_source, double* 
         if ((e = prof(c, BFPN_KERNEL_ENERGY, [&] { return launch_energy<T>(a, c->energy_block, c->stream); })) !=
             cudaSuccess)
             return e;
-        if ((e = ooc_lane_copy(c, c->st[species][0], c->dl[0], k, false)) != cudaSuccess) return e;
-        if ((e = ooc_lane_copy(c, c->st[species][1], c->dl[1], k, false)) != cudaSuccess) return e;
+        // out: after the chunk's kernels
+        if ((e = cudaEventRecord(c->ev_comp[sl], c->stream)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(c->s_out, c->ev_comp[sl], 0)) != cudaSuccess) return e;
+        if ((e = ooc_lane_copy(c, c->st[species][0], B[0], k, false, c->s_out)) != cudaSuccess) return e;
+        if ((e = ooc_lane_copy(c, c->st[species][1], B[1], k, false, c->s_out)) != cudaSuccess) return e;
+        if ((e = cudaEventRecord(c->ev_out[sl], c->s_out)) != cudaSuccess) return e;
     }
     if (count) *count = c->n_lc * gpc;
-    return cudaSuccess;
+    return ooc_pass_end(c);
 }
 
 // Transport half-step, angle step, transport half-step on one array, group chunk by group chunk.
@@ -734,23 +770,29 @@ cudaError_t ooc_tat_pass(bfpn_ctx* c, int species, int coef, bool do_tr, bool do
     char* X = static_cast<char*>(c->st[species][coef]);
     const size_t row = static_cast<size_t>(c->per_e) * c->elem;
     cudaError_t e;
-    for (int e0 = 0; e0 < c->Ng; e0 += c->ecg) {
-        const int g = std::min(c->ecg, c->Ng - e0);
+    int k = 0;
+    for (int e0 = 0; e0 < c->Ng; e0 += c->ecg, ++k) {
+        const int g = std::min(c->ecg, c->Ng - e0), sl = k & 1;
+        void* D = c->dgc[sl];
         const void* fac = static_cast<const char*>(c->fac_step) + static_cast<size_t>(e0) * c->NA * c->elem;
-        if ((e = cudaMemcpyAsync(c->dgc, X + e0 * row, g * row, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess)
-            return e;
+        if ((e = cudaStreamWaitEvent(c->s_in, c->ev_out[sl], 0)) != cudaSuccess) return e;
+        if ((e = cudaMemcpyAsync(D, X + e0 * row, g * row, cudaMemcpyHostToDevice, c->s_in)) != cudaSuccess) return e;
+        if ((e = cudaEventRecord(c->ev_in[sl], c->s_in)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(c->stream, c->ev_in[sl], 0)) != cudaSuccess) return e;
         if (do_tr) {
-            void* Y = transport_in_place(c) ? c->dgc : c->tmp;
-            if ((e = enq_transport<T>(c, c->dgc, Y, h, preserve, g)) != cudaSuccess) return e;
+            void* Y = transport_in_place(c) ? D : c->tmp;
+            if ((e = enq_transport<T>(c, D, Y, h, preserve, g)) != cudaSuccess) return e;
             if (do_an && (e = enq_angle<T>(c, Y, fac, g)) != cudaSuccess) return e;
-            if ((e = enq_transport<T>(c, Y, c->dgc, h, preserve, g)) != cudaSuccess) return e;
+            if ((e = enq_transport<T>(c, Y, D, h, preserve, g)) != cudaSuccess) return e;
         } else if (do_an) {
-            if ((e = enq_angle<T>(c, c->dgc, fac, g)) != cudaSuccess) return e;
+            if ((e = enq_angle<T>(c, D, fac, g)) != cudaSuccess) return e;
         }
-        if ((e = cudaMemcpyAsync(X + e0 * row, c->dgc, g * row, cudaMemcpyDeviceToHost, c->stream)) != cudaSuccess)
-            return e;
+        if ((e = cudaEventRecord(c->ev_comp[sl], c->stream)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(c->s_out, c->ev_comp[sl], 0)) != cudaSuccess) return e;
+        if ((e = cudaMemcpyAsync(X + e0 * row, D, g * row, cudaMemcpyDeviceToHost, c->s_out)) != cudaSuccess) return e;
+        if ((e = cudaEventRecord(c->ev_out[sl], c->s_out)) != cudaSuccess) return e;
     }
-    return cudaSuccess;
+    return ooc_pass_end(c);
 }
 
 // One depth step: enq_step's operator sequence, streamed.
@@ -1165,6 +1207,12 @@ bfpn_status bfpn_destroy(bfpn_ctx* ctx) {
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     free_all(ctx);
+    for (cudaStream_t st : {ctx->s_in, ctx->s_out})
+        if (st) cudaStreamDestroy(st);
+    for (int k = 0; k < 2; ++k)
+        for (cudaEvent_t ev : {ctx->ev_in[k], ctx->ev_comp[k], ctx->ev_out[k]})
+            if (ev) cudaEventDestroy(ev);
+    if (ctx->ev_pass) cudaEventDestroy(ctx->ev_pass);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
@@ -1299,12 +1347,12 @@ bfpn_status bfpn_init_beam(bfpn_ctx* c) {
         for (int e0 = 0; e0 < c->Ng; e0 += c->ecg) {
             const int g = std::min(c->ecg, c->Ng - e0);
             if (c->prec == BFPN_PREC_FP64)
-                CUDA_TRY(c, launch_init_beam<double>(as<double>(c->dgc), c->beam_yza, c->beam_e + e0, c->per_e, g,
+                CUDA_TRY(c, launch_init_beam<double>(as<double>(c->dgc[0]), c->beam_yza, c->beam_e + e0, c->per_e, g,
                                                      c->stream));
             else
-                CUDA_TRY(c, launch_init_beam<float>(as<float>(c->dgc), c->beam_yza, c->beam_e + e0, c->per_e, g,
+                CUDA_TRY(c, launch_init_beam<float>(as<float>(c->dgc[0]), c->beam_yza, c->beam_e + e0, c->per_e, g,
                                                     c->stream));
-            CUDA_TRY(c, cudaMemcpyAsync(static_cast<char*>(c->st[0][0]) + e0 * row, c->dgc, g * row,
+            CUDA_TRY(c, cudaMemcpyAsync(static_cast<char*>(c->st[0][0]) + e0 * row, c->dgc[0], g * row,
                                         cudaMemcpyDeviceToHost, c->stream));
         }
         CUDA_TRY(c, cudaStreamSynchronize(c->stream));
