@@ -461,6 +461,53 @@ def run_serve(args):
     print(json.dumps(out), flush=True)
 
 
+def run_out_of_core(args):
+    """The out-of-core mode (the reference's --streaming-full): the state in
+    pinned host memory, each step streamed through the GPU in chunks.  K steps
+    timed with CUDA events on the context stream; one replica."""
+    import dataclasses
+    import torch
+    from bfpn_gpu_b200 import Context, capi, make_config, read_tables
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    cfg = dataclasses.replace(make_config(**WORKLOAD), streaming_full=True)
+    prec = capi.PREC_MIXED if args.precision == "mixed" else capi.PREC_FP64
+    mu, sig = read_tables(TABLES, cfg.ng)
+    ctx = Context(cfg.grid(), cfg.phys(), prec, device=local)
+    ctx.set_option(capi.OPT_LANE_CHUNK, args.lane_chunk)
+    ctx.set_option(capi.OPT_ENERGY_CHUNK, args.energy_chunk)
+    ctx.load_tables(mu, sig)
+    ctx.init_beam()
+    ctx.step(2, fetch=False)  # the first step (no secondary) and one regular step
+    sampler = ClockSampler(local)
+    torch.cuda.synchronize()
+    barrier(world)
+    sampler.start()
+    ms = ctx.timed_steps(args.steps)
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = sampler.stop()
+    ms = max_over_ranks(ms, world, local)
+    updates_per_step = 2 * ctx.cells
+    value = job_throughput(world, updates_per_step, args.steps, ms)
+    elem = 4 if prec == capi.PREC_MIXED else 8
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": value, "unit": "updates/s", "n_gpus": world, "steps": args.steps,
+            "warmup": 2, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 state / f64 recursion" if prec == capi.PREC_MIXED else "f64",
+            "data": "reference tables; synthetic initial beam", "mode": "out-of-core",
+            "config": {"workload": WORKLOAD_NAME, "precision": args.precision, "cells_per_array": ctx.cells,
+                       "host_state_bytes": 4 * ctx.cells * elem, "lane_chunk": args.lane_chunk,
+                       "energy_chunk": args.energy_chunk, "parallelism": "replicas x%d" % world},
+            "gpu_launches": ctx.kernels_per_step() * args.steps, "clocks": clocks}), flush=True)
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -485,6 +532,10 @@ def main():
                     help="single-beam workload (the default is the one the metric is quoted on)")
     ap.add_argument("--ng", type=int, default=None,
                     help="energy groups (profiling captures on a smaller state; not for bench lines)")
+    ap.add_argument("--out-of-core", action="store_true",
+                    help="time the out-of-core mode (state in pinned host memory) on --workload")
+    ap.add_argument("--lane-chunk", type=int, default=262144)
+    ap.add_argument("--energy-chunk", type=int, default=128)
     args = ap.parse_args()
     global WORKLOAD, WORKLOAD_NAME, TABLES
     WORKLOAD, WORKLOAD_NAME = WORKLOADS[args.workload]
@@ -493,6 +544,8 @@ def main():
         WORKLOAD["ng"] = args.ng
     if args.serve:
         run_serve(args)
+    elif args.out_of_core:
+        run_out_of_core(args)
     elif args.impl == "reference":
         run_reference(args)
     else:
