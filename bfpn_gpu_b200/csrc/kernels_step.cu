@@ -686,6 +686,17 @@ __device__ __forceinline__ void walk_plane_line2(const float2* X, const float2* 
 
 __device__ __forceinline__ float2 max_lo2(float2 v, float lo) { return make_float2(fmaxf(v.x, lo), fmaxf(v.y, lo)); }
 
+// 16-byte global -> shared copy without a register round trip (cp.async,
+// L2 only); an invalid piece is filled with zeros (source size 0, nothing is
+// read from src).  cp_async_wait_all: every copy of this thread has landed.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, bool valid) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(valid ? 16 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
 template <int NP, int AC>
 __global__ void __launch_bounds__((NP * AC / 2 + 31) / 32 * 32) transport_plane_f2_kernel(TransportArgs<float> a,
                                                                                            int n_chunks) {
@@ -714,15 +725,16 @@ __global__ void __launch_bounds__((NP * AC / 2 + 31) / 32 * 32) transport_plane_
 
     float* Fsf = reinterpret_cast<float*>(Fs);
     if (AC % 4 == 0 && NA % 4 == 0) {
+        // every 16-byte piece of the plane in flight at once
         constexpr int NV = NP * NP * AC / 4;
 #pragma unroll 4
         for (int v = threadIdx.x; v < NV; v += NT) {
             const int e = v * 4, aa = e % AC, p = e / AC;
             const int z = p / NP, y = p - z * NP;
-            float4 val{};
-            if (a0 + aa < NA) val = *reinterpret_cast<const float4*>(in + static_cast<size_t>(p) * NA + aa);
-            *reinterpret_cast<float4*>(Fsf + 2 * (z * RS + y * A2) + aa) = val;
+            const bool ok = a0 + aa < NA;
+            cp_async16(Fsf + 2 * (z * RS + y * A2) + aa, ok ? in + static_cast<size_t>(p) * NA + aa : in, ok);
         }
+        cp_async_wait_all();
     } else {
 #pragma unroll 4
         for (int e = threadIdx.x; e < NP * NP * AC; e += NT) {
@@ -921,13 +933,11 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(ClusterPlane<NP, CL
 
     // stage 0: the band of F; column items also take F 2 rows either side (clamped to the plane)
     float* Fsf = reinterpret_cast<float*>(Fs);
-    if (NA % 4 == 0) {
+    if (NA % 4 == 0) {  // every 16-byte piece of the band in flight at once
         for (int v = tid; v < B * NP * (AC / 4); v += S::NT) {
             const int hp = v % (AC / 4), p = v / (AC / 4);
-            float4 val{};
-            if (a0 + 4 * hp < NA)
-                val = *reinterpret_cast<const float4*>(in + static_cast<size_t>(z0 * NP + p) * NA + 4 * hp);
-            *reinterpret_cast<float4*>(Fsf + p * (2 * A2) + 4 * hp) = val;
+            const bool ok = a0 + 4 * hp < NA;
+            cp_async16(Fsf + p * (2 * A2) + 4 * hp, ok ? in + static_cast<size_t>(z0 * NP + p) * NA + 4 * hp : in, ok);
         }
     } else {
         for (int v = tid; v < B * NP * A2; v += S::NT) {
@@ -946,6 +956,7 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(ClusterPlane<NP, CL
         fa[0] = *reinterpret_cast<const float2*>(col + min(z1, N) * zs);
         fa[1] = *reinterpret_cast<const float2*>(col + min(z1 + 1, N) * zs);
     }
+    if (NA % 4 == 0) cp_async_wait_all();
     __syncthreads();
     // stage 1, y-part of div F (rows) into Ps
     if (row_item) {
