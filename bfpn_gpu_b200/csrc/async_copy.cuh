@@ -71,6 +71,17 @@ __device__ __forceinline__ void bulk_wait() {
     asm volatile("cp.async.bulk.wait_group %0;" ::"n"(N) : "memory");
 }
 
+// 16-byte global -> shared copy without a register round trip (cp.async,
+// L2 only); an invalid piece is filled with zeros (source size 0, nothing is
+// read from src).  cp_async_wait_all: every copy of this thread has landed.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, bool valid) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(valid ? 16 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
 // Orders this thread's earlier generic-proxy shared-memory accesses before
 // later async-proxy ones (bulk copies into a buffer just read).
 __device__ __forceinline__ void fence_proxy_async_smem() {

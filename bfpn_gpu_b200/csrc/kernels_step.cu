@@ -553,18 +553,17 @@ __global__ void __launch_bounds__((NP * AC + 31) / 32 * 32) transport_plane_kern
 
     constexpr int NT = (NP * AC + 31) / 32 * 32;  // == blockDim.x
     if (AC % Vec16<T>::W == 0 && NA % Vec16<T>::W == 0) {
-        // 16-byte loads, several in flight per thread (a0 and NA are multiples of
-        // the vector width, so a vector is wholly inside or wholly past NA)
-        using V = typename Vec16<T>::type;
+        // 16-byte pieces by cp.async, all in flight at once (a0 and NA are
+        // multiples of the vector width, so a piece is wholly inside or wholly past NA)
         constexpr int W = Vec16<T>::W, NV = NP * NP * AC / W;
 #pragma unroll 4
         for (int v = threadIdx.x; v < NV; v += NT) {
             const int e = v * W, aa = e % AC, p = e / AC;
             const int z = p / NP, y = p - z * NP;
-            V val{};
-            if (a0 + aa < NA) val = *reinterpret_cast<const V*>(in + static_cast<size_t>(p) * NA + aa);
-            *reinterpret_cast<V*>(Fs + z * RS + y * AC + aa) = val;
+            const bool ok = a0 + aa < NA;
+            cp_async16(Fs + z * RS + y * AC + aa, ok ? in + static_cast<size_t>(p) * NA + aa : in, ok);
         }
+        cp_async_wait_all();
     } else {
 #pragma unroll 4
         for (int e = threadIdx.x; e < NP * NP * AC; e += NT) {
@@ -686,16 +685,7 @@ __device__ __forceinline__ void walk_plane_line2(const float2* X, const float2* 
 
 __device__ __forceinline__ float2 max_lo2(float2 v, float lo) { return make_float2(fmaxf(v.x, lo), fmaxf(v.y, lo)); }
 
-// 16-byte global -> shared copy without a register round trip (cp.async,
-// L2 only); an invalid piece is filled with zeros (source size 0, nothing is
-// read from src).  cp_async_wait_all: every copy of this thread has landed.
-__device__ __forceinline__ void cp_async16(void* dst, const void* src, bool valid) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(valid ? 16 : 0)
-                 : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() {
-    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
-}
+
 
 template <int NP, int AC>
 __global__ void __launch_bounds__((NP * AC / 2 + 31) / 32 * 32) transport_plane_f2_kernel(TransportArgs<float> a,
@@ -1108,17 +1098,16 @@ __global__ void __launch_bounds__((R * AC + 31) / 32 * 32) transport_tile_kernel
     const T lo = a.preserve_sign ? -INFINITY : T(0);
 
     if (AC % Vec16<T>::W == 0 && NA % Vec16<T>::W == 0) {
-        using V = typename Vec16<T>::type;
         constexpr int W = Vec16<T>::W, NV = R * R * AC / W;
 #pragma unroll 4
         for (int v = threadIdx.x; v < NV; v += NT) {
             const int e = v * W, aa = e % AC, p = e / AC;
             const int lz = p / R, ly = p - lz * R;
             const int gy = min(max(ry0 + ly, 0), Ny), gz = min(max(rz0 + lz, 0), Nz);
-            V val{};
-            if (a0 + aa < NA) val = *reinterpret_cast<const V*>(in + (static_cast<size_t>(gz) * Ny1 + gy) * NA + aa);
-            *reinterpret_cast<V*>(Fs + lz * RS + ly * AC + aa) = val;
+            const bool ok = a0 + aa < NA;
+            cp_async16(Fs + lz * RS + ly * AC + aa, ok ? in + (static_cast<size_t>(gz) * Ny1 + gy) * NA + aa : in, ok);
         }
+        cp_async_wait_all();
     } else {
 #pragma unroll 4
         for (int e = threadIdx.x; e < R * R * AC; e += NT) {
