@@ -132,10 +132,18 @@ __global__ void __launch_bounds__(256) pack_source_operand_kernel(UmmaPackArgs a
     const int g = a.groups[gz];
     const float* __restrict__ src = (is_p2 ? a.P2 : a.P1) + (static_cast<size_t>(g) * a.nyz + pos) * a.NA;
     const bool row_ok = pos < a.nyz;
+    if (row_ok && (a.NA & 3) == 0 && k0 + 8 <= a.NA) {  // two 16-byte loads (row starts are 16-byte aligned)
+        const float4 u = __ldg(reinterpret_cast<const float4*>(src + k0));
+        const float4 w = __ldg(reinterpret_cast<const float4*>(src + k0 + 4));
+        x[0] = u.x; x[1] = u.y; x[2] = u.z; x[3] = u.w;
+        x[4] = w.x; x[5] = w.y; x[6] = w.z; x[7] = w.w;
+    } else {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) x[q] = (row_ok && k0 + q < a.NA) ? __ldg(src + k0 + q) : 0.f;
+    }
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
-        const float v = (row_ok && k0 + q < a.NA) ? __ldg(src + k0 + q) : 0.f;
-        x[q] = is_p2 ? v : fmaxf(v, 0.f);
+        if (!is_p2) x[q] = fmaxf(x[q], 0.f);
         r[q] = x[q] - __bfloat162float(__float2bfloat16_rn(x[q]));
     }
     uint4 hi, lo;
