@@ -172,6 +172,127 @@ __global__ void __launch_bounds__(NTH, MINB) energy_kernel(EnergyArgs<T> a) {
     }
 }
 
+// Float state, lanes a multiple of 4: each thread sweeps 4 consecutive lanes
+// and keeps its own ring of the next groups' old values in shared memory,
+// filled by 16-byte cp.async copies (no registers held by the prefetch, no
+// block barrier: a thread only reads what it copied).  Slot i % D holds group
+// Ng-1-i; the slot consumed in one iteration is refilled in the next, so up
+// to D-2 groups are in flight ahead of the one in use.  Same update and IDD
+// partials as energy_kernel.
+constexpr int kEnergyRing = 8, kEnergyRingThreads = 64;
+
+template <int MODE, int D, int NTH>
+__global__ void __launch_bounds__(NTH) energy_ring_kernel(EnergyArgs<float> a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float4* ring = reinterpret_cast<float4*>(smem_raw);  // [D][3][NTH]
+    const long long L = a.lanes;
+    const int Ng = a.Ng, tid = threadIdx.x;
+    const long long lane0 = (static_cast<long long>(blockIdx.x) * NTH + tid) * 4;
+    const bool ok = lane0 < L;  // L % 4 == 0: the 4 lanes are all in or all out
+    const float* __restrict__ sp = a.src;
+    auto slot = [&](int k, int arr) { return ring + (k * 3 + arr) * NTH + tid; };
+    auto fill = [&](int i) {  // group Ng-1-i into slot i % D, one commit group per call
+        const int e = Ng - 1 - i;
+        if (ok && e >= 0) {
+            const size_t off = static_cast<size_t>(e) * L + lane0;
+            cp_async16(slot(i % D, 0), a.F + off, true);
+            cp_async16(slot(i % D, 1), a.f + off, true);
+            if (sp) cp_async16(slot(i % D, 2), sp + off, true);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    for (int i = 0; i < D; ++i) fill(i);
+    double F_hi_old[4], f_hi_old[4], next_F[4], next_f[4], w_pos[4], acc = 0.0, accp = 0.0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        F_hi_old[j] = f_hi_old[j] = next_F[j] = next_f[j] = 0.0;
+        w_pos[j] = 1.0;
+        if (a.partials && a.trapezoidal && ok) {
+            const int pos = static_cast<int>((lane0 + j + a.lane0) / a.NA);
+            const int iy = pos % (a.Ny + 1), iz = pos / (a.Ny + 1);
+            if (iy == 0 || iy == a.Ny) w_pos[j] *= 0.5;
+            if (iz == 0 || iz == a.Nz) w_pos[j] *= 0.5;
+        }
+    }
+    constexpr bool kStrag = MODE == EMODE_EQ15_STRAG;
+    for (int i = 0; i < Ng; ++i) {
+        const int ek = Ng - 1 - i;
+        // groups 0 .. i (and i+1 for straggling) have landed
+        if (kStrag) asm volatile("cp.async.wait_group %0;" ::"n"(D - 3) : "memory");
+        else asm volatile("cp.async.wait_group %0;" ::"n"(D - 2) : "memory");
+        const float4 vF = *slot(i % D, 0), vf = *slot(i % D, 1);
+        const float4 vs = sp ? *slot(i % D, 2) : make_float4(0.f, 0.f, 0.f, 0.f);
+        float4 vn = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (kStrag && ek > 0) vn = *slot((i + 1) % D, 0);
+        if (i > 0) fill(i - 1 + D);  // the slot read in the previous iteration
+        const double* __restrict__ c = a.coef + ek * kEnergyCoef;
+        const double* __restrict__ dc = a.dose_coef + 2 * ek;
+        const float Fa[4] = {vF.x, vF.y, vF.z, vF.w}, fa[4] = {vf.x, vf.y, vf.z, vf.w};
+        const float sa[4] = {vs.x, vs.y, vs.z, vs.w}, na[4] = {vn.x, vn.y, vn.z, vn.w};
+        float Fo[4], fo[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const double Fg = Fa[j], fg = fa[j];
+            double Fv, fv;
+            energy_lane_update<MODE>(c, ek, Fg, fg, static_cast<double>(sa[j]), static_cast<double>(na[j]), F_hi_old[j],
+                                     f_hi_old[j], next_F[j], next_f[j], Fv, fv);
+            Fo[j] = static_cast<float>(Fv);
+            fo[j] = static_cast<float>(fv);
+            if (a.partials && ok) {
+                acc += w_pos[j] * (__ldg(dc) * static_cast<double>(Fo[j]) + __ldg(dc + 1) * static_cast<double>(fo[j]));
+                accp += static_cast<double>(fo[j]);
+            }
+            F_hi_old[j] = Fg;
+            f_hi_old[j] = fg;
+            next_F[j] = Fv;
+            next_f[j] = fv;
+        }
+        if (ok) {
+            const size_t off = static_cast<size_t>(ek) * L + lane0;
+            *reinterpret_cast<float4*>(a.F + off) = make_float4(Fo[0], Fo[1], Fo[2], Fo[3]);
+            *reinterpret_cast<float4*>(a.f + off) = make_float4(fo[0], fo[1], fo[2], fo[3]);
+        }
+    }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    if (a.partials) {
+        __shared__ double red[2][NTH / 32];
+        for (int o = 16; o > 0; o >>= 1) {
+            acc += __shfl_down_sync(0xffffffffu, acc, o);
+            accp += __shfl_down_sync(0xffffffffu, accp, o);
+        }
+        const int w = tid >> 5, l = tid & 31;
+        if (l == 0) {
+            red[0][w] = acc;
+            red[1][w] = accp;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            double s0 = 0.0, s1 = 0.0;
+            for (int k = 0; k < NTH / 32; ++k) {
+                s0 += red[0][k];
+                s1 += red[1][k];
+            }
+            a.partials[2 * blockIdx.x] = s0;
+            a.partials[2 * blockIdx.x + 1] = s1;
+        }
+    }
+}
+
+int energy_ring_grid(long long lanes) {
+    const long long per_block = 4LL * kEnergyRingThreads;
+    return static_cast<int>((lanes + per_block - 1) / per_block);
+}
+
+cudaError_t launch_energy_ring(const EnergyArgs<float>& a, cudaStream_t s) {
+    if (a.lanes % 4 != 0 || a.mode == EMODE_LEGACY) return cudaErrorNotSupported;
+    constexpr int D = kEnergyRing, NTH = kEnergyRingThreads;
+    const size_t smem = static_cast<size_t>(D) * 3 * NTH * sizeof(float4);
+    const int grid = energy_ring_grid(a.lanes);
+    if (a.mode == EMODE_EQ15) energy_ring_kernel<EMODE_EQ15, D, NTH><<<grid, NTH, smem, s>>>(a);
+    else energy_ring_kernel<EMODE_EQ15_STRAG, D, NTH><<<grid, NTH, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
 int energy_grid(long long lanes, int block) {
     const long long per_block = static_cast<long long>(block) * kEnergyLanesPerThread;
     return static_cast<int>((lanes + per_block - 1) / per_block);
@@ -180,6 +301,14 @@ int energy_grid(long long lanes, int block) {
 template <typename T>
 cudaError_t launch_energy(const EnergyArgs<T>& a, int block, cudaStream_t s) {
     constexpr int LPT = kEnergyLanesPerThread;
+    if constexpr (sizeof(T) == 4) {
+        // planes of at least 2^20 lanes fill the GPU with 64-thread ring blocks
+        // (4 lanes a thread); smaller ones keep more threads per SM with the
+        // register ring.  Same partial count: 4 * 64 lanes per block = 2 * 128.
+        if (a.lanes >= (1LL << 20) && a.lanes % 4 == 0 && a.mode != EMODE_LEGACY &&
+            block * LPT == 4 * kEnergyRingThreads)
+            return launch_energy_ring(a, s);
+    }
     const int grid = energy_grid(a.lanes, block);
     switch (a.mode) {
         case EMODE_EQ15: energy_kernel<EMODE_EQ15, T, LPT><<<grid, block, 0, s>>>(a); break;

@@ -262,6 +262,27 @@ def test_cluster_transport_matches_tiled_kernel(n):
         ctx.set_option(capi.OPT_CLUSTER_TRANSPORT, 3)
 
 
+@pytest.mark.parametrize("flags", [{}, {"eq15_straggling": True, "trapezoidal_yz": True}])
+def test_energy_ring_kernel_large_planes(flags):
+    """Planes of at least 2^20 lanes (64 x 64 positions x 16 x 16 angles) take
+    the mixed-precision energy sweep with a per-thread cp.async ring: the
+    energy operator against the FP64 oracle on the same float-rounded state,
+    and whole steps (fused IDD) against the FP64 path."""
+    cfg = small_cfg(ny=63, nz=63, nmu=16, nom=16, ng=8, ly=8.0, lz=8.0, **flags)
+    ctx, ora = build(cfg, precision=capi.PREC_MIXED)
+    states = [a.astype(np.float32).astype(np.float64) for a in seeded_states(ctx, 31)]
+    set_both(ctx, ora, states)
+    ctx.energy(0, 0.5 * cfg.dt())
+    ora.energy(0, 0.5 * cfg.dt())
+    assert_states(ctx, ora, 1e-6, ((0, 0), (0, 1)))
+    ctx.close()
+    fp, _ = build(cfg)
+    mix, _ = build(cfg, precision=capi.PREC_MIXED)
+    i64, _ = fp.step(4)
+    i32, _ = mix.step(4)
+    assert rel_err(i32, i64) < 1e-5
+
+
 def test_angle_operator():
     cfg = small_cfg(nmu=7, nom=6)
     ctx, ora = build(cfg)
