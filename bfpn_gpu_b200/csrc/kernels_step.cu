@@ -940,6 +940,7 @@ struct ClusterPlane {
     static constexpr int N = NP - 1;
     static constexpr int BZ = (NP + CL - 1) / CL;         // rows of the largest band
     static constexpr int YS = (NP + BZ - 1) / BZ;         // row segments
+    static constexpr int SL = (NP + YS - 1) / YS;         // cells of the longest segment
     static constexpr int YT = (BZ * A2 + 31) / 32 * 32;   // threads per row segment
     static constexpr int NT = (NP * A2 > YS * YT ? (NP * A2 + 31) / 32 * 32 : YS * YT);
     static constexpr int RS = NP * A2;                    // row stride (float2)
@@ -971,37 +972,36 @@ __device__ __forceinline__ void walk_get2(const Get& get, float2 wr, float2 h, c
     }
 }
 
-// Row segment [C0, C1) of a row at X (stride A2): faces C0 .. C1, cell = face - s.
-template <int N, int C0, int C1, int A2, typename Emit>
-__device__ __forceinline__ void walk_row_segment(const float2* X, float2 wr, float2 h, int s, const Emit& emit) {
-    constexpr int L = C1 - C0 + 4;
-    walk_get2<L>([&](int k) { return X[min(max(C0 - 2 + k, 0), N) * A2]; }, wr, h,
-                 [&](int i, float2 d, float2, float2) {
-                     const int cell = C0 + i - s;
-                     if (cell >= C0 && cell < C1) emit(cell, d);
-                 });
+// Row segment [c0, c1) of a row at X (stride A2), c1 - c0 <= SL: faces
+// c0 .. c0 + SL (those past c1 are walked on clamped loads and not emitted),
+// cell = face - s.  One code path for every segment of a row (small code).
+template <int N, int SL, int A2, typename Emit>
+__device__ __forceinline__ void walk_row_segment(const float2* X, int c0, int c1, float2 wr, float2 h, int s,
+                                                 const Emit& emit) {
+    walk_get2<SL + 4>([&](int k) { return X[min(max(c0 - 2 + k, 0), N) * A2]; }, wr, h,
+                      [&](int i, float2 d, float2, float2) {
+                          const int cell = c0 + i - s;
+                          if (cell >= c0 && cell < c1) emit(cell, d);
+                      });
 }
 
-template <int N, int YS, int K, int A2, typename Emit>
-__device__ __forceinline__ void walk_row_dispatch(int seg, const float2* X, float2 wr, float2 h, int s,
-                                                  const Emit& emit) {
-    if constexpr (K < YS) {
-        if (seg == K) {
-            walk_row_segment<N, K * (N + 1) / YS, (K + 1) * (N + 1) / YS, A2>(X, wr, h, s, emit);
-            return;
-        }
-        walk_row_dispatch<N, YS, K + 1, A2>(seg, X, wr, h, s, emit);
-    }
-}
-
-// Column over a band of B rows at Xb (stride RS) with 2 rows either side in
-// registers: faces z0 .. z0 + B, cell (band row) = face - z0 - s; emit gets
-// the X value of the cell as its third argument.
-template <int B, int RS, typename Emit>
-__device__ __forceinline__ void walk_band_column(const float2* Xb, const float2 (&below)[2], const float2 (&above)[2],
-                                                 float2 wr, float2 h, int s, const Emit& emit) {
-    walk_get2<B + 4>(
-        [&](int k) { return k < 2 ? below[k] : (k < B + 2 ? Xb[(k - 2) * RS] : above[k - B - 2]); }, wr, h,
+// Column over a band of B rows (B = BZ or BZ - 1) at Xb (stride RS), with 2
+// rows below and 3 above in registers: faces z0 .. z0 + BZ, cell (band row) =
+// face - z0 - s, emitted for cells < B; emit gets the X value of the cell as
+// its third argument.  One code path for both band heights.
+template <int BZ, int RS, typename Emit>
+__device__ __forceinline__ void walk_band_column(const float2* Xb, int B, const float2 (&below)[2],
+                                                 const float2 (&above)[3], float2 wr, float2 h, int s,
+                                                 const Emit& emit) {
+    const bool full = B == BZ;
+    walk_get2<BZ + 4>(
+        [&](int k) {
+            if (k < 2) return below[k];
+            if (k < BZ + 1) return Xb[(k - 2) * RS];
+            if (k == BZ + 1) return full ? Xb[(BZ - 1) * RS] : above[0];
+            return full ? above[k - BZ - 2] : above[k - BZ - 1];
+        },
+        wr, h,
         [&](int i, float2 d, float2 xm, float2 x0) {
             const int cell = i - s;
             if (cell >= 0 && cell < B) emit(cell, d, s ? xm : x0);
@@ -1067,13 +1067,13 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(ClusterPlane<NP, CL
             Fs[p * A2 + q] = val;
         }
     }
-    float2 fb[2] = {}, fa[2] = {};
+    float2 fb[2] = {}, fa[3] = {};
     if (col_item && a0 + 2 * cq < NA) {
         const float* col = in + static_cast<size_t>(cy) * NA + 2 * cq;
         fb[0] = *reinterpret_cast<const float2*>(col + max(z0 - 2, 0) * zs);
         fb[1] = *reinterpret_cast<const float2*>(col + max(z0 - 1, 0) * zs);
-        fa[0] = *reinterpret_cast<const float2*>(col + min(z1, N) * zs);
-        fa[1] = *reinterpret_cast<const float2*>(col + min(z1 + 1, N) * zs);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) fa[k] = *reinterpret_cast<const float2*>(col + min(z1 + k, N) * zs);
     }
     if (NA % 4 == 0) cp_async_wait_all();
     __syncthreads();
@@ -1084,8 +1084,8 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(ClusterPlane<NP, CL
         bool ok0, ok1;
         pair_setup(rq, wry, wrz, hy, hz, sy, sz, ok0, ok1);
         float2* D = Ps + rz * RS + rq;
-        walk_row_dispatch<N, S::YS, 0, A2>(seg, Fs + rz * RS + rq, wry, hy, sy,
-                                           [&](int cell, float2 d) { D[cell * A2] = d; });
+        walk_row_segment<N, S::SL, A2>(Fs + rz * RS + rq, seg * NP / S::YS, (seg + 1) * NP / S::YS, wry, hy, sy,
+                                       [&](int cell, float2 d) { D[cell * A2] = d; });
     }
     __syncthreads();
     // stage 1, z-part (columns): predictor into Ps, H over F
@@ -1101,8 +1101,7 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(ClusterPlane<NP, CL
             Pc[cell * RS] = max_lo2(__ffma2_rn(ndt, d, f), lo);
             Xc[cell * RS] = __ffma2_rn(nhdt, d, f);
         };
-        if (B == BZ) walk_band_column<BZ, RS>(Xc, fb, fa, wrz, hz, sz, emit);
-        else walk_band_column<BZ - 1, RS>(Xc, fb, fa, wrz, hz, sz, emit);
+        walk_band_column<BZ, RS>(Xc, B, fb, fa, wrz, hz, sz, emit);
     }
     cluster.barrier_arrive();  // this CTA's predictor rows are final
     __syncthreads();
@@ -1113,9 +1112,8 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(ClusterPlane<NP, CL
         bool ok0, ok1;
         pair_setup(rq, wry, wrz, hy, hz, sy, sz, ok0, ok1);
         float2* Fe = Fs + rz * RS + rq;
-        walk_row_dispatch<N, S::YS, 0, A2>(
-            seg, Ps + rz * RS + rq, wry, hy, sy,
-            [&](int cell, float2 d) { Fe[cell * A2] = __ffma2_rn(nhdt, d, Fe[cell * A2]); });
+        walk_row_segment<N, S::SL, A2>(Ps + rz * RS + rq, seg * NP / S::YS, (seg + 1) * NP / S::YS, wry, hy, sy,
+                                       [&](int cell, float2 d) { Fe[cell * A2] = __ffma2_rn(nhdt, d, Fe[cell * A2]); });
     }
     __syncthreads();
     cluster.barrier_wait();  // the neighbours' predictor rows are final
@@ -1126,7 +1124,7 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(ClusterPlane<NP, CL
         bool ok0, ok1;
         pair_setup(cq, wry, wrz, hy, hz, sy, sz, ok0, ok1);
         const int off = cy * A2 + cq;
-        float2 pb[2], pa[2];
+        float2 pb[2], pa[3];
         if (rank > 0) {
             const int Bm = z0 - (rank - 1) * NP / CL;  // rows of the band below
             const float2* rem = cluster.map_shared_rank(Ps, rank - 1);
@@ -1137,10 +1135,10 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(ClusterPlane<NP, CL
         }
         if (rank < CL - 1) {
             const float2* rem = cluster.map_shared_rank(Ps, rank + 1);
-            pa[0] = rem[off];
-            pa[1] = rem[RS + off];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) pa[k] = rem[k * RS + off];
         } else {
-            pa[0] = pa[1] = Ps[(B - 1) * RS + off];
+            pa[0] = pa[1] = pa[2] = Ps[(B - 1) * RS + off];
         }
         const float2* Fc = Fs + off;
         float* o = out + static_cast<size_t>(z0) * zs + static_cast<size_t>(cy) * NA + 2 * cq;
@@ -1150,8 +1148,7 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(ClusterPlane<NP, CL
             if (ok1) *reinterpret_cast<float2*>(dst) = v;
             else if (ok0) *dst = v.x;
         };
-        if (B == BZ) walk_band_column<BZ, RS>(Ps + off, pb, pa, wrz, hz, sz, emit);
-        else walk_band_column<BZ - 1, RS>(Ps + off, pb, pa, wrz, hz, sz, emit);
+        walk_band_column<BZ, RS>(Ps + off, B, pb, pa, wrz, hz, sz, emit);
     }
     cluster.sync();  // no CTA leaves while a neighbour still reads its rows
 }
