@@ -14,6 +14,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <type_traits>
 #include <string>
@@ -386,15 +387,23 @@ bfpn_status upload_as(bfpn_ctx* c, void* dst, const double* host, size_t n) {
         CUDA_TRY(c, cudaMemcpyAsync(dst, host, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
         return BFPN_OK;
     }
-    std::vector<T> tmp(host, host + n);
-    CUDA_TRY(c, cudaMemcpyAsync(dst, tmp.data(), n * sizeof(T), cudaMemcpyHostToDevice, c->stream));
+    // converted on the host's threads into a buffer they touch first
+    std::unique_ptr<T[]> tmp(new T[n]);
+    parallel_ranges(n, size_t(1) << 20, [&](size_t b, size_t e) {
+        for (size_t i = b; i < e; ++i) tmp[i] = static_cast<T>(host[i]);
+    });
+    CUDA_TRY(c, cudaMemcpyAsync(dst, tmp.get(), n * sizeof(T), cudaMemcpyHostToDevice, c->stream));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     return BFPN_OK;
 }
 
-bfpn_status upload_state_table(bfpn_ctx* c, void* dst, const std::vector<double>& h) {
-    return c->prec == BFPN_PREC_FP64 ? upload_as<double>(c, dst, h.data(), h.size())
-                                     : upload_as<float>(c, dst, h.data(), h.size());
+bfpn_status upload_state_table(bfpn_ctx* c, void* dst, const double* h, size_t n) {
+    return c->prec == BFPN_PREC_FP64 ? upload_as<double>(c, dst, h, n) : upload_as<float>(c, dst, h, n);
+}
+
+template <typename V>
+bfpn_status upload_state_table(bfpn_ctx* c, void* dst, const V& h) {
+    return upload_state_table(c, dst, h.data(), h.size());
 }
 
 bfpn_status upload_f64(bfpn_ctx* c, void* dst, const void* host, size_t bytes) {
@@ -939,27 +948,39 @@ bfpn_status check_device_error(bfpn_ctx* c) {
     return fail(c, BFPN_TIMEOUT, "a bounded device wait ran out (code " + std::to_string(h) + "); results of the step are invalid");
 }
 
-const std::vector<double>* table_of(const BeamTables& T, int which, std::vector<double>& tmp) {
+struct TableView {
+    const double* data;
+    size_t size;
+    bool known;
+};
+
+template <typename V>
+TableView view_of(const V& v) {
+    return TableView{v.data(), v.size(), true};
+}
+
+// known == false for an unknown table id
+TableView table_of(const BeamTables& T, int which, std::vector<double>& tmp) {
     switch (which) {
-        case BFPN_TABLE_S_S: return &T.S_s;
-        case BFPN_TABLE_T_C: return &T.T_c;
-        case BFPN_TABLE_SIG_TRG: return &T.sig_trg;
-        case BFPN_TABLE_SIGMA_C: return &T.sigma;
-        case BFPN_TABLE_EN: return &T.en;
-        case BFPN_TABLE_OMEND: return &T.omega;
-        case BFPN_TABLE_KER_E1: return &T.ker_e1;
-        case BFPN_TABLE_KER_E2: return &T.ker_e2;
-        case BFPN_TABLE_KER_V: return &T.ker_v;
+        case BFPN_TABLE_S_S: return view_of(T.S_s);
+        case BFPN_TABLE_T_C: return view_of(T.T_c);
+        case BFPN_TABLE_SIG_TRG: return view_of(T.sig_trg);
+        case BFPN_TABLE_SIGMA_C: return view_of(T.sigma);
+        case BFPN_TABLE_EN: return view_of(T.en);
+        case BFPN_TABLE_OMEND: return view_of(T.omega);
+        case BFPN_TABLE_KER_E1: return view_of(T.ker_e1);
+        case BFPN_TABLE_KER_E2: return view_of(T.ker_e2);
+        case BFPN_TABLE_KER_V: return view_of(T.ker_v);
         case BFPN_TABLE_BAND:
             tmp.resize(2 * static_cast<size_t>(T.Ng));
             for (int i = 0; i < T.Ng; ++i) {
                 tmp[2 * i] = T.band_begin[i];
                 tmp[2 * i + 1] = T.band_end[i];
             }
-            return &tmp;
-        case BFPN_TABLE_BEAM_YZA: return &T.beam_yza;
-        case BFPN_TABLE_BEAM_E: return &T.beam_e;
-        default: return nullptr;
+            return view_of(tmp);
+        case BFPN_TABLE_BEAM_YZA: return view_of(T.beam_yza);
+        case BFPN_TABLE_BEAM_E: return view_of(T.beam_e);
+        default: return TableView{nullptr, 0, false};
     }
 }
 
@@ -1020,11 +1041,11 @@ bfpn_status bfpn_host_table(const bfpn_grid* grid, const bfpn_phys* phys, const 
     BeamTables T;
     if (!build_tables(*grid, *phys, mu, mu_rows, sigma_c, sigma_rows, T, why)) return fail(nullptr, BFPN_INVALID_ARG, why);
     std::vector<double> tmp;
-    const std::vector<double>* src = table_of(T, which, tmp);
-    if (!src) return fail(nullptr, BFPN_INVALID_ARG, "unknown table id");
-    *n_out = src->size();
-    if (src->size() > n) return fail(nullptr, BFPN_INVALID_ARG, "output buffer too small for the table");
-    std::memcpy(out, src->data(), src->size() * sizeof(double));
+    const TableView src = table_of(T, which, tmp);
+    if (!src.known) return fail(nullptr, BFPN_INVALID_ARG, "unknown table id");
+    *n_out = src.size;
+    if (src.size > n) return fail(nullptr, BFPN_INVALID_ARG, "output buffer too small for the table");
+    if (src.size) std::memcpy(out, src.data, src.size * sizeof(double));
     return BFPN_OK;
 }
 
@@ -1277,7 +1298,6 @@ bfpn_status bfpn_load_tables(bfpn_ctx* c, const double* mu, int32_t mu_rows, con
         // tensor-core source: output tiles of <= 256 columns, multiples of 16
         c->umma_ntiles = (c->NA + 255) / 256;
         c->umma_nt = ((c->NA + c->umma_ntiles - 1) / c->umma_ntiles + 15) / 16 * 16;
-        std::vector<uint8_t> blob;
         // the packed split-bf16 copy of the A operand; without room for it the
         // source's angular stage stays on the fp32 CUDA-core kernel
         const size_t pack = umma_pack_bytes(c->n_groups, c->nyz, c->NA, c->umma_bk);
@@ -1286,12 +1306,13 @@ bfpn_status bfpn_load_tables(bfpn_ctx* c, const double* mu, int32_t mu_rows, con
             void* ab = nullptr;
             if (dalloc(c, &ab, pack) == BFPN_OK) c->ablob = ab;
         }
-        build_umma_blob(T.ker_v.data(), groups.data(), c->n_groups, c->NA, c->umma_nt, c->umma_bk, blob);
+        // B tiles from the float ker_v already on the device
         void* d = nullptr;
-        if ((s = dalloc(c, &d, blob.size())) != BFPN_OK) return s;
-        if ((s = upload_f64(c, d, blob.data(), blob.size())) != BFPN_OK) return s;
-        CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+        if ((s = dalloc(c, &d, umma_blob_bytes(c->n_groups, c->NA, c->umma_nt, c->umma_bk))) != BFPN_OK) return s;
         c->bblob = d;
+        CUDA_TRY(c, launch_build_umma_blob(as<const float>(c->ker_v), c->groups, c->n_groups, c->NA, c->umma_nt,
+                                           c->umma_bk, static_cast<uint8_t*>(d), c->stream));
+        CUDA_TRY(c, cudaStreamSynchronize(c->stream));
         // energy stage: banded coefficient tiles and per-output-tile work lists
         std::vector<uint8_t> eb;
         std::vector<int> work, begin;
@@ -1671,10 +1692,10 @@ bfpn_status bfpn_table_download(bfpn_ctx* c, int32_t which, double* host, uint64
     if (!c || !host) return BFPN_INVALID_ARG;
     if (!c->tables_loaded) return fail(c, BFPN_NOT_READY, "tables not loaded");
     std::vector<double> tmp;
-    const std::vector<double>* src = table_of(c->tables, which, tmp);
-    if (!src) return fail(c, BFPN_INVALID_ARG, "unknown table id");
-    if (src->size() > n) return fail(c, BFPN_INVALID_ARG, "host buffer too small for the table");
-    std::memcpy(host, src->data(), src->size() * sizeof(double));
+    const TableView src = table_of(c->tables, which, tmp);
+    if (!src.known) return fail(c, BFPN_INVALID_ARG, "unknown table id");
+    if (src.size > n) return fail(c, BFPN_INVALID_ARG, "host buffer too small for the table");
+    if (src.size) std::memcpy(host, src.data, src.size * sizeof(double));
     return BFPN_OK;
 }
 

@@ -171,10 +171,12 @@ size_t energy_umma_smem(int emax_cols);
 void build_energy_umma(const double* e1, const double* e2, const int* band_begin, const int* band_end, int Ng,
                        double dg, std::vector<uint8_t>& blob, std::vector<int>& work, std::vector<int>& begin,
                        int& emax_cols);
-// Host: split-bf16 B tiles of ker_v ([Ng][NA][NA] double) for the listed
-// groups, in the kernel's shared-memory layout.
-void build_umma_blob(const double* ker_v, const int* groups, int n_groups, int NA, int NT, int BK,
-                     std::vector<uint8_t>& blob);
+// Split-bf16 B tiles of the float ker_v ([Ng][NA][NA], device) for the listed
+// groups (device array), in the kernel's shared-memory layout, built on the
+// device into blob (umma_blob_bytes bytes).
+size_t umma_blob_bytes(int n_groups, int NA, int NT, int BK);
+cudaError_t launch_build_umma_blob(const float* ker_v, const int* groups, int n_groups, int NA, int NT, int BK,
+                                   uint8_t* blob, cudaStream_t s);
 
 // Dynamic shared memory of one transport block (tile ty x tz, ac angles).
 size_t transport_smem(int Ny1, int Nz1, int ty, int tz, int ac, size_t elem);

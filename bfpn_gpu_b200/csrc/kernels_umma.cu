@@ -642,34 +642,67 @@ void build_energy_umma(const double* e1, const double* e2, const int* band_begin
     }
 }
 
-// Host: B tiles of every used group in the device layout of the kernel above.
-void build_umma_blob(const double* ker_v, const int* groups, int n_groups, int NA, int NT, int BK,
-                     std::vector<uint8_t>& blob) {
-    const int nk = (NA + BK - 1) / BK;
-    const int n_ntiles = (NA + NT - 1) / NT;
+// B tiles of every used group in the device layout of the kernel above, built
+// on the device from the float copy of ker_v ([Ng][NA][NA], [src][in][out]):
+// one thread per 8-value k piece of one row n of one (group, n tile, k chunk)
+// tile writes the piece's bf16 hi and lo halves (16 bytes each); pieces past
+// NA are zeros.  Adjacent threads take adjacent rows, so the reads of ker_v
+// (consecutive n) coalesce.
+__global__ void build_umma_blob_kernel(const float* __restrict__ ker_v, const int* __restrict__ groups, int NA,
+                                       int NT, int BK, int n_ntiles, int nk, long long n_pieces,
+                                       uint8_t* __restrict__ blob) {
+    const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n_pieces) return;
+    const int kp = BK / 8;
+    const int nn = static_cast<int>(i % NT);
+    long long r = i / NT;
+    const int kh = static_cast<int>(r % kp);
+    r /= kp;
+    const int kc = static_cast<int>(r % nk);
+    r /= nk;
+    const int t = static_cast<int>(r % n_ntiles);
+    const int z = static_cast<int>(r / n_ntiles);
     const size_t part = static_cast<size_t>(NT) * BK * 2;
-    blob.assign(static_cast<size_t>(n_groups) * n_ntiles * nk * 2 * part, 0);
-    for (int z = 0; z < n_groups; ++z) {
-        const double* K = ker_v + static_cast<size_t>(groups[z]) * NA * NA;  // [in][out]
-        for (int t = 0; t < n_ntiles; ++t)
-            for (int kc = 0; kc < nk; ++kc) {
-                uint8_t* base = blob.data() + ((static_cast<size_t>(z) * n_ntiles + t) * nk + kc) * 2 * part;
-                for (int nn = 0; nn < NT; ++nn) {
-                    const int n = t * NT + nn;
-                    if (n >= NA) continue;
-                    for (int kk = 0; kk < BK; ++kk) {
-                        const int k = kc * BK + kk;
-                        if (k >= NA) continue;
-                        const float v = static_cast<float>(K[static_cast<size_t>(k) * NA + n]);
-                        const __nv_bfloat16 h = __float2bfloat16_rn(v);
-                        const __nv_bfloat16 l = __float2bfloat16_rn(v - __bfloat162float(h));
-                        const size_t off = umma_kmajor_offset(nn, kk, NT);
-                        std::memcpy(base + off, &h, 2);
-                        std::memcpy(base + part + off, &l, 2);
-                    }
-                }
-            }
+    uint8_t* base = blob + ((static_cast<size_t>(z) * n_ntiles + t) * nk + kc) * 2 * part;
+    const int n = t * NT + nn, k0 = kc * BK + kh * 8;
+    const float* K = ker_v + static_cast<size_t>(groups[z]) * NA * NA;
+    uint32_t hw[4], lw[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        __nv_bfloat16 h2[2], l2[2];
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            const int k = k0 + 2 * q + e;
+            const float v = (n < NA && k < NA) ? K[static_cast<size_t>(k) * NA + n] : 0.f;
+            h2[e] = __float2bfloat16_rn(v);
+            l2[e] = __float2bfloat16_rn(v - __bfloat162float(h2[e]));
+        }
+        hw[q] = static_cast<uint32_t>(__bfloat16_as_ushort(h2[0])) |
+                (static_cast<uint32_t>(__bfloat16_as_ushort(h2[1])) << 16);
+        lw[q] = static_cast<uint32_t>(__bfloat16_as_ushort(l2[0])) |
+                (static_cast<uint32_t>(__bfloat16_as_ushort(l2[1])) << 16);
     }
+    const size_t off = umma_kmajor_offset(nn, kh * 8, NT);
+    *reinterpret_cast<uint4*>(base + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+    *reinterpret_cast<uint4*>(base + part + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+}
+
+size_t umma_blob_bytes(int n_groups, int NA, int NT, int BK) {
+    const size_t nk = (NA + BK - 1) / BK, n_ntiles = (NA + NT - 1) / NT;
+    return static_cast<size_t>(n_groups) * n_ntiles * nk * 2 * static_cast<size_t>(NT) * BK * 2;
+}
+
+cudaError_t launch_build_umma_blob(const float* ker_v, const int* groups, int n_groups, int NA, int NT, int BK,
+                                   uint8_t* blob, cudaStream_t s) {
+    if (n_groups <= 0) return cudaSuccess;
+    if (BK % 8 != 0 || NT % 8 != 0) return cudaErrorInvalidValue;
+    const int nk = (NA + BK - 1) / BK, n_ntiles = (NA + NT - 1) / NT;
+    const long long n_pieces = static_cast<long long>(n_groups) * n_ntiles * nk * (BK / 8) * NT;
+    const long long grid = (n_pieces + 255) / 256;
+    if (grid > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+    build_umma_blob_kernel<<<static_cast<unsigned>(grid), 256, 0, s>>>(ker_v, groups, NA, NT, BK, n_ntiles, nk,
+                                                                       n_pieces, blob);
+    return cudaGetLastError();
 }
 
 }  // namespace bfpn

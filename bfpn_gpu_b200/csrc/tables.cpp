@@ -10,6 +10,7 @@
 #include <cmath>
 #include <fstream>
 #include <atomic>
+#include <cstdint>
 #include <limits>
 #include <thread>
 
@@ -170,9 +171,18 @@ void energy_kernels(BeamTables& t) {
 // with mu1, mu2 != 0, a column-normalised theta^(mu1-1) exp(-theta/mu2)
 // (1+|w_in|^2)^-1.5 over the input directions, entries below 1e-3 after
 // normalisation dropped.  The last group carries no kernel.
+//
+// Same values as the reference's loop, built faster: theta(in, out) takes far
+// fewer distinct values than NA^2 (it is symmetric bit for bit, and shifted
+// direction pairs repeat), so theta^(mu1-1) exp(-theta/mu2) is evaluated once
+// per distinct value and group; the rows are then filled in memory order,
+// each column sum still adding its inputs in increasing order.  Groups are
+// spread over the host's threads, and each thread is the first to touch the
+// table pages it fills.
 void angular_kernel(BeamTables& t) {
     const int NA = t.NA, Ng = t.Ng;
-    std::vector<double> theta(static_cast<size_t>(NA) * NA);  // [in][out], degrees
+    const size_t NA2 = static_cast<size_t>(NA) * NA;
+    std::vector<double> theta(NA2);  // [in][out], degrees
     for (int out = 0; out < NA; ++out) {
         const double oy = t.omega[2 * out], oz = t.omega[2 * out + 1];
         const double on = std::sqrt(1.0 + oy * oy + oz * oz);
@@ -189,41 +199,58 @@ void angular_kernel(BeamTables& t) {
         const double iy = t.omega[2 * in], iz = t.omega[2 * in + 1];
         jac[in] = std::pow(1.0 + iy * iy + iz * iz, -1.5);
     }
-    t.ker_v.assign(static_cast<size_t>(Ng) * NA * NA, 0.0);
-    auto group = [&](int ek) {
+    // distinct theta values (all finite and >= +0, so == separates bit patterns)
+    std::vector<double> uniq(theta);
+    std::sort(uniq.begin(), uniq.end());
+    uniq.erase(std::unique(uniq.begin(), uniq.end()), uniq.end());
+    const size_t U = uniq.size();
+    std::vector<uint32_t> idx(NA2);
+    for (size_t i = 0; i < NA2; ++i)
+        idx[i] = static_cast<uint32_t>(std::lower_bound(uniq.begin(), uniq.end(), theta[i]) - uniq.begin());
+    t.ker_v.resize(static_cast<size_t>(Ng) * NA2);  // uninitialised: every group's block is written below
+    auto group = [&](int ek, std::vector<double>& f, std::vector<double>& col) {
+        double* K = t.ker_v.data() + static_cast<size_t>(ek) * NA2;
         const double m1 = t.mu[ek * 3], m2 = t.mu[ek * 3 + 1];
-        if (m1 == 0.0 || m2 == 0.0) return;
-        double* K = t.ker_v.data() + static_cast<size_t>(ek) * NA * NA;
-        for (int out = 0; out < NA; ++out) {
-            double col = 0.0;
-            for (int in = 0; in < NA; ++in) {
-                double v = std::pow(theta[static_cast<size_t>(in) * NA + out], m1 - 1.0)
-                           * std::exp(-theta[static_cast<size_t>(in) * NA + out] / m2) * jac[in];
+        if (ek == Ng - 1 || m1 == 0.0 || m2 == 0.0) {
+            std::fill(K, K + NA2, 0.0);
+            return;
+        }
+        for (size_t u = 0; u < U; ++u) f[u] = std::pow(uniq[u], m1 - 1.0) * std::exp(-uniq[u] / m2);
+        std::fill(col.begin(), col.end(), 0.0);
+        for (int in = 0; in < NA; ++in) {
+            const double j = jac[in];
+            const uint32_t* ir = idx.data() + static_cast<size_t>(in) * NA;
+            double* Kr = K + static_cast<size_t>(in) * NA;
+            for (int out = 0; out < NA; ++out) {
+                double v = f[ir[out]] * j;
                 if (!std::isfinite(v)) v = 0.0;
-                K[static_cast<size_t>(in) * NA + out] = v;
-                col += v;
+                Kr[out] = v;
+                col[out] += v;
             }
-            if (col > kEpsilon)
-                for (int in = 0; in < NA; ++in) {
-                    double& v = K[static_cast<size_t>(in) * NA + out];
-                    v /= col;
+        }
+        for (int in = 0; in < NA; ++in) {
+            double* Kr = K + static_cast<size_t>(in) * NA;
+            for (int out = 0; out < NA; ++out)
+                if (col[out] > kEpsilon) {
+                    double v = Kr[out] / col[out];
                     if (v < kKernelThreshold) v = 0.0;
+                    Kr[out] = v;
                 }
         }
     };
-    // groups are independent: split them over the host's cores (same values
-    // whatever the split)
     const int n_threads = static_cast<int>(std::max(1u, std::min(32u, std::thread::hardware_concurrency())));
     const long long work = static_cast<long long>(Ng) * NA * NA;
     if (n_threads == 1 || work < (1 << 20)) {
-        for (int ek = 0; ek < Ng - 1; ++ek) group(ek);
+        std::vector<double> f(U), col(NA);
+        for (int ek = 0; ek < Ng; ++ek) group(ek, f, col);
         return;
     }
     std::atomic<int> next{0};
     std::vector<std::thread> pool;
     for (int i = 0; i < n_threads; ++i)
         pool.emplace_back([&] {
-            for (int ek = next++; ek < Ng - 1; ek = next++) group(ek);
+            std::vector<double> f(U), col(NA);
+            for (int ek = next++; ek < Ng; ek = next++) group(ek, f, col);
         });
     for (auto& th : pool) th.join();
 }
@@ -300,6 +327,22 @@ bool beam_factors(const bfpn_grid& g, const bfpn_phys& p, BeamTables& t, std::st
 }
 
 }  // namespace
+
+void parallel_ranges(size_t n, size_t min_per_thread, const std::function<void(size_t, size_t)>& f) {
+    const size_t hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    const size_t nt = std::min(hw, std::max<size_t>(1, n / std::max<size_t>(1, min_per_thread)));
+    if (nt <= 1) {
+        f(0, n);
+        return;
+    }
+    const size_t per = (n + nt - 1) / nt;
+    std::vector<std::thread> pool;
+    for (size_t i = 0; i < nt; ++i) {
+        const size_t b = i * per, e = std::min(n, b + per);
+        if (b < e) pool.emplace_back(f, b, e);
+    }
+    for (auto& th : pool) th.join();
+}
 
 Deltas compute_deltas(const bfpn_grid& g) {
     Deltas d;

@@ -5,10 +5,41 @@
 
 #include "../../include/bfpn_capi.h"
 
+#include <cstddef>
+#include <functional>
+#include <new>
 #include <string>
+#include <utility>
 #include <vector>
 
 namespace bfpn {
+
+// Allocator whose new elements are left uninitialised: a large table is first
+// written (and so first touched) by the threads that fill it, instead of
+// being zeroed page by page on one thread beforehand.
+template <typename T>
+struct UninitAlloc : std::allocator<T> {
+    template <typename U>
+    struct rebind {
+        using other = UninitAlloc<U>;
+    };
+    UninitAlloc() = default;
+    template <typename U>
+    UninitAlloc(const UninitAlloc<U>&) noexcept {}
+    template <typename U>
+    void construct(U* p) noexcept {
+        ::new (static_cast<void*>(p)) U;
+    }
+    template <typename U, typename... A>
+    void construct(U* p, A&&... args) {
+        ::new (static_cast<void*>(p)) U(std::forward<A>(args)...);
+    }
+};
+using HostTable = std::vector<double, UninitAlloc<double>>;
+
+// Runs f(begin, end) over [0, n) split into contiguous ranges, one per host
+// thread (up to 32); one call on the caller's thread when n < min_per_thread.
+void parallel_ranges(size_t n, size_t min_per_thread, const std::function<void(size_t, size_t)>& f);
 
 struct Deltas {
     double dt, dy, dz, dg, du, dv;
@@ -29,7 +60,7 @@ struct BeamTables {
     std::vector<double> omega;     // NA x 2 (omega_y, omega_z)
     std::vector<double> ker_e1, ker_e2;  // Ng x Ng, row = output group, column = source group
     std::vector<int> band_begin, band_end;  // per output group
-    std::vector<double> ker_v;     // Ng x NA x NA, [src][in][out]
+    HostTable ker_v;               // Ng x NA x NA, [src][in][out]
     std::vector<double> sine_u, sine_v;     // Nom x Nom, Nmu x Nmu
     std::vector<double> beam_yza;  // nyz x NA  (initial-beam transverse/angular factor)
     std::vector<double> beam_e;    // Ng        (initial-beam energy factor)
