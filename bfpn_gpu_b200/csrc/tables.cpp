@@ -216,7 +216,16 @@ void angular_kernel(BeamTables& t) {
             return;
         }
         for (size_t u = 0; u < U; ++u) f[u] = std::pow(uniq[u], m1 - 1.0) * std::exp(-uniq[u] / m2);
+        // column sums first, then each entry written once, already normalised
         std::fill(col.begin(), col.end(), 0.0);
+        for (int in = 0; in < NA; ++in) {
+            const double j = jac[in];
+            const uint32_t* ir = idx.data() + static_cast<size_t>(in) * NA;
+            for (int out = 0; out < NA; ++out) {
+                const double v = f[ir[out]] * j;
+                col[out] += std::isfinite(v) ? v : 0.0;
+            }
+        }
         for (int in = 0; in < NA; ++in) {
             const double j = jac[in];
             const uint32_t* ir = idx.data() + static_cast<size_t>(in) * NA;
@@ -224,18 +233,12 @@ void angular_kernel(BeamTables& t) {
             for (int out = 0; out < NA; ++out) {
                 double v = f[ir[out]] * j;
                 if (!std::isfinite(v)) v = 0.0;
-                Kr[out] = v;
-                col[out] += v;
-            }
-        }
-        for (int in = 0; in < NA; ++in) {
-            double* Kr = K + static_cast<size_t>(in) * NA;
-            for (int out = 0; out < NA; ++out)
                 if (col[out] > kEpsilon) {
-                    double v = Kr[out] / col[out];
+                    v /= col[out];
                     if (v < kKernelThreshold) v = 0.0;
-                    Kr[out] = v;
                 }
+                Kr[out] = v;
+            }
         }
     };
     const int n_threads = static_cast<int>(std::max(1u, std::min(32u, std::thread::hardware_concurrency())));
