@@ -36,7 +36,7 @@ FLAG_LITE_MEMORY = 1 << 13
 FLAG_STREAMING_FULL = 1 << 14
 # run-time options
 (OPT_TENSOR_CORES, OPT_CUDA_GRAPHS, OPT_PLANE_TRANSPORT, OPT_PAIRED_ANGLES, OPT_CLUSTER_TRANSPORT, OPT_LANE_CHUNK,
- OPT_ENERGY_CHUNK) = range(7)
+ OPT_ENERGY_CHUNK, OPT_STEP_OVERLAP) = range(8)
 # kernel classes of the profile
 KERNEL_CLASSES = ["energy", "transport", "angle", "source_angular", "source_energy", "idd"]
 # tables

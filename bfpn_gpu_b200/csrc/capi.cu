@@ -131,6 +131,14 @@ struct bfpn_ctx {
     cudaGraphExec_t graph_exec = nullptr;
     int graph_key = -1;
     bool use_graphs = true;
+    // overlapped steps: the secondary half of step n (source, energy and
+    // transport of the secondary species, the step's IDD) runs on s_sec beside
+    // the primary half of step n+1; graph ovl_exec[p] serves steps of parity p
+    bool overlap = true;
+    bool pending_sec = false;  // the secondary half of step steps_done-1 is still owed
+    cudaStream_t s_sec = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_pread = nullptr, ev_join = nullptr;
+    cudaGraphExec_t ovl_exec[2] = {nullptr, nullptr};
     bool profiling = false;
     struct Pending {
         int cls;
@@ -307,6 +315,18 @@ void dfree(bfpn_ctx* c, void*& p) {
     p = nullptr;
 }
 
+// Step graphs capture buffer addresses and kernel choices: dropped whenever
+// either changes.
+void drop_graphs(bfpn_ctx* c) {
+    if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+    c->graph_exec = nullptr;
+    c->graph_key = -1;
+    for (auto& g : c->ovl_exec) {
+        if (g) cudaGraphExecDestroy(g);
+        g = nullptr;
+    }
+}
+
 void free_all(bfpn_ctx* c) {
     for (auto& p : c->pending) {
         cudaEventDestroy(p.a);
@@ -315,8 +335,14 @@ void free_all(bfpn_ctx* c) {
     c->pending.clear();
     for (auto e : c->ev_pool) cudaEventDestroy(e);
     c->ev_pool.clear();
-    if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
-    c->graph_exec = nullptr;
+    drop_graphs(c);
+    for (cudaEvent_t* e : {&c->ev_fork, &c->ev_pread, &c->ev_join})
+        if (*e) {
+            cudaEventDestroy(*e);
+            *e = nullptr;
+        }
+    if (c->s_sec) cudaStreamDestroy(c->s_sec);
+    c->s_sec = nullptr;
     for (auto& b : c->allocs) cudaFree(b.p);
     c->allocs.clear();
     for (void* p : c->host_allocs) cudaFreeHost(p);
@@ -482,9 +508,11 @@ cudaError_t enq_angle(bfpn_ctx* c, void* X, const void* fac, int ng = -1) {
 
 // The source from primary arrays P1, P2 of nyz positions (row stride
 // nyz * NA) into S; A1 / A2 (and the tensor-core operand) in the context's
-// A block, sized for those positions.
+// A block, sized for those positions.  pread (may be null) is recorded once
+// the last kernel that reads P1 and P2 has been enqueued.
 template <typename T>
-cudaError_t enq_source_on(bfpn_ctx* c, const void* P1, const void* P2, void* S, int nyz) {
+cudaError_t enq_source_on(bfpn_ctx* c, const void* P1, const void* P2, void* S, int nyz,
+                          cudaEvent_t pread = nullptr) {
     SourceArgs<T> a;
     a.P1 = as<const T>(const_cast<void*>(P1));
     a.P2 = as<const T>(const_cast<void*>(P2));
@@ -513,7 +541,7 @@ cudaError_t enq_source_on(bfpn_ctx* c, const void* P1, const void* P2, void* S, 
                                               as<const float>(const_cast<void*>(P2)),
                                               static_cast<uint8_t*>(c->ablob), static_cast<const uint8_t*>(c->bblob),
                                               c->groups, c->n_groups, q, c->Ng, c->dev_err, nyz, c->NA,
-                                              c->umma_nt, c->umma_bk, c->umma_ntiles, c->stream);
+                                              c->umma_nt, c->umma_bk, c->umma_ntiles, c->stream, pread);
         });
         if (e != cudaSuccess) return e;
         return prof(c, BFPN_KERNEL_SOURCE_ENERGY, [&] {
@@ -523,12 +551,13 @@ cudaError_t enq_source_on(bfpn_ctx* c, const void* P1, const void* P2, void* S, 
     }
     e = prof(c, BFPN_KERNEL_SOURCE_ANGULAR, [&] { return launch_source_angular<T>(a, c->stream); });
     if (e != cudaSuccess) return e;
+    if (pread && (e = cudaEventRecord(pread, c->stream)) != cudaSuccess) return e;
     return prof(c, BFPN_KERNEL_SOURCE_ENERGY, [&] { return launch_source_energy<T>(a, c->tile_e, c->stream); });
 }
 
 template <typename T>
-cudaError_t enq_source(bfpn_ctx* c) {
-    return enq_source_on<T>(c, c->st[0][0], c->st[0][1], c->src, c->nyz);
+cudaError_t enq_source(bfpn_ctx* c, cudaEvent_t pread = nullptr) {
+    return enq_source_on<T>(c, c->st[0][0], c->st[0][1], c->src, c->nyz, pread);
 }
 
 // transport half-step, angle full step, transport half-step on one array
@@ -572,38 +601,68 @@ cudaError_t enq_lite_step(bfpn_ctx* c) {
     });
 }
 
+// IDD partial sums of the primary's last energy pass, by step parity (the
+// secondary half of one step and the primary half of the next can be in
+// flight together).
+double* primary_partials(bfpn_ctx* c, int step) {
+    return c->partials + ((step & 1) ? 4 : 0) * static_cast<size_t>(c->n_part);
+}
+
+// stepPrimary (bfpm_solver.cu:3238-3311) / stepPrimaryEnergyOnly (3313-3333),
+// the last energy pass writing the IDD partials into partP.
 template <typename T>
-cudaError_t enq_step(bfpn_ctx* c, bool first, bool secondary_zero) {
-    if (c->lite) return enq_lite_step<T>(c);
+cudaError_t enq_primary_half(bfpn_ctx* c, double* partP) {
     const unsigned fl = c->p.flags;
-    const bool energy_only = fl & BFPN_FLAG_ENERGY_ONLY;
-    const bool do_tr = !(fl & BFPN_FLAG_NO_TRANSPORT), do_an = !(fl & BFPN_FLAG_NO_ANGLE);
-    double* partP = c->partials;
-    double* partS = c->partials + 2 * c->n_part;
     cudaError_t e;
-    // stepPrimary (3238-3311) / stepPrimaryEnergyOnly (3313-3333)
     if ((e = enq_energy<T>(c, 0, c->ecoef_half, false, nullptr)) != cudaSuccess) return e;
-    if (!energy_only) {
+    if (!(fl & BFPN_FLAG_ENERGY_ONLY)) {
+        const bool do_tr = !(fl & BFPN_FLAG_NO_TRANSPORT), do_an = !(fl & BFPN_FLAG_NO_ANGLE);
         const bool clip_F = !(fl & BFPN_FLAG_NO_SPATIAL_CLIPPING);
         if ((e = enq_tat<T>(c, 0, 0, do_tr, do_an, !clip_F)) != cudaSuccess) return e;
         if ((e = enq_tat<T>(c, 0, 1, do_tr, do_an, true)) != cudaSuccess) return e;
     }
-    if ((e = enq_energy<T>(c, 0, c->ecoef_half, false, partP)) != cudaSuccess) return e;
+    return enq_energy<T>(c, 0, c->ecoef_half, false, partP);
+}
+
+template <typename T>
+cudaError_t enq_finalize(bfpn_ctx* c, const double* partP, const double* partS, int nS) {
     const int nP = energy_grid(c->per_e, c->energy_block);
+    const double w = c->d.du * c->d.dv * c->d.dy * c->d.dz;
+    return prof(c, BFPN_KERNEL_IDD, [&] {
+        return launch_finalize_idd(partP, nP, partS, nS, w, c->d.dg, c->hist_idd, c->hist_proxy, c->counter,
+                                   c->hist_cap, 1, c->stream);
+    });
+}
+
+// stepSecondary (3335-3394) and the step's IDD (partP from its primary
+// half): the source depends only on the primary, which this half does not
+// change, so both of the reference's evaluations are the same tensor; it is
+// built once.  Transport of the secondary always clips F1 (3355-3356) and
+// always runs.  pread: see enq_source_on.
+template <typename T>
+cudaError_t enq_secondary_half(bfpn_ctx* c, const double* partP, cudaEvent_t pread) {
+    double* partS = c->partials + 2 * static_cast<size_t>(c->n_part);
+    cudaError_t e;
+    if ((e = enq_source<T>(c, pread)) != cudaSuccess) return e;
+    if ((e = enq_energy<T>(c, 1, c->ecoef_half, true, nullptr)) != cudaSuccess) return e;
+    if ((e = enq_tat<T>(c, 1, 0, true, true, false)) != cudaSuccess) return e;
+    if ((e = enq_tat<T>(c, 1, 1, true, true, true)) != cudaSuccess) return e;
+    if ((e = enq_energy<T>(c, 1, c->ecoef_half, true, partS)) != cudaSuccess) return e;
+    return enq_finalize<T>(c, partP, partS, energy_grid(c->per_e, c->energy_block));
+}
+
+template <typename T>
+cudaError_t enq_step(bfpn_ctx* c, bool first, bool secondary_zero) {
+    if (c->lite) return enq_lite_step<T>(c);
+    const unsigned fl = c->p.flags;
+    double* partP = primary_partials(c, c->steps_done);
+    double* partS = c->partials + 2 * static_cast<size_t>(c->n_part);
+    cudaError_t e;
+    if ((e = enq_primary_half<T>(c, partP)) != cudaSuccess) return e;
+    const bool secondary = !(fl & (BFPN_FLAG_ENERGY_ONLY | BFPN_FLAG_PRIMARY_ONLY)) && !first;
+    if (secondary) return enq_secondary_half<T>(c, partP, nullptr);
     int nS = 0;
-    const bool secondary = !energy_only && !(fl & BFPN_FLAG_PRIMARY_ONLY) && !first;
-    if (secondary) {
-        // stepSecondary (3335-3394): the source depends only on the primary,
-        // which this half does not change, so both of the reference's
-        // evaluations are the same tensor; it is built once.  Transport of
-        // the secondary always clips F1 (3355-3356) and always runs.
-        if ((e = enq_source<T>(c)) != cudaSuccess) return e;
-        if ((e = enq_energy<T>(c, 1, c->ecoef_half, true, nullptr)) != cudaSuccess) return e;
-        if ((e = enq_tat<T>(c, 1, 0, true, true, false)) != cudaSuccess) return e;
-        if ((e = enq_tat<T>(c, 1, 1, true, true, true)) != cudaSuccess) return e;
-        if ((e = enq_energy<T>(c, 1, c->ecoef_half, true, partS)) != cudaSuccess) return e;
-        nS = nP;
-    } else if (!secondary_zero) {
+    if (!secondary_zero) {
         nS = idd_partials_grid(c->per_e);
         e = prof(c, BFPN_KERNEL_IDD, [&] {
             return launch_idd_partials<T>(as<const T>(c->st[1][0]), as<const T>(c->st[1][1]), c->dose_coef, c->Ng,
@@ -612,11 +671,32 @@ cudaError_t enq_step(bfpn_ctx* c, bool first, bool secondary_zero) {
         });
         if (e != cudaSuccess) return e;
     }
-    const double w = c->d.du * c->d.dv * c->d.dy * c->d.dz;
-    return prof(c, BFPN_KERNEL_IDD, [&] {
-        return launch_finalize_idd(partP, nP, partS, nS, w, c->d.dg, c->hist_idd, c->hist_proxy, c->counter,
-                                   c->hist_cap, 1, c->stream);
-    });
+    return enq_finalize<T>(c, partP, partS, nS);
+}
+
+// Overlapped form of regular steps (one context stream, the secondary half on
+// s_sec):
+//   body(n) = [secondary half of step n-1 + its IDD] on s_sec, beside
+//             [primary half of step n] on the context stream,
+// where the primary's first kernel waits for the event recorded after the
+// source's last read of the primary (the pack), and the body joins s_sec
+// back before it ends.  The primary half of step n writes the partials of
+// parity n while the secondary half of n-1 reads those of parity n-1.  Same
+// kernels on the same inputs as the sequential order, so the same values.
+template <typename T>
+cudaError_t enq_overlap_body(bfpn_ctx* c, int step) {
+    cudaError_t e;
+    if ((e = cudaEventRecord(c->ev_fork, c->stream)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(c->s_sec, c->ev_fork, 0)) != cudaSuccess) return e;
+    cudaStream_t main = c->stream;
+    c->stream = c->s_sec;
+    e = enq_secondary_half<T>(c, primary_partials(c, step - 1), c->ev_pread);
+    c->stream = main;
+    if (e != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(c->stream, c->ev_pread, 0)) != cudaSuccess) return e;
+    if ((e = enq_primary_half<T>(c, primary_partials(c, step))) != cudaSuccess) return e;
+    if ((e = cudaEventRecord(c->ev_join, c->s_sec)) != cudaSuccess) return e;
+    return cudaStreamWaitEvent(c->stream, c->ev_join, 0);
 }
 
 cudaError_t enq_step_any(bfpn_ctx* c, bool first, bool secondary_zero) {
@@ -852,11 +932,66 @@ bfpn_status ensure_history(bfpn_ctx* c, int needed) {
     c->hist_idd = static_cast<double*>(ni);
     c->hist_proxy = static_cast<double*>(np);
     c->hist_cap = cap;
-    if (c->graph_exec) {
-        cudaGraphExecDestroy(c->graph_exec);
-        c->graph_exec = nullptr;
-        c->graph_key = -1;
+    drop_graphs(c);
+    return BFPN_OK;
+}
+
+// Regular steps of this context may overlap: graphs on, the standard
+// operator set, transport in place (no shared scratch array).
+bool overlap_ok(const bfpn_ctx* c) {
+    const unsigned fl = c->p.flags;
+    return c->overlap && c->use_graphs && !c->lite && !c->ooc && transport_in_place(c) &&
+           !(fl & (BFPN_FLAG_ENERGY_ONLY | BFPN_FLAG_PRIMARY_ONLY | BFPN_FLAG_NO_TRANSPORT | BFPN_FLAG_NO_ANGLE));
+}
+
+bfpn_status ensure_overlap_objects(bfpn_ctx* c) {
+    if (c->s_sec) return BFPN_OK;
+    CUDA_TRY(c, cudaStreamCreateWithFlags(&c->s_sec, cudaStreamNonBlocking));
+    for (cudaEvent_t* e : {&c->ev_fork, &c->ev_pread, &c->ev_join})
+        CUDA_TRY(c, cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    return BFPN_OK;
+}
+
+// The owed secondary half of step steps_done-1, enqueued on the context stream.
+bfpn_status flush_secondary(bfpn_ctx* c) {
+    if (!c->pending_sec) return BFPN_OK;
+    c->pending_sec = false;
+    const double* partP = primary_partials(c, c->steps_done - 1);
+    if (c->prec == BFPN_PREC_FP64) CUDA_TRY(c, enq_secondary_half<double>(c, partP, nullptr));
+    else CUDA_TRY(c, enq_secondary_half<float>(c, partP, nullptr));
+    return BFPN_OK;
+}
+
+// One overlapped regular step (step = steps_done): the primary half alone
+// when no secondary half is owed, else the captured body of its parity.
+bfpn_status overlap_step(bfpn_ctx* c) {
+    const int step = c->steps_done;
+    if (!c->pending_sec) {
+        double* partP = primary_partials(c, step);
+        if (c->prec == BFPN_PREC_FP64) CUDA_TRY(c, enq_primary_half<double>(c, partP));
+        else CUDA_TRY(c, enq_primary_half<float>(c, partP));
+        c->pending_sec = true;
+        return BFPN_OK;
     }
+    cudaGraphExec_t& g = c->ovl_exec[step & 1];
+    if (!g) {
+        cudaGraph_t graph = nullptr;
+        CUDA_TRY(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        const long long before = c->launches;
+        cudaError_t ce = c->prec == BFPN_PREC_FP64 ? enq_overlap_body<double>(c, step) : enq_overlap_body<float>(c, step);
+        c->kernels_per_step = static_cast<int>(c->launches - before);
+        cudaError_t ee = cudaStreamEndCapture(c->stream, &graph);
+        if (ce != cudaSuccess || ee != cudaSuccess) {
+            if (graph) cudaGraphDestroy(graph);
+            cudaGetLastError();
+            return fail(c, BFPN_CUDA_ERROR,
+                        std::string("step capture failed: ") + cudaGetErrorString(ce != cudaSuccess ? ce : ee));
+        }
+        ce = cudaGraphInstantiate(&g, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ce != cudaSuccess) return fail(c, BFPN_CUDA_ERROR, std::string("graph instantiate: ") + cudaGetErrorString(ce));
+    }
+    CUDA_TRY(c, cudaGraphLaunch(g, c->stream));
     return BFPN_OK;
 }
 
@@ -883,11 +1018,15 @@ bfpn_status run_steps(bfpn_ctx* c, int nsteps) {
         }
         return BFPN_OK;
     }
+    const bool ovl = overlap_ok(c);
+    if (ovl && (s = ensure_overlap_objects(c)) != BFPN_OK) return s;
     for (int i = 0; i < nsteps; ++i) {
         const bool first = c->steps_done == 0;
         const bool secondary_stepping =
             !first && !(c->p.flags & (BFPN_FLAG_ENERGY_ONLY | BFPN_FLAG_PRIMARY_ONLY));
-        if (first || !c->use_graphs) {
+        if (ovl && !first) {
+            if ((s = overlap_step(c)) != BFPN_OK) return s;
+        } else if (first || !c->use_graphs) {
             const long long before = c->launches;
             CUDA_TRY(c, enq_step_any(c, first, c->secondary_zero));
             if (!first) c->kernels_per_step = static_cast<int>(c->launches - before);
@@ -919,7 +1058,8 @@ bfpn_status run_steps(bfpn_ctx* c, int nsteps) {
         if (secondary_stepping) c->secondary_zero = false;
         c->steps_done++;
     }
-    return BFPN_OK;
+    // every call leaves whole steps behind it
+    return flush_secondary(c);
 }
 
 template <typename T>
@@ -1194,7 +1334,8 @@ bfpn_status bfpn_create(const bfpn_grid* grid, const bfpn_phys* phys, int precis
     ALLOC(c->tile_hi, static_cast<size_t>(c->Ng) * sizeof(int));
     ALLOC(c->beam_yza, static_cast<size_t>(c->per_e) * sizeof(double));
     ALLOC(c->beam_e, static_cast<size_t>(c->Ng) * sizeof(double));
-    ALLOC(c->partials, 4 * static_cast<size_t>(c->n_part) * sizeof(double));
+    // [primary, even steps | secondary | primary, odd steps] x n_part x 2
+    ALLOC(c->partials, 6 * static_cast<size_t>(c->n_part) * sizeof(double));
     ALLOC(c->hist_idd, static_cast<size_t>(c->hist_cap) * sizeof(double));
     ALLOC(c->hist_proxy, static_cast<size_t>(c->hist_cap) * sizeof(double));
     ALLOC(c->counter, sizeof(int));
@@ -1280,11 +1421,7 @@ bfpn_status bfpn_load_tables(bfpn_ctx* c, const double* mu, int32_t mu_rows, con
     // tables of an earlier load (a context reused for another beam): the step
     // graph captured their addresses, so it goes too
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
-    if (c->graph_exec) {
-        cudaGraphExecDestroy(c->graph_exec);
-        c->graph_exec = nullptr;
-        c->graph_key = -1;
-    }
+    drop_graphs(c);
     dfree(c, c->ablob);
     dfree(c, c->bblob);
     dfree(c, c->eblob);
@@ -1534,6 +1671,9 @@ bfpn_status bfpn_set_option(bfpn_ctx* c, int32_t option, int32_t value) {
         case BFPN_OPT_CUDA_GRAPHS:
             c->use_graphs = value != 0 && !c->profiling;
             break;
+        case BFPN_OPT_STEP_OVERLAP:
+            c->overlap = value != 0;
+            break;
         case BFPN_OPT_PAIRED_ANGLES:
             c->tr_pairs = value != 0;
             break;
@@ -1575,11 +1715,7 @@ bfpn_status bfpn_set_option(bfpn_ctx* c, int32_t option, int32_t value) {
         default:
             return fail(c, BFPN_INVALID_ARG, "unknown option");
     }
-    if (c->graph_exec) {
-        cudaGraphExecDestroy(c->graph_exec);
-        c->graph_exec = nullptr;
-        c->graph_key = -1;
-    }
+    drop_graphs(c);
     return BFPN_OK;
 }
 

@@ -149,14 +149,16 @@ cudaError_t launch_spot_plane(const T* F, const T* f, const T* F1, const T* f1, 
 
 // Tensor-core (tcgen05) angular contraction of the source, float state
 // (kernels_umma.cu): pack the A operand into ablob (umma_pack_bytes), then a
-// bulk-copy-fed GEMM; bblob from build_umma_blob with BK = 16; err receives a
+// bulk-copy-fed GEMM; bblob from launch_build_umma_blob with BK = 16; err receives a
 // non-zero code if a CTA's bounded wait ran out.
 // The epilogue writes A1 / A2 split into bf16 hi / lo into q (umma_q_bytes,
 // the energy stage's operand layout); rows of groups it does not write must
-// be zero.
+// be zero.  packed (may be null) is recorded on s once the pack, the last
+// reader of P1 and P2, has been enqueued.
 cudaError_t launch_source_angular_pipe(const float* P1, const float* P2, uint8_t* ablob, const uint8_t* bblob,
                                        const int* groups, int n_groups, uint8_t* q, int Ng, int* err, int nyz,
-                                       int NA, int NT, int BK, int n_ntiles, cudaStream_t s);
+                                       int NA, int NT, int BK, int n_ntiles, cudaStream_t s,
+                                       cudaEvent_t packed = nullptr);
 size_t umma_pack_bytes(int n_groups, int nyz, int NA, int BK);
 size_t umma_q_bytes(long long per_e, int Ng);
 // Tensor-core energy stage: S[e][l] from q with the coefficient tiles and

@@ -353,8 +353,8 @@ size_t umma_pipe_smem(int NT, int BK) {
 
 cudaError_t launch_source_angular_pipe(const float* P1, const float* P2, uint8_t* ablob, const uint8_t* bblob,
                                        const int* groups, int n_groups, uint8_t* q, int Ng, int* err, int nyz,
-                                       int NA, int NT, int BK, int n_ntiles, cudaStream_t s) {
-    if (n_groups <= 0) return cudaSuccess;
+                                       int NA, int NT, int BK, int n_ntiles, cudaStream_t s, cudaEvent_t packed) {
+    if (n_groups <= 0) return packed ? cudaEventRecord(packed, s) : cudaSuccess;
     if (BK != 16 || NT % 16 != 0 || NT < 16 || NT > 256) return cudaErrorInvalidValue;
     const int n_mt = (nyz + kPos - 1) / kPos, nk = (NA + BK - 1) / BK;
     UmmaPackArgs p{P1, P2, groups, ablob, nyz, NA, nk, n_mt, BK};
@@ -363,6 +363,7 @@ cudaError_t launch_source_angular_pipe(const float* P1, const float* P2, uint8_t
     pack_source_operand_kernel<<<dim3(static_cast<unsigned>((per_group + 255) / 256), n_groups), 256, 0, s>>>(p);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
+    if (packed && (e = cudaEventRecord(packed, s)) != cudaSuccess) return e;
     UmmaPipeArgs a{ablob, bblob, groups, q, err, nyz, NA, NT, nk, n_ntiles, n_mt, 2 * ((Ng + 15) / 16)};
     size_t smem = umma_pipe_smem(NT, BK);
     // at most two CTAs per SM when each holds 256 tensor-memory columns (512 per SM)

@@ -273,7 +273,14 @@ int32_t bfpn_source_groups(bfpn_ctx* ctx);
  * BFPN_OPT_LANE_CHUNK / BFPN_OPT_ENERGY_CHUNK (out-of-core mode only): lanes
  *   per lane chunk (rounded down to whole positions, at least one; default
  *   262,144, the reference's --lane-chunk) and groups per group chunk (default
- *   128, --energy-chunk); the device buffers are sized on the next step. */
+ *   128, --energy-chunk); the device buffers are sized on the next step.
+ * BFPN_OPT_STEP_OVERLAP: 1 (default) lets the secondary half of one depth
+ *   step (source, secondary energy / transport / angular passes, the step's
+ *   IDD) run on a second stream beside the primary half of the next step,
+ *   inside one CUDA graph, when graphs are on and the transport is in place
+ *   (mixed precision on whole-plane or cluster kernels); every bfpn_step /
+ *   bfpn_step_async call still ends on whole steps.  0 runs the halves one
+ *   after the other.  Same kernels on the same inputs: the same values. */
 enum {
     BFPN_OPT_TENSOR_CORES = 0,
     BFPN_OPT_CUDA_GRAPHS = 1,
@@ -281,7 +288,8 @@ enum {
     BFPN_OPT_PAIRED_ANGLES = 3,
     BFPN_OPT_CLUSTER_TRANSPORT = 4,
     BFPN_OPT_LANE_CHUNK = 5,
-    BFPN_OPT_ENERGY_CHUNK = 6
+    BFPN_OPT_ENERGY_CHUNK = 6,
+    BFPN_OPT_STEP_OVERLAP = 7
 };
 bfpn_status bfpn_set_option(bfpn_ctx* ctx, int32_t option, int32_t value);
 

@@ -341,6 +341,34 @@ def test_depth_steps_tiled_transport():
     assert_states(ctx, ora, STEP_TOL)
 
 
+def _stepped(cfg, precision, overlap, calls):
+    ctx, ora = build(cfg, precision=precision)
+    ctx.set_option(capi.OPT_STEP_OVERLAP, overlap)
+    idd = np.concatenate([ctx.step(n)[0] for n in calls])
+    states = [ctx.get_state(sp, cf) for sp in (0, 1) for cf in (0, 1)]
+    return ctx, ora, idd, states
+
+
+@pytest.mark.parametrize("precision", [capi.PREC_MIXED, capi.PREC_FP64])
+def test_overlapped_steps_equal_sequential_steps(precision):
+    """The secondary half of step n on a second stream beside the primary half
+    of step n+1 (square planes: in-place transport) gives the sequential
+    order's IDD history and states bit for bit, over calls of 1, 2, 5 and 3
+    steps (each call ends on whole steps)."""
+    cfg = small_cfg(ny=8, nz=8, nmu=4, nom=4, ng=40, ly=2.0, lz=2.0)
+    calls = [1, 2, 5, 3]
+    _, _, idd_s, st_s = _stepped(cfg, precision, 0, calls)
+    ctx, ora, idd_o, st_o = _stepped(cfg, precision, 1, calls)
+    assert np.abs(idd_s).max() > 0
+    assert np.array_equal(idd_s, idd_o)
+    for a, b in zip(st_s, st_o):
+        assert np.array_equal(a, b)
+    if precision == capi.PREC_FP64:
+        idd_r, _ = ora.step(sum(calls))
+        assert rel_err(idd_o, idd_r) < STEP_TOL
+        assert_states(ctx, ora, STEP_TOL)
+
+
 def test_step_api_pieces_agree():
     """bfpn_step in one call == step by step == async + history download."""
     cfg = small_cfg()
