@@ -182,31 +182,37 @@ void energy_kernels(BeamTables& t) {
 void angular_kernel(BeamTables& t) {
     const int NA = t.NA, Ng = t.Ng;
     const size_t NA2 = static_cast<size_t>(NA) * NA;
-    std::vector<double> theta(NA2);  // [in][out], degrees
-    for (int out = 0; out < NA; ++out) {
-        const double oy = t.omega[2 * out], oz = t.omega[2 * out + 1];
-        const double on = std::sqrt(1.0 + oy * oy + oz * oz);
-        for (int in = 0; in < NA; ++in) {
+    std::vector<double> theta(NA2);  // [in][out], degrees; rows of inputs over the host's threads
+    parallel_ranges(NA, 64, [&](size_t in0, size_t in1) {
+        for (size_t in = in0; in < in1; ++in) {
             const double iy = t.omega[2 * in], iz = t.omega[2 * in + 1];
             const double inn = std::sqrt(1.0 + iy * iy + iz * iz);
-            double c = (1.0 + iy * oy + iz * oz) / std::max(inn * on, kEpsilon);
-            c = std::max(-1.0, std::min(1.0, c));
-            theta[static_cast<size_t>(in) * NA + out] = std::abs(std::acos(c) * 180.0 / kPi);
+            for (int out = 0; out < NA; ++out) {
+                const double oy = t.omega[2 * out], oz = t.omega[2 * out + 1];
+                const double on = std::sqrt(1.0 + oy * oy + oz * oz);
+                double c = (1.0 + iy * oy + iz * oz) / std::max(inn * on, kEpsilon);
+                c = std::max(-1.0, std::min(1.0, c));
+                theta[in * NA + out] = std::abs(std::acos(c) * 180.0 / kPi);
+            }
         }
-    }
+    });
     std::vector<double> jac(NA);
     for (int in = 0; in < NA; ++in) {
         const double iy = t.omega[2 * in], iz = t.omega[2 * in + 1];
         jac[in] = std::pow(1.0 + iy * iy + iz * iz, -1.5);
     }
     // distinct theta values (all finite and >= +0, so == separates bit patterns)
-    std::vector<double> uniq(theta);
-    std::sort(uniq.begin(), uniq.end());
-    uniq.erase(std::unique(uniq.begin(), uniq.end()), uniq.end());
-    const size_t U = uniq.size();
+    // (one sort of (value, position) pairs, then ranks in one pass)
+    std::vector<std::pair<double, uint32_t>> order(NA2);
+    for (size_t i = 0; i < NA2; ++i) order[i] = {theta[i], static_cast<uint32_t>(i)};
+    std::sort(order.begin(), order.end());
+    std::vector<double> uniq;
     std::vector<uint32_t> idx(NA2);
-    for (size_t i = 0; i < NA2; ++i)
-        idx[i] = static_cast<uint32_t>(std::lower_bound(uniq.begin(), uniq.end(), theta[i]) - uniq.begin());
+    for (size_t i = 0; i < NA2; ++i) {
+        if (uniq.empty() || order[i].first != uniq.back()) uniq.push_back(order[i].first);
+        idx[order[i].second] = static_cast<uint32_t>(uniq.size() - 1);
+    }
+    const size_t U = uniq.size();
     t.ker_v.resize(static_cast<size_t>(Ng) * NA2);  // uninitialised: every group's block is written below
     auto group = [&](int ek, std::vector<double>& f, std::vector<double>& col) {
         double* K = t.ker_v.data() + static_cast<size_t>(ek) * NA2;
