@@ -1390,7 +1390,10 @@ bfpn_status bfpn_load_tables(bfpn_ctx* c, const double* mu, int32_t mu_rows, con
     if (s != BFPN_OK) return s;
     std::string err;
     BeamTables t;
-    if (!build_tables(c->g, c->p, mu, mu_rows, sigma_c, sigma_rows, t, err)) return fail(c, BFPN_INVALID_ARG, err);
+    // a float-state context keeps only the float angular kernel on the host
+    const bool f32_kernel = c->prec == BFPN_PREC_MIXED;
+    if (!build_tables(c->g, c->p, mu, mu_rows, sigma_c, sigma_rows, t, err, f32_kernel))
+        return fail(c, BFPN_INVALID_ARG, err);
     c->tables = std::move(t);
     c->raw_sigma.assign(sigma_c, sigma_c + std::min<int>(sigma_rows, c->Ng));
     BeamTables& T = c->tables;
@@ -1405,7 +1408,15 @@ bfpn_status bfpn_load_tables(bfpn_ctx* c, const double* mu, int32_t mu_rows, con
     if ((s = upload_state_table(c, c->fac_step, angle_factor(T, c->p, c->d.dt))) != BFPN_OK) return s;
     if ((s = upload_state_table(c, c->sine_u, T.sine_u)) != BFPN_OK) return s;
     if ((s = upload_state_table(c, c->sine_v, T.sine_v)) != BFPN_OK) return s;
-    if (c->ker_v && (s = upload_state_table(c, c->ker_v, T.ker_v)) != BFPN_OK) return s;
+    if (c->ker_v) {
+        if (f32_kernel) {
+            CUDA_TRY(c, cudaMemcpyAsync(c->ker_v, T.ker_v_f.data(), T.ker_v_f.size() * sizeof(float),
+                                        cudaMemcpyHostToDevice, c->stream));
+            CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+        } else if ((s = upload_state_table(c, c->ker_v, T.ker_v)) != BFPN_OK) {
+            return s;
+        }
+    }
     if ((s = upload_f64(c, c->e1, T.ker_e1.data(), T.ker_e1.size() * sizeof(double))) != BFPN_OK) return s;
     if ((s = upload_f64(c, c->e2, T.ker_e2.data(), T.ker_e2.size() * sizeof(double))) != BFPN_OK) return s;
     // source groups that some output band uses and that carry a kernel
@@ -1828,6 +1839,7 @@ bfpn_status bfpn_table_download(bfpn_ctx* c, int32_t which, double* host, uint64
     if (!c || !host) return BFPN_INVALID_ARG;
     if (!c->tables_loaded) return fail(c, BFPN_NOT_READY, "tables not loaded");
     std::vector<double> tmp;
+    if (which == BFPN_TABLE_KER_V) angular_kernel_f64(c->tables);
     const TableView src = table_of(c->tables, which, tmp);
     if (!src.known) return fail(c, BFPN_INVALID_ARG, "unknown table id");
     if (src.size > n) return fail(c, BFPN_INVALID_ARG, "host buffer too small for the table");

@@ -179,7 +179,7 @@ void energy_kernels(BeamTables& t) {
 // each column sum still adding its inputs in increasing order.  Groups are
 // spread over the host's threads, and each thread is the first to touch the
 // table pages it fills.
-void angular_kernel(BeamTables& t) {
+void angular_kernel(BeamTables& t, bool as_float) {
     const int NA = t.NA, Ng = t.Ng;
     const size_t NA2 = static_cast<size_t>(NA) * NA;
     std::vector<double> theta(NA2);  // [in][out], degrees; rows of inputs over the host's threads
@@ -213,12 +213,17 @@ void angular_kernel(BeamTables& t) {
         idx[order[i].second] = static_cast<uint32_t>(uniq.size() - 1);
     }
     const size_t U = uniq.size();
-    t.ker_v.resize(static_cast<size_t>(Ng) * NA2);  // uninitialised: every group's block is written below
+    // uninitialised: every group's block is written below, in double or, for
+    // a float-state context, as the float rounding of the same double values
+    if (as_float) t.ker_v_f.resize(static_cast<size_t>(Ng) * NA2);
+    else t.ker_v.resize(static_cast<size_t>(Ng) * NA2);
     auto group = [&](int ek, std::vector<double>& f, std::vector<double>& col) {
-        double* K = t.ker_v.data() + static_cast<size_t>(ek) * NA2;
+        double* K = as_float ? nullptr : t.ker_v.data() + static_cast<size_t>(ek) * NA2;
+        float* Kf = as_float ? t.ker_v_f.data() + static_cast<size_t>(ek) * NA2 : nullptr;
         const double m1 = t.mu[ek * 3], m2 = t.mu[ek * 3 + 1];
         if (ek == Ng - 1 || m1 == 0.0 || m2 == 0.0) {
-            std::fill(K, K + NA2, 0.0);
+            if (as_float) std::fill(Kf, Kf + NA2, 0.0f);
+            else std::fill(K, K + NA2, 0.0);
             return;
         }
         for (size_t u = 0; u < U; ++u) f[u] = std::pow(uniq[u], m1 - 1.0) * std::exp(-uniq[u] / m2);
@@ -235,7 +240,7 @@ void angular_kernel(BeamTables& t) {
         for (int in = 0; in < NA; ++in) {
             const double j = jac[in];
             const uint32_t* ir = idx.data() + static_cast<size_t>(in) * NA;
-            double* Kr = K + static_cast<size_t>(in) * NA;
+            const size_t row = static_cast<size_t>(in) * NA;
             for (int out = 0; out < NA; ++out) {
                 double v = f[ir[out]] * j;
                 if (!std::isfinite(v)) v = 0.0;
@@ -243,7 +248,8 @@ void angular_kernel(BeamTables& t) {
                     v /= col[out];
                     if (v < kKernelThreshold) v = 0.0;
                 }
-                Kr[out] = v;
+                if (as_float) Kf[row + out] = static_cast<float>(v);
+                else K[row + out] = v;
             }
         }
     };
@@ -353,6 +359,11 @@ void parallel_ranges(size_t n, size_t min_per_thread, const std::function<void(s
     for (auto& th : pool) th.join();
 }
 
+const HostTable& angular_kernel_f64(BeamTables& t) {
+    if (t.ker_v.empty() && t.Ng > 0 && t.NA > 0) angular_kernel(t, false);
+    return t.ker_v;
+}
+
 Deltas compute_deltas(const bfpn_grid& g) {
     Deltas d;
     d.dt = g.Lx / g.Nx;
@@ -365,7 +376,7 @@ Deltas compute_deltas(const bfpn_grid& g) {
 }
 
 bool build_tables(const bfpn_grid& g, const bfpn_phys& p, const double* mu, int mu_rows, const double* sigma,
-                  int sigma_rows, BeamTables& t, std::string& err) {
+                  int sigma_rows, BeamTables& t, std::string& err, bool float_kernel) {
     t.Ng = g.Ng;
     t.Ny = g.Ny;
     t.Nz = g.Nz;
@@ -406,7 +417,7 @@ bool build_tables(const bfpn_grid& g, const bfpn_phys& p, const double* mu, int 
     straggling(Ng, t.T_c);
     transport_cross_section(Ng, t.d.dg, t.sig_trg);
     energy_kernels(t);
-    angular_kernel(t);
+    angular_kernel(t, float_kernel);
     t.sine_u.resize(static_cast<size_t>(t.Nom) * t.Nom);
     t.sine_v.resize(static_cast<size_t>(t.Nmu) * t.Nmu);
     for (int m = 0; m < t.Nom; ++m)

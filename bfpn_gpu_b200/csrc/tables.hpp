@@ -60,7 +60,8 @@ struct BeamTables {
     std::vector<double> omega;     // NA x 2 (omega_y, omega_z)
     std::vector<double> ker_e1, ker_e2;  // Ng x Ng, row = output group, column = source group
     std::vector<int> band_begin, band_end;  // per output group
-    HostTable ker_v;               // Ng x NA x NA, [src][in][out]
+    HostTable ker_v;               // Ng x NA x NA, [src][in][out]; empty when built as float only
+    std::vector<float, UninitAlloc<float>> ker_v_f;  // the same table rounded to float (float-state contexts)
     std::vector<double> sine_u, sine_v;     // Nom x Nom, Nmu x Nmu
     std::vector<double> beam_yza;  // nyz x NA  (initial-beam transverse/angular factor)
     std::vector<double> beam_e;    // Ng        (initial-beam energy factor)
@@ -71,8 +72,13 @@ struct BeamTables {
 
 // Builds every table; returns false with a message on invalid input
 // (mirrors the reference's runtime_error cases).
+// float_kernel: the angular kernel is built as ker_v_f (the float rounding of
+// each double entry) instead of ker_v.
 bool build_tables(const bfpn_grid& g, const bfpn_phys& p, const double* mu, int mu_rows, const double* sigma,
-                  int sigma_rows, BeamTables& t, std::string& err);
+                  int sigma_rows, BeamTables& t, std::string& err, bool float_kernel = false);
+
+// ker_v in double, built on first use when the tables were built float only.
+const HostTable& angular_kernel_f64(BeamTables& t);
 
 // Energy-sweep constants [Ng][kEnergyCoef] for half-step dt (see common.cuh).
 std::vector<double> energy_coefficients(const BeamTables& t, const bfpn_phys& p, double dt);

@@ -341,6 +341,18 @@ def test_depth_steps_tiled_transport():
     assert_states(ctx, ora, STEP_TOL)
 
 
+def test_mixed_context_tables_equal_host_tables():
+    """A float-state context keeps only the float angular kernel on the host;
+    its table download still returns the double table, equal to the
+    context-free builder's (and so to the oracle's)."""
+    cfg = small_cfg(ny=8, nz=8, nmu=4, nom=4, ng=40, ly=2.0, lz=2.0)
+    mu, sig = read_tables(table_dir("synthetic500"), cfg.ng)
+    ctx, _ = build(cfg, precision=capi.PREC_MIXED)
+    NA = cfg.nmu * cfg.nom
+    for which, n in ((capi.TABLE_KER_V, cfg.ng * NA * NA), (capi.TABLE_KER_E1, cfg.ng ** 2)):
+        assert np.array_equal(ctx.table(which, n), capi.host_table(cfg.grid(), cfg.phys(), mu, sig, which))
+
+
 def _stepped(cfg, precision, overlap, calls):
     ctx, ora = build(cfg, precision=precision)
     ctx.set_option(capi.OPT_STEP_OVERLAP, overlap)
