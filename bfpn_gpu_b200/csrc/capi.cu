@@ -138,6 +138,12 @@ struct bfpn_ctx {
     bool pending_sec = false;  // the secondary half of step steps_done-1 is still owed
     cudaStream_t s_sec = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_pread = nullptr, ev_join = nullptr;
+    // inside an overlapped body the T-A-T chains of psi^2 also get their own
+    // streams (one per species): s_f[k], forked / joined by ev_ff[k] / ev_fj[k]
+    bool split_tat = false;
+    bool split_chains = true;  // option: split the chains in overlapped bodies
+    cudaStream_t s_f[2] = {nullptr, nullptr};
+    cudaEvent_t ev_ff[2] = {nullptr, nullptr}, ev_fj[2] = {nullptr, nullptr};
     cudaGraphExec_t ovl_exec[2] = {nullptr, nullptr};
     bool profiling = false;
     struct Pending {
@@ -336,13 +342,16 @@ void free_all(bfpn_ctx* c) {
     for (auto e : c->ev_pool) cudaEventDestroy(e);
     c->ev_pool.clear();
     drop_graphs(c);
-    for (cudaEvent_t* e : {&c->ev_fork, &c->ev_pread, &c->ev_join})
+    for (cudaEvent_t* e : {&c->ev_fork, &c->ev_pread, &c->ev_join, &c->ev_ff[0], &c->ev_ff[1], &c->ev_fj[0], &c->ev_fj[1]})
         if (*e) {
             cudaEventDestroy(*e);
             *e = nullptr;
         }
-    if (c->s_sec) cudaStreamDestroy(c->s_sec);
-    c->s_sec = nullptr;
+    for (cudaStream_t* st : {&c->s_sec, &c->s_f[0], &c->s_f[1]})
+        if (*st) {
+            cudaStreamDestroy(*st);
+            *st = nullptr;
+        }
     for (auto& b : c->allocs) cudaFree(b.p);
     c->allocs.clear();
     for (void* p : c->host_allocs) cudaFreeHost(p);
@@ -601,6 +610,28 @@ cudaError_t enq_lite_step(bfpn_ctx* c) {
     });
 }
 
+// T-A-T of both arrays of a species: psi^1 on the context stream and, inside
+// an overlapped body, psi^2 beside it on s_f[species] (the two chains share
+// no array: the transport is in place there); one after the other elsewhere.
+template <typename T>
+cudaError_t enq_tat_pair(bfpn_ctx* c, int species, bool do_tr, bool do_an, bool preserve_F, bool preserve_f) {
+    cudaError_t e;
+    if (!c->split_tat) {
+        if ((e = enq_tat<T>(c, species, 0, do_tr, do_an, preserve_F)) != cudaSuccess) return e;
+        return enq_tat<T>(c, species, 1, do_tr, do_an, preserve_f);
+    }
+    cudaStream_t own = c->stream, side = c->s_f[species];
+    if ((e = cudaEventRecord(c->ev_ff[species], own)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(side, c->ev_ff[species], 0)) != cudaSuccess) return e;
+    c->stream = side;
+    e = enq_tat<T>(c, species, 1, do_tr, do_an, preserve_f);
+    c->stream = own;
+    if (e != cudaSuccess) return e;
+    if ((e = enq_tat<T>(c, species, 0, do_tr, do_an, preserve_F)) != cudaSuccess) return e;
+    if ((e = cudaEventRecord(c->ev_fj[species], side)) != cudaSuccess) return e;
+    return cudaStreamWaitEvent(own, c->ev_fj[species], 0);
+}
+
 // IDD partial sums of the primary's last energy pass, by step parity (the
 // secondary half of one step and the primary half of the next can be in
 // flight together).
@@ -618,8 +649,7 @@ cudaError_t enq_primary_half(bfpn_ctx* c, double* partP) {
     if (!(fl & BFPN_FLAG_ENERGY_ONLY)) {
         const bool do_tr = !(fl & BFPN_FLAG_NO_TRANSPORT), do_an = !(fl & BFPN_FLAG_NO_ANGLE);
         const bool clip_F = !(fl & BFPN_FLAG_NO_SPATIAL_CLIPPING);
-        if ((e = enq_tat<T>(c, 0, 0, do_tr, do_an, !clip_F)) != cudaSuccess) return e;
-        if ((e = enq_tat<T>(c, 0, 1, do_tr, do_an, true)) != cudaSuccess) return e;
+        if ((e = enq_tat_pair<T>(c, 0, do_tr, do_an, !clip_F, true)) != cudaSuccess) return e;
     }
     return enq_energy<T>(c, 0, c->ecoef_half, false, partP);
 }
@@ -645,8 +675,7 @@ cudaError_t enq_secondary_half(bfpn_ctx* c, const double* partP, cudaEvent_t pre
     cudaError_t e;
     if ((e = enq_source<T>(c, pread)) != cudaSuccess) return e;
     if ((e = enq_energy<T>(c, 1, c->ecoef_half, true, nullptr)) != cudaSuccess) return e;
-    if ((e = enq_tat<T>(c, 1, 0, true, true, false)) != cudaSuccess) return e;
-    if ((e = enq_tat<T>(c, 1, 1, true, true, true)) != cudaSuccess) return e;
+    if ((e = enq_tat_pair<T>(c, 1, true, true, false, true)) != cudaSuccess) return e;
     if ((e = enq_energy<T>(c, 1, c->ecoef_half, true, partS)) != cudaSuccess) return e;
     return enq_finalize<T>(c, partP, partS, energy_grid(c->per_e, c->energy_block));
 }
@@ -690,11 +719,13 @@ cudaError_t enq_overlap_body(bfpn_ctx* c, int step) {
     if ((e = cudaStreamWaitEvent(c->s_sec, c->ev_fork, 0)) != cudaSuccess) return e;
     cudaStream_t main = c->stream;
     c->stream = c->s_sec;
+    c->split_tat = c->split_chains;
     e = enq_secondary_half<T>(c, primary_partials(c, step - 1), c->ev_pread);
     c->stream = main;
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(c->stream, c->ev_pread, 0);
+    if (e == cudaSuccess) e = enq_primary_half<T>(c, primary_partials(c, step));
+    c->split_tat = false;
     if (e != cudaSuccess) return e;
-    if ((e = cudaStreamWaitEvent(c->stream, c->ev_pread, 0)) != cudaSuccess) return e;
-    if ((e = enq_primary_half<T>(c, primary_partials(c, step))) != cudaSuccess) return e;
     if ((e = cudaEventRecord(c->ev_join, c->s_sec)) != cudaSuccess) return e;
     return cudaStreamWaitEvent(c->stream, c->ev_join, 0);
 }
@@ -947,7 +978,8 @@ bool overlap_ok(const bfpn_ctx* c) {
 bfpn_status ensure_overlap_objects(bfpn_ctx* c) {
     if (c->s_sec) return BFPN_OK;
     CUDA_TRY(c, cudaStreamCreateWithFlags(&c->s_sec, cudaStreamNonBlocking));
-    for (cudaEvent_t* e : {&c->ev_fork, &c->ev_pread, &c->ev_join})
+    for (cudaStream_t* st : {&c->s_f[0], &c->s_f[1]}) CUDA_TRY(c, cudaStreamCreateWithFlags(st, cudaStreamNonBlocking));
+    for (cudaEvent_t* e : {&c->ev_fork, &c->ev_pread, &c->ev_join, &c->ev_ff[0], &c->ev_ff[1], &c->ev_fj[0], &c->ev_fj[1]})
         CUDA_TRY(c, cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     return BFPN_OK;
 }
@@ -1683,7 +1715,9 @@ bfpn_status bfpn_set_option(bfpn_ctx* c, int32_t option, int32_t value) {
             c->use_graphs = value != 0 && !c->profiling;
             break;
         case BFPN_OPT_STEP_OVERLAP:
+            if (value < 0 || value > 2) return fail(c, BFPN_INVALID_ARG, "step overlap: 0, 1 or 2");
             c->overlap = value != 0;
+            c->split_chains = value == 2;
             break;
         case BFPN_OPT_PAIRED_ANGLES:
             c->tr_pairs = value != 0;

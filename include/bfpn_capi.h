@@ -274,13 +274,15 @@ int32_t bfpn_source_groups(bfpn_ctx* ctx);
  *   per lane chunk (rounded down to whole positions, at least one; default
  *   262,144, the reference's --lane-chunk) and groups per group chunk (default
  *   128, --energy-chunk); the device buffers are sized on the next step.
- * BFPN_OPT_STEP_OVERLAP: 1 (default) lets the secondary half of one depth
+ * BFPN_OPT_STEP_OVERLAP: 2 (default) lets the secondary half of one depth
  *   step (source, secondary energy / transport / angular passes, the step's
  *   IDD) run on a second stream beside the primary half of the next step,
- *   inside one CUDA graph, when graphs are on and the transport is in place
- *   (mixed precision on whole-plane or cluster kernels); every bfpn_step /
- *   bfpn_step_async call still ends on whole steps.  0 runs the halves one
- *   after the other.  Same kernels on the same inputs: the same values. */
+ *   inside one CUDA graph, and within each half runs the transport-angle-
+ *   transport chain of psi^2 beside that of psi^1; 1 overlaps the halves
+ *   only; 0 runs everything one kernel after the other.  Applies when graphs
+ *   are on and the transport is in place (whole-plane or cluster kernels);
+ *   every bfpn_step / bfpn_step_async call still ends on whole steps.  Same
+ *   kernels on the same inputs: the same values. */
 enum {
     BFPN_OPT_TENSOR_CORES = 0,
     BFPN_OPT_CUDA_GRAPHS = 1,

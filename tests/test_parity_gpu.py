@@ -361,16 +361,17 @@ def _stepped(cfg, precision, overlap, calls):
     return ctx, ora, idd, states
 
 
-@pytest.mark.parametrize("precision", [capi.PREC_MIXED, capi.PREC_FP64])
-def test_overlapped_steps_equal_sequential_steps(precision):
+@pytest.mark.parametrize("precision,overlap", [(capi.PREC_MIXED, 1), (capi.PREC_MIXED, 2), (capi.PREC_FP64, 2)])
+def test_overlapped_steps_equal_sequential_steps(precision, overlap):
     """The secondary half of step n on a second stream beside the primary half
-    of step n+1 (square planes: in-place transport) gives the sequential
+    of step n+1 (square planes: in-place transport), with (2) or without (1)
+    the psi^2 T-A-T chains on streams of their own, gives the sequential
     order's IDD history and states bit for bit, over calls of 1, 2, 5 and 3
     steps (each call ends on whole steps)."""
     cfg = small_cfg(ny=8, nz=8, nmu=4, nom=4, ng=40, ly=2.0, lz=2.0)
     calls = [1, 2, 5, 3]
     _, _, idd_s, st_s = _stepped(cfg, precision, 0, calls)
-    ctx, ora, idd_o, st_o = _stepped(cfg, precision, 1, calls)
+    ctx, ora, idd_o, st_o = _stepped(cfg, precision, overlap, calls)
     assert np.abs(idd_s).max() > 0
     assert np.array_equal(idd_s, idd_o)
     for a, b in zip(st_s, st_o):
