@@ -2,24 +2,27 @@
 """Depth-step throughput of the BFPn pencil-beam solver on B200.
 
 Metric: phase-space updates/s -- cells of both species advanced one full
-Strang depth step per second.  Workload (the single-beam configuration of the
-benchmark plan): water, 230 MeV beam, sigma_E 2.3 MeV (1 %), sigma_yz 0.5 cm,
-8 x 8 cm lateral domain, Ny = Nz = 20, Nmu = Nom = 20, Ng = 500, 40 cm depth
-(Nx = 1000, 1000 steps); 88.2 M cells per array, both species.  Inputs are the
-reference's water tables (tests/golden/tables/water).  Mixed precision by
-default (float state; double energy recursion and IDD), --precision fp64 for
-the parity mode.
+Strang depth step per second.  Default workload: the full paper-scale grid,
+the largest single-GPU configuration -- water, 230 MeV beam, sigma_E 2.3 MeV
+(1 %), sigma_yz 0.5 cm, 16 x 16 cm lateral domain, Ny = Nz = 80,
+Nmu = Nom = 20, Ng = 500, 40 cm depth (Nx = 1000, 1000 steps); 1.31 G cells
+per array, both species, about 21 GB of float state resident in HBM.  Inputs
+are the reference's water tables (tests/golden/tables/water).  Mixed
+precision by default (float state; double energy recursion and IDD),
+--precision fp64 for the parity mode.  --workload water230_20 runs the
+20 x 20 single-beam configuration, bone230_80 the bone (1.85 g/cm3) grid.
 
 One "step" = one depth step of the whole beam (both species) with the state
-resident in HBM.  The four state arrays (1.4 GB in mixed precision) exceed the
-126 MB L2, so no flush is needed between timed steps.
+resident in HBM.  The four state arrays exceed the 126 MB L2 many times
+over, so no flush is needed between timed steps.
 
 Multi-GPU: independent replicas (one beam per GPU, no collective on the data
 path); the timed region is bracketed by barriers and the time is the max over
 ranks.
 
 --impl reference times the CPU oracle (FP64 restatement of the reference's
-eq15 path, all host threads) on the same workload, one depth step per step.
+eq15 path, all host threads) on a bounded sample of the same workload; that
+arm loads only the oracle's library.
 """
 import argparse
 import json
@@ -36,8 +39,8 @@ sys.path.insert(0, ROOT)
 
 import numpy as np  # noqa: E402
 
-# Single-beam workloads: the default is the one the metric is quoted on; the 80x80 grids
-# are the full paper-scale state (about 42 GB of device memory in mixed precision).
+# Single-beam workloads.  The default is the largest single-GPU configuration
+# (80 x 80 lateral grid, about 48 GB of device memory in mixed precision).
 WORKLOADS = {
     "water230_20": (dict(nx=1000, t_final=40.0, ny=20, nz=20, nmu=20, nom=20, ng=500, ly=8.0, lz=8.0,
                          beam_energy=230.0, sigma_e=2.3, sigma_yz=0.5, material_name="water"),
@@ -51,9 +54,59 @@ WORKLOADS = {
                    "bone (1.85 g/cm3) 230 MeV pencil beam, 80x80 yz / 20x20 angles / 500 groups, 40 cm "
                    "(1000 depth steps)"),
 }
-WORKLOAD, WORKLOAD_NAME = WORKLOADS["water230_20"]
+DEFAULT_WORKLOAD = "water230_80"
+WORKLOAD_KEY = DEFAULT_WORKLOAD
+WORKLOAD, WORKLOAD_NAME = WORKLOADS[DEFAULT_WORKLOAD]
 TABLES = os.path.join(ROOT, "tests", "golden", "tables", "water")
 METRIC = "phase-space updates/s"
+# Lateral positions per side of the CPU sample (see cpu_sample).
+CPU_SAMPLE_NY = 20
+
+
+def host_cpu():
+    """Model name of the host CPU and the cores this process may run on."""
+    name = "unknown"
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    name = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    try:
+        cores = len(os.sched_getaffinity(0))
+    except AttributeError:
+        cores = os.cpu_count()
+    return name, cores
+
+
+def cpu_sample(workload):
+    """The bounded CPU sample of a workload: its central CPU_SAMPLE_NY x
+    CPU_SAMPLE_NY lateral positions at the same spacing (dy, dz unchanged),
+    with the full angular and energy grids, tables, beam and depth step.
+    Every operator's work is per cell (the energy sweep, the source and the
+    DST per lane; transport per plane cell), so updates/s carries over to the
+    full grid.  Returns (workload dict, description)."""
+    w = dict(workload)
+    if w["ny"] <= CPU_SAMPLE_NY:
+        return w, "the whole grid"
+    w["ly"] = w["ly"] * CPU_SAMPLE_NY / w["ny"]
+    w["lz"] = w["lz"] * CPU_SAMPLE_NY / w["nz"]
+    w["ny"] = w["nz"] = CPU_SAMPLE_NY
+    return w, ("the central %dx%d lateral positions (%.1f x %.1f cm at the workload's %.2f cm spacing) with "
+               "the full %dx%d angles x %d groups" % (CPU_SAMPLE_NY, CPU_SAMPLE_NY, w["ly"], w["lz"],
+                                                      w["ly"] / CPU_SAMPLE_NY, w["nmu"], w["nom"], w["ng"]))
+
+
+def product_library_loaded():
+    """True when this process has mapped the solver library (the reference
+    arm must not)."""
+    try:
+        with open("/proc/self/maps") as f:
+            return any("libbfpn_b200" in line for line in f)
+    except OSError:
+        return False
 
 
 def peaks():
@@ -172,16 +225,24 @@ def kernel_bytes(cls, cells, elem, n_groups, nyz, NA):
     return "hbm", 0.0
 
 
-# DRAM bytes (read + write) per cell of one launch of each kernel class, from ncu captures of
-# the same kernels on this workload with 250 groups (profiles/*_water230_ng250.txt), mixed
-# precision; traffic grows in proportion to the cells, so a full launch is this times cells.
+# DRAM bytes (read + write) per cell of one launch of each kernel class, from ncu
+# captures of the same kernels on a smaller state of the same lateral and
+# angular grid (profiles/*.txt: the 20x20 kernels at 250 groups, the 80x80
+# kernels at 40 groups), mixed precision; traffic grows in proportion to the
+# cells, so a full launch is this times its cells.
 NCU_DRAM_BYTES_PER_CELL = {
-    "transport": (176.52e6 + 122.73e6) / 44.1e6,
-    "angle": (176.85e6 + 119.49e6) / 44.1e6,
-    "energy": (352.90e6 + 295.12e6) / 44.1e6,
-    "source_angular": (190.52e6 + 153.69e6 + 284.85e6 + 154.88e6) / 44.1e6,  # pack + GEMM
-    "source_energy": (249.24e6 + 132.63e6) / 44.1e6,
+    "water230_20": {
+        "transport": (176.52e6 + 122.73e6) / 44.1e6,
+        "angle": (176.85e6 + 119.49e6) / 44.1e6,
+        "energy": (352.90e6 + 295.12e6) / 44.1e6,
+        "source_angular": (190.52e6 + 153.69e6 + 284.85e6 + 154.88e6) / 44.1e6,  # pack + GEMM
+        "source_energy": (249.24e6 + 132.63e6) / 44.1e6,
+    },
+    "water230_80": {
+        "transport": (420.1e6 + 366.1e6) / 104.976e6,  # transport_cluster_kernel, 81x81x400x40
+    },
 }
+NCU_DRAM_BYTES_PER_CELL["bone230_80"] = NCU_DRAM_BYTES_PER_CELL["water230_80"]
 
 
 def run_ours(args):
@@ -240,8 +301,8 @@ def run_ours(args):
     dom = max(prof.items(), key=lambda kv: kv[1][0])[0]
     bound, work = kernel_bytes(dom, cells, elem, n_groups, nyz, NA)
     avg_s = prof[dom][0] / prof[dom][1] / 1e3
-    per_cell = NCU_DRAM_BYTES_PER_CELL.get(dom) if prec == capi.PREC_MIXED else None
-    traffic = per_cell * cells if per_cell else None  # bytes per launch
+    per_cell = NCU_DRAM_BYTES_PER_CELL.get(WORKLOAD_KEY, {}).get(dom) if prec == capi.PREC_MIXED else None
+    traffic = per_cell * cells if per_cell and args.ng is None else None  # bytes per launch
     if bound == "hbm":
         achieved = work / avg_s / 1e9
         peak = pk["hbm_gbs"]
@@ -265,12 +326,13 @@ def run_ours(args):
     if clocks:
         out["clocks"] = clocks
 
+    idd_e2e = None
     if rank == 0 and not args.no_e2e:
-        out["e2e"] = e2e_job(cfg, prec, local, mu, sig)
+        out["e2e"], idd_e2e = e2e_job(cfg, prec, local)
     if rank == 0 and world == 1 and not args.no_accuracy and prec == capi.PREC_MIXED:
-        out["accuracy"] = accuracy(cfg, local, mu, sig, args.accuracy_steps)
+        out["accuracy"] = accuracy(cfg, local, mu, sig, args.accuracy_steps, idd_e2e)
     if rank == 0 and world == 1 and not args.no_cpu:
-        out["cpu_baseline"] = cpu_baseline(cfg, mu, sig, args.cpu_steps)
+        out["cpu_baseline"] = cpu_baseline(args.cpu_steps)
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
@@ -279,8 +341,9 @@ def run_ours(args):
         print(json.dumps(out), flush=True)
 
 
-def e2e_job(cfg, prec, device, mu_host, sig_host):
-    """The whole beam solve through the public C ABI: host tables in, IDD out."""
+def e2e_job(cfg, prec, device):
+    """The whole beam solve through the public C ABI: host tables in, IDD
+    history out.  Returns the e2e record and the IDD curve."""
     from bfpn_gpu_b200 import Context, capi, read_tables
 
     steps = cfg.max_steps()
@@ -299,99 +362,98 @@ def e2e_job(cfg, prec, device, mu_host, sig_host):
            + cfg.ng * 40 * 8)
     ctx.close()
     updates = cells * (2 * steps - 1)  # the first step advances the primary only
-    return {"value": updates / (t1 - t0), "unit": "updates/s", "h2d_bytes_per_step": h2d / steps,
-            "d2h_bytes_per_step": 16, "steps": steps, "seconds": t1 - t0,
-            "what": "create + load tables + initial beam + %d depth steps + IDD/proxy history to host" % steps}
+    rec = {"value": updates / (t1 - t0), "unit": "updates/s", "h2d_bytes_per_step": h2d / steps,
+           "d2h_bytes_per_step": 16, "steps": steps, "seconds": t1 - t0,
+           "what": "create + load tables + initial beam + %d depth steps + IDD/proxy history to host" % steps}
+    return rec, idd
 
 
-def accuracy(cfg, device, mu, sig, nsteps):
-    """IDD of the mixed-precision run against the FP64 run, same inputs."""
+def accuracy(cfg, device, mu, sig, nsteps, idd_mixed=None):
+    """IDD of the mixed-precision run against the FP64 run of the same beam
+    (the FP64 path is pinned to the oracle at 1e-10 by the parity tests; the
+    oracle itself needs days for this grid).  idd_mixed: the mixed curve of
+    the e2e job, when it ran over the same steps."""
     from bfpn_gpu_b200 import Context, capi
+    from bfpn_gpu_b200.validation import idd_accuracy
 
-    res = {}
     idds = {}
+    if idd_mixed is not None and len(idd_mixed) == nsteps:
+        idds[capi.PREC_MIXED] = idd_mixed
+    t0 = time.perf_counter()
     for prec in (capi.PREC_FP64, capi.PREC_MIXED):
+        if prec in idds:
+            continue
         ctx = Context(cfg.grid(), cfg.phys(), prec, device=device)
         ctx.load_tables(mu, sig)
         ctx.init_beam()
         idds[prec], _ = ctx.step(nsteps)
         ctx.close()
-    a, b = idds[capi.PREC_MIXED], idds[capi.PREC_FP64]
-    peak = np.abs(b).max()
-    big = b > 0.01 * peak
-    res["steps"] = nsteps
-    res["idd_max_rel_err_above_1pct_peak"] = float((np.abs(a - b)[big] / b[big]).max())
-    res["idd_max_err_rel_to_peak"] = float(np.abs(a - b).max() / peak)
-    dx = cfg.dt()
-    res["bragg_peak_cm_fp64"] = float((np.argmax(b) + 1) * dx)
-    res["bragg_peak_shift_mm"] = float(abs(peak_depth(a, dx) - peak_depth(b, dx)) * 10)
+    res = idd_accuracy(idds[capi.PREC_MIXED], idds[capi.PREC_FP64], cfg.dt())
+    res["against"] = "the FP64 GPU path over the same depth steps"
+    res["seconds"] = time.perf_counter() - t0
     return res
 
 
-def peak_depth(idd, dx):
-    """Depth of the IDD maximum, refined by the parabola through the maximum
-    sample and its two neighbours (sub-step resolution)."""
-    i = int(np.argmax(idd))
-    x = (i + 1) * dx
-    if 0 < i < len(idd) - 1:
-        y0, y1, y2 = idd[i - 1], idd[i], idd[i + 1]
-        den = y0 - 2 * y1 + y2
-        if den != 0:
-            x += 0.5 * dx * (y0 - y2) / den
-    return x
-
-
-def cpu_baseline(cfg, mu, sig, nsteps):
-    """The oracle (FP64 restatement of the reference's path) on the host cores:
-    a bounded sample of the same workload -- depth steps after the first."""
+def oracle_sample(steps, budget_s=None, warmup=0):
+    """The oracle (FP64 restatement of the reference's path) on the host
+    cores, on the bounded CPU sample of the workload (cpu_sample): regular
+    depth steps (both species) from the initial beam, the first step's
+    primary-only half skipped.  Loads only the oracle's library: the tables
+    come through the oracle's own loader."""
+    from bfpn_gpu_b200.config import make_config
     from oracle import oracle as O
 
+    w, what = cpu_sample(WORKLOAD)
+    cfg = make_config(**w)
+    mu, sig = O.read_tables(TABLES, cfg.ng)
     threads = O.max_threads()
     o = O.Oracle(cfg.grid(), cfg.phys(), mu, sig)
-    o.step(1)  # first step: primary only
+    o.set_steps_done(1)  # regular steps: the secondary is advanced from the first one
+    if warmup:
+        o.step(warmup)
+    done = 0
     t0 = time.perf_counter()
-    o.step(nsteps)
+    while done < steps:
+        o.step(1)
+        done += 1
+        if budget_s is not None and time.perf_counter() - t0 > budget_s:
+            break
     sec = time.perf_counter() - t0
+    cells = o.cells
     o.close()
-    return {"value": 2 * o.cells * nsteps / sec, "unit": "updates/s", "cores": threads, "kind": "port",
-            "sample": "%d depth step(s) (both species, FP64) of the same workload after the first" % nsteps,
-            "seconds": sec}
+    model, _ = host_cpu()
+    return {"value": 2 * cells * done / sec, "unit": "updates/s", "cores": threads, "kind": "port",
+            "sample": "%d regular depth step(s) (both species, FP64) of %s: %d cells per array; updates/s per "
+                      "cell carries to the full workload" % (done, what, cells),
+            "cpu": model, "seconds": sec, "steps": done}
+
+
+def cpu_baseline(nsteps):
+    """The oracle on the host cores, a bounded sample of the same workload."""
+    return oracle_sample(nsteps)
 
 
 def run_reference(args):
-    """CPU reference arm: the oracle port on all host threads, rank 0 only."""
+    """CPU reference arm: the oracle port on all host threads, rank 0 only,
+    on the bounded CPU sample of the workload, time-bounded."""
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
-    from bfpn_gpu_b200 import make_config, read_tables
-    from oracle import oracle as O
-
-    cfg = make_config(**WORKLOAD)
-    mu, sig = read_tables(TABLES, cfg.ng)
-    threads = O.max_threads()
-    o = O.Oracle(cfg.grid(), cfg.phys(), mu, sig)
-    o.step(1)  # first step (primary only)
-    warm = min(args.warmup, 1)
-    if warm:
-        o.step(warm)
-    budget = args.reference_budget_s
-    done = 0
-    t0 = time.perf_counter()
-    while done < args.steps:
-        o.step(1)
-        done += 1
-        if time.perf_counter() - t0 > budget:
-            break
-    sec = time.perf_counter() - t0
-    value = 2 * o.cells * done / sec
-    o.close()
-    sample = "%d depth step(s) of the workload, FP64, %d threads (time-bounded at %.0f s)" % (done, threads, budget)
+    rec = oracle_sample(args.steps, budget_s=args.reference_budget_s, warmup=min(args.warmup, 1))
+    if product_library_loaded():
+        raise RuntimeError("the reference arm mapped the solver library")
+    done = rec["steps"]
+    value = rec["value"]
+    cpu = dict(rec)
+    cpu.pop("steps")
     out = {"metric": METRIC, "value": value, "unit": "updates/s", "n_gpus": world, "steps": done,
-           "warmup": warm, "ms_per_step": sec * 1e3 / done, "higher_is_better": True, "scaling": "weak",
-           "vs_baseline": None, "dtype": "f64", "data": "reference water tables; synthetic initial beam",
-           "config": {"workload": WORKLOAD_NAME, "precision": "fp64"}, "impl": "reference",
-           "cpu_baseline": {"value": value, "unit": "updates/s", "cores": threads, "kind": "port", "sample": sample},
+           "warmup": min(args.warmup, 1), "ms_per_step": rec["seconds"] * 1e3 / done, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "reference %s tables; synthetic initial beam" % WORKLOAD["material_name"],
+           "config": {"workload": WORKLOAD_NAME, "precision": "fp64",
+                      "sample": rec["sample"], "time_bound_s": args.reference_budget_s},
+           "impl": "reference", "cpu_baseline": cpu,
            "e2e": {"value": value, "unit": "updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
 
@@ -528,8 +590,8 @@ def main():
     ap.add_argument("--serve-workers", type=int, default=8)
     ap.add_argument("--serve-rate", type=float, default=None, help="Poisson arrival rate (default 0.9 x batched)")
     ap.add_argument("--serve-seed", type=int, default=20261203)
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="water230_20",
-                    help="single-beam workload (the default is the one the metric is quoted on)")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD,
+                    help="single-beam workload (default: the 80x80 paper-scale grid)")
     ap.add_argument("--ng", type=int, default=None,
                     help="energy groups (profiling captures on a smaller state; not for bench lines)")
     ap.add_argument("--out-of-core", action="store_true",
@@ -537,8 +599,10 @@ def main():
     ap.add_argument("--lane-chunk", type=int, default=262144)
     ap.add_argument("--energy-chunk", type=int, default=128)
     args = ap.parse_args()
-    global WORKLOAD, WORKLOAD_NAME, TABLES
+    global WORKLOAD, WORKLOAD_NAME, TABLES, WORKLOAD_KEY
+    WORKLOAD_KEY = args.workload
     WORKLOAD, WORKLOAD_NAME = WORKLOADS[args.workload]
+    WORKLOAD = dict(WORKLOAD)
     TABLES = os.path.join(ROOT, "tests", "golden", "tables", WORKLOAD["material_name"])
     if args.ng:
         WORKLOAD["ng"] = args.ng

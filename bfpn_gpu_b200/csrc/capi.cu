@@ -960,10 +960,15 @@ bfpn_status ensure_history(bfpn_ctx* c, int needed) {
     CUDA_TRY(c, cudaMemcpyAsync(ni, c->hist_idd, c->hist_cap * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
     CUDA_TRY(c, cudaMemcpyAsync(np, c->hist_proxy, c->hist_cap * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    // the step graphs hold the old addresses: drop them before the old buffers go
+    drop_graphs(c);
+    void* old_idd = c->hist_idd;
+    void* old_proxy = c->hist_proxy;
+    dfree(c, old_idd);
+    dfree(c, old_proxy);
     c->hist_idd = static_cast<double*>(ni);
     c->hist_proxy = static_cast<double*>(np);
     c->hist_cap = cap;
-    drop_graphs(c);
     return BFPN_OK;
 }
 

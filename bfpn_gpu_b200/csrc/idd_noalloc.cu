@@ -23,7 +23,6 @@
 #include "common.cuh"
 #include "tables.hpp"
 
-#include <mutex>
 #include <string>
 
 using namespace bfpn;
@@ -43,7 +42,6 @@ constexpr long long kMaxLanes = static_cast<long long>(kMaxBlocks) * kLanesPerBl
 // each block.  65,792 bytes in all.
 constexpr size_t kHeaderBytes = 256;
 constexpr size_t kScratchBytes = kHeaderBytes + 2 * sizeof(double) * kMaxBlocks;
-constexpr int kMaxDevices = 64;
 
 }  // namespace
 
@@ -119,10 +117,6 @@ __global__ void __launch_bounds__(kThreads) idd_noalloc_kernel(const T* __restri
     }
 }
 
-// Device address of the scratch on each device, looked up once per device.
-std::mutex g_setup_mutex;
-void* g_scratch_ptr[kMaxDevices] = {};
-
 bfpn_status noalloc_fail(bfpn_status s, const std::string& msg) {
     set_context_free_error(msg);
     return s;
@@ -163,7 +157,7 @@ extern "C" bfpn_status bfpn_idd_noalloc(const bfpn_grid* grid, int32_t precision
         cudaGetLastError();
         return noalloc_fail(BFPN_NO_DEVICE, "bfpn_idd_noalloc: no CUDA device available");
     }
-    if (device < 0 || device >= ndev || device >= kMaxDevices)
+    if (device < 0 || device >= ndev)
         return noalloc_fail(BFPN_INVALID_ARG, "bfpn_idd_noalloc: device ordinal out of range");
 
     DeviceGuard guard;
@@ -172,20 +166,19 @@ extern "C" bfpn_status bfpn_idd_noalloc(const bfpn_grid* grid, int32_t precision
     e = cudaSetDevice(device);
     if (e != cudaSuccess) return noalloc_fail(BFPN_CUDA_ERROR, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
 
-    // Set-up, once per device, with that device current: the device address
-    // of the scratch (the host-side symbol is not one).
+    // The device address of the scratch (the host-side symbol is not one),
+    // with the device current.  It is looked up on every call rather than
+    // cached: after a cudaDeviceReset (or any other teardown of the primary
+    // context) the module is loaded again and the array may move.  The first
+    // call on a device also loads the module there.
     unsigned char* scratch = nullptr;
     {
-        std::lock_guard<std::mutex> lock(g_setup_mutex);
-        if (!g_scratch_ptr[device]) {
-            void* p = nullptr;
-            e = cudaGetSymbolAddress(&p, g_idd_scratch);
-            if (e != cudaSuccess || !p)
-                return noalloc_fail(BFPN_CUDA_ERROR,
-                                    std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
-            g_scratch_ptr[device] = p;
-        }
-        scratch = static_cast<unsigned char*>(g_scratch_ptr[device]);
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_idd_scratch);
+        if (e != cudaSuccess || !p)
+            return noalloc_fail(BFPN_CUDA_ERROR,
+                                std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+        scratch = static_cast<unsigned char*>(p);
     }
 
     const Deltas d = compute_deltas(g);

@@ -85,6 +85,50 @@ def entrance(x, dose):
     return float(dose[0] / np.max(dose))
 
 
+def peak_depth(idd, dx):
+    """Depth (cm) of the IDD maximum of a run whose row i lies at (i+1)*dx,
+    refined by the parabola through the maximum sample and its two
+    neighbours (sub-step resolution)."""
+    idd = np.asarray(idd, dtype=np.float64)
+    i = int(np.argmax(idd))
+    x = (i + 1) * dx
+    if 0 < i < len(idd) - 1:
+        y0, y1, y2 = idd[i - 1], idd[i], idd[i + 1]
+        den = y0 - 2 * y1 + y2
+        if den != 0:
+            x += 0.5 * dx * (y0 - y2) / den
+    return x
+
+
+# Accuracy bar of a reduced-precision run against an FP64 run of the same
+# beam: the IDD within 0.1 % at every depth where the FP64 dose exceeds 1 % of
+# its peak, and the Bragg peak within 0.1 mm.
+IDD_REL_TOL = 1e-3
+PEAK_FLOOR = 0.01
+BRAGG_SHIFT_TOL_MM = 0.1
+
+
+def idd_accuracy(idd, idd_fp64, dx):
+    """IDD error of `idd` against the FP64 curve of the same beam (same
+    depth grid of step dx cm): the worst pointwise relative error above
+    PEAK_FLOOR of the peak, the worst error relative to the peak, the
+    Bragg-peak shift in mm, and whether the bar above is met."""
+    a = np.asarray(idd, dtype=np.float64)
+    b = np.asarray(idd_fp64, dtype=np.float64)
+    if a.shape != b.shape or a.size == 0:
+        raise ValueError("IDD curves differ in length or are empty")
+    peak = float(np.abs(b).max())
+    big = b > PEAK_FLOOR * peak
+    rel = float((np.abs(a - b)[big] / b[big]).max())
+    shift = abs(peak_depth(a, dx) - peak_depth(b, dx)) * 10.0
+    return {"steps": int(b.size), "idd_max_rel_err_above_1pct_peak": rel,
+            "idd_max_err_rel_to_peak": float(np.abs(a - b).max() / peak),
+            "bragg_peak_cm_fp64": float(peak_depth(b, dx)), "bragg_peak_shift_mm": float(shift),
+            "criterion": "rel err <= %g above %g of peak, Bragg-peak shift <= %g mm"
+                         % (IDD_REL_TOL, PEAK_FLOOR, BRAGG_SHIFT_TOL_MM),
+            "pass": bool(rel <= IDD_REL_TOL and shift <= BRAGG_SHIFT_TOL_MM)}
+
+
 def load_idd(path):
     data = np.loadtxt(path, comments="#", ndmin=2)
     if data.shape[1] < 2:

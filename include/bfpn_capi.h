@@ -399,9 +399,10 @@ bfpn_status bfpn_batch_run(const bfpn_beam* beams, int32_t n, const int32_t* dev
  *
  * Limits: (Ny+1)(Nz+1)*Nmu*Nom <= 4,194,304 lanes (the scratch holds 4096
  * block partials of 1024 lanes each); a larger plane returns
- * BFPN_INVALID_ARG with a message.  The first call on each device does set-up
- * (it looks up the scratch's device address) and should come before any
- * stream capture on that device.  All calls on one device share the scratch:
+ * BFPN_INVALID_ARG with a message.  Every call looks up the scratch's device
+ * address with the device current (so a cudaDeviceReset between calls is
+ * safe); the first call on each device also loads the library's device code
+ * there and should come before any stream capture on that device.  All calls on one device share the scratch:
  * calls that overlap in time on that device (two streams, two host threads)
  * race and give wrong results -- order them on one stream.  Errors are
  * reported through bfpn_last_error(NULL). */

@@ -3,8 +3,8 @@
 FP64 mode: every operator and whole depth steps agree with the CPU FP64
 restatement to 1e-10 relative (operators 1e-11), on seeded states, and the full
 1000-step water 230 MeV runs reproduce the reference's own golden IDD files.
-Mixed mode (float state, double energy recursion): IDD within 1e-3 of the
-peak against FP64.
+Mixed mode (float state, double energy recursion): operator kernels against
+FP64 here; whole-run IDD accuracy at full depth in test_accuracy_gpu.py.
 """
 import numpy as np
 import pytest
@@ -412,20 +412,6 @@ def test_reference_golden_full_run_fp64(grid):
     assert rel_err(idd, gold[:, 1]) < STEP_TOL
     big = gold[:, 1] > 0.01 * gold[:, 1].max()
     assert (np.abs(idd - gold[:, 1])[big] / gold[big, 1]).max() < 1e-9
-
-
-def test_mixed_precision_idd_within_tolerance():
-    cfg = small_cfg(t_final=8.0)
-    mu, sig = read_tables(table_dir("synthetic500"), cfg.ng)
-    ref = Context(cfg.grid(), cfg.phys(), capi.PREC_FP64)
-    mix = Context(cfg.grid(), cfg.phys(), capi.PREC_MIXED)
-    for c in (ref, mix):
-        c.load_tables(mu, sig)
-        c.init_beam()
-    n = cfg.max_steps()
-    i_ref, _ = ref.step(n)
-    i_mix, _ = mix.step(n)
-    assert rel_err(i_mix, i_ref) < 1e-3
 
 
 @pytest.mark.parametrize("flags", [{}, {"trapezoidal_yz": True, "discrete_angle_delta": True,

@@ -75,3 +75,20 @@ def test_table2_runner_with_a_stand_in_solver(tmp_path):
     # analysis only, on the outputs just written
     again = V.run_table2(exe="/nonexistent", outdir="t2", cwd=str(tmp_path), skip_run=True)
     assert again == res
+
+
+def test_accuracy_metric_flags_a_planted_error():
+    """The criterion itself, on the CPU: a 0.2 % bump above 1 % of the peak
+    or a one-step peak shift fails; a bump in the tail below 1 % passes."""
+    x = np.arange(1, 1001) * 0.04
+    ref = np.exp(-0.5 * ((x - 30.0) / 1.5) ** 2) + 0.2 * (x < 30.0)
+    ok = ref * (1 + 5e-4)
+    assert V.idd_accuracy(ok, ref, 0.04)["pass"]
+    bad = ref.copy()
+    bad[500] *= 1.002
+    assert not V.idd_accuracy(bad, ref, 0.04)["pass"]
+    tail = ref.copy()
+    tail[-1] *= 1.5  # the tail is below 1 % of the peak
+    assert ref[-1] < 0.01 * ref.max() and V.idd_accuracy(tail, ref, 0.04)["pass"]
+    shifted = np.roll(ref, 1)
+    assert V.idd_accuracy(shifted, ref, 0.04)["bragg_peak_shift_mm"] > V.BRAGG_SHIFT_TOL_MM

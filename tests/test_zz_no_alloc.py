@@ -107,3 +107,39 @@ def test_noalloc_rejects_oversized_plane_and_bad_arguments():
         capi.idd_noalloc(g, capi.PREC_FP64, False, None, p, None, None, p, p)
     with pytest.raises(capi.BfpnError, match="precision"):
         capi.idd_noalloc(g, 7, False, p, p, None, None, p, p)
+
+
+@pytest.mark.parametrize("ny,nmu,trap", [(40, 12, False), (40, 12, True), (100, 20, True)])
+def test_noalloc_large_planes_and_edge_weights(ny, nmu, trap):
+    """Planes of a few hundred and of nearly 4096 blocks (101 x 101 x 400 =
+    4,080,400 lanes), with and without the trapezoidal yz edge weights, on
+    seeded states: the ticket / last-block path against bfpn_idd."""
+    from bfpn_gpu_b200 import make_config
+    from conftest import table_dir
+    from bfpn_gpu_b200 import read_tables
+
+    cfg = make_config(nx=400, ny=ny, nz=ny, nmu=nmu, nom=nmu, ng=6, ly=4.0, lz=4.0, lg=12.0, beam_energy=6.0,
+                      sigma_e=1.0, sigma_yz=0.5, material_name="water", trapezoidal_yz=trap)
+    mu, sig = read_tables(table_dir("synthetic500"), cfg.ng)
+    ctx = Context(cfg.grid(), cfg.phys(), capi.PREC_FP64)
+    ctx.load_tables(mu, sig)
+    rng = np.random.default_rng(20261203 + ny + nmu + trap)
+    for s in (0, 1):
+        ctx.set_state(s, 0, rng.random(ctx.cells))
+        ctx.set_state(s, 1, rng.normal(0.0, 1e-3, ctx.cells))
+    ref_idd, ref_proxy = ctx.idd()
+    arrays = device_state(ctx, torch.float64)
+    dc = torch.from_numpy(dose_weights(ctx, cfg)).cuda()
+    out = torch.zeros(2, dtype=torch.float64, device="cuda")
+    got = noalloc(cfg, capi.PREC_FP64, arrays, dc, out)
+    assert abs(got[0] - ref_idd) <= 1e-12 * abs(ref_idd)
+    proxy_scale = float(arrays[1].abs().sum()) * cfg.grid().Lg / cfg.ng
+    assert abs(got[1] - ref_proxy) <= 1e-12 * proxy_scale
+    # a warm call takes no device memory: the free bytes the driver reports do not move
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    again = noalloc(cfg, capi.PREC_FP64, arrays, dc, out)
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    assert np.array_equal(again, got)
+    ctx.close()
