@@ -36,7 +36,7 @@ FLAG_LITE_MEMORY = 1 << 13
 FLAG_STREAMING_FULL = 1 << 14
 # run-time options
 (OPT_TENSOR_CORES, OPT_CUDA_GRAPHS, OPT_PLANE_TRANSPORT, OPT_PAIRED_ANGLES, OPT_CLUSTER_TRANSPORT, OPT_LANE_CHUNK,
- OPT_ENERGY_CHUNK, OPT_STEP_OVERLAP) = range(8)
+ OPT_ENERGY_CHUNK, OPT_STEP_OVERLAP, OPT_STREAM_TRANSPORT) = range(9)
 # kernel classes of the profile
 KERNEL_CLASSES = ["energy", "transport", "angle", "source_angular", "source_energy", "idd"]
 # tables
@@ -123,6 +123,20 @@ SIGNATURES = {
     "bfpn_server_last_error": (ctypes.c_char_p, []),
     "bfpn_batch_run": (ctypes.c_int, [ctypes.POINTER(Beam), _i32, ctypes.POINTER(_i32), _i32, _i32,
                                       ctypes.POINTER(_dp), ctypes.POINTER(_dp), ctypes.POINTER(ctypes.c_int)]),
+    "bfpn_bundle_accepts": (ctypes.c_int, [ctypes.POINTER(Beam)]),
+    "bfpn_bundle_create": (ctypes.c_int, [_i32, _i32, ctypes.POINTER(_vp)]),
+    "bfpn_server_set_batching": (ctypes.c_int, [_vp, _i32]),
+    "bfpn_bundle_set_option": (ctypes.c_int, [_vp, _i32, _i32]),
+    "bfpn_bundle_admit": (ctypes.c_int, [_vp, ctypes.POINTER(Beam), ctypes.POINTER(_i32)]),
+    "bfpn_bundle_step": (ctypes.c_int, [_vp, _i32]),
+    "bfpn_bundle_sync": (ctypes.c_int, [_vp]),
+    "bfpn_bundle_running": (_i32, [_vp]),
+    "bfpn_bundle_slot": (ctypes.c_int, [_vp, _i32, ctypes.POINTER(_i32), ctypes.POINTER(_i32)]),
+    "bfpn_bundle_collect": (ctypes.c_int, [_vp, _i32, _dp, _dp, _i32]),
+    "bfpn_bundle_tuning": (_i32, [_vp, ctypes.c_char_p, _i32]),
+    "bfpn_bundle_stream": (_vp, [_vp]),
+    "bfpn_bundle_destroy": (ctypes.c_int, [_vp]),
+    "bfpn_bundle_last_error": (ctypes.c_char_p, [_vp]),
     "bfpn_device_count": (_i32, []),
     "bfpn_device_info": (_i32, [_i32, ctypes.c_char_p, _i32]),
     "bfpn_stream": (_vp, [_vp]),
@@ -212,13 +226,20 @@ class Server:
     """bfpn_server_*: a queue of independent beams served by worker threads,
     each owning one context on one device."""
 
-    def __init__(self, devices=(0,), workers_per_device=1):
+    def __init__(self, devices=(0,), workers_per_device=1, batching=True):
         devs = (_i32 * len(devices))(*devices)
         h = _vp()
         rc = lib().bfpn_server_create(devs, len(devices), workers_per_device, ctypes.byref(h))
         if rc != OK:
             raise _server_error(rc)
         self._h = h
+        if not batching:
+            self.set_batching(False)
+
+    def set_batching(self, on):
+        rc = lib().bfpn_server_set_batching(self._h, 1 if on else 0)
+        if rc != OK:
+            raise _server_error(rc)
 
     def submit(self, beam):
         t = ctypes.c_uint64(0)
@@ -242,6 +263,86 @@ class Server:
     def close(self):
         if getattr(self, "_h", None):
             lib().bfpn_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def bundle_accepts(beam):
+    """True when a bundle can hold the beam (host-side check)."""
+    return lib().bfpn_bundle_accepts(ctypes.byref(beam)) == OK
+
+
+# bundle options
+BUNDLE_OPT_AUTOTUNE, BUNDLE_OPT_TRANSPORT_ANGLES, BUNDLE_OPT_DST_STAGES, BUNDLE_OPT_ENERGY_RING = 1, 2, 3, 4
+
+
+class Bundle:
+    """bfpn_bundle_*: mixed-precision beams of one shape class advanced
+    together, one launch per operator per depth step for every slot."""
+
+    def __init__(self, device=0, max_slots=16):
+        h = _vp()
+        rc = lib().bfpn_bundle_create(device, max_slots, ctypes.byref(h))
+        if rc != OK:
+            raise BfpnError(rc, lib().bfpn_bundle_last_error(None).decode())
+        self._h = h
+        self._beams = {}
+
+    def _check(self, rc):
+        if rc != OK:
+            raise BfpnError(rc, lib().bfpn_bundle_last_error(self._h).decode())
+
+    def set_option(self, option, value):
+        self._check(lib().bfpn_bundle_set_option(self._h, option, value))
+
+    def admit(self, beam):
+        """Slot of the admitted beam (a make_beam request)."""
+        slot = _i32(-1)
+        self._check(lib().bfpn_bundle_admit(self._h, ctypes.byref(beam), ctypes.byref(slot)))
+        self._beams[slot.value] = beam
+        return slot.value
+
+    def step(self, n):
+        self._check(lib().bfpn_bundle_step(self._h, int(n)))
+
+    def sync(self):
+        self._check(lib().bfpn_bundle_sync(self._h))
+
+    def running(self):
+        return int(lib().bfpn_bundle_running(self._h))
+
+    def slot(self, k):
+        done, total = _i32(0), _i32(0)
+        self._check(lib().bfpn_bundle_slot(self._h, k, ctypes.byref(done), ctypes.byref(total)))
+        return done.value, total.value
+
+    def collect(self, k):
+        """(idd, proxy) of a finished slot; frees the slot."""
+        _, n = self.slot(k)
+        idd, prox = np.empty(n), np.empty(n)
+        self._check(lib().bfpn_bundle_collect(self._h, k, _ptr(idd), _ptr(prox), n))
+        self._beams.pop(k, None)
+        return idd, prox
+
+    def tuning(self):
+        buf = ctypes.create_string_buffer(512)
+        lib().bfpn_bundle_tuning(self._h, buf, 512)
+        return buf.value.decode()
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().bfpn_bundle_destroy(self._h)
             self._h = None
 
     def __del__(self):

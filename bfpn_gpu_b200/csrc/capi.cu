@@ -8,6 +8,7 @@
 
 #include "../../include/bfpn_capi.h"
 #include "common.cuh"
+#include "context.cuh"
 #include "tables.hpp"
 
 #include <algorithm>
@@ -26,139 +27,7 @@ namespace {
 
 thread_local std::string g_create_error;
 
-struct DevBuf {
-    void* p = nullptr;
-    size_t bytes = 0;
-};
-
 }  // namespace
-
-struct bfpn_ctx {
-    bfpn_grid g{};
-    bfpn_phys p{};
-    int prec = BFPN_PREC_FP64;
-    int device = 0;
-    size_t elem = 8;
-    Deltas d{};
-    int Ng = 0, Ny = 0, Nz = 0, Nmu = 0, Nom = 0, nyz = 0, NA = 0;
-    long long per_e = 0, cells = 0;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-
-    std::vector<DevBuf> allocs;
-    void* st[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
-    void* tmp = nullptr;       // out-of-place transport target (tiled planes only)
-    void* src = nullptr;       // secondary source
-    void* A1 = nullptr;        // angular contractions of the primary (one block of a_bytes; A2 inside it,
-    void* A2 = nullptr;        // or the whole block in the tensor-core operand layout)
-    size_t a_bytes = 0;
-    double* ecoef_half = nullptr;   // energy constants for dt/2
-    double* ecoef_op = nullptr;     // energy constants for a per-operator dt
-    double ecoef_op_dt = -1.0;
-    double* dose_coef = nullptr;
-    void* omega = nullptr;
-    void* fac_step = nullptr;       // angle factor for the full step dt
-    void* fac_op = nullptr;         // angle factor for a per-operator dt
-    double fac_op_dt = -1.0;
-    void* sine_u = nullptr;
-    void* sine_v = nullptr;
-    void* ker_v = nullptr;
-    double* e1 = nullptr;
-    double* e2 = nullptr;
-    int* groups = nullptr;
-    int n_groups = 0;
-    int* tile_lo = nullptr;
-    int* tile_hi = nullptr;
-    int tile_e = 16;
-    double* beam_yza = nullptr;
-    double* beam_e = nullptr;
-    double* partials = nullptr;     // [2][energy_grid][2]
-    int n_part = 0;
-    double* hist_idd = nullptr;
-    double* hist_proxy = nullptr;
-    int hist_cap = 0;
-    int* counter = nullptr;
-    int* zero_counter = nullptr;    // scratch counter for one-off IDD reductions
-    int* dev_err = nullptr;         // device error word (bounded waits that ran out)
-    void* bblob = nullptr;          // split-bf16 angular kernel tiles for the tensor-core source
-    void* ablob = nullptr;          // packed split-bf16 A operand (pipelined tensor-core source)
-    void* eblob = nullptr;          // split-bf16 energy coefficient tiles (tensor-core source)
-    int* ework = nullptr;           // energy work items {chunk, column, columns, e group}
-    int* ework_begin = nullptr;     // [e tiles + 1]
-    int e_et = 0, e_emax = 0;
-    bool use_umma = true;
-    int umma_nt = 0, umma_bk = 16, umma_ntiles = 0;
-    double* scalar_out = nullptr;   // [2] one-off IDD / proxy
-    double* moments = nullptr;      // [Ng][2]
-    double* plane = nullptr;        // [nyz] spot dose plane
-    bool lite = false;              // lite-memory mode: psi^1 of the primary only
-    // out-of-core mode: st[][] are pinned host arrays; device chunk buffers
-    bool ooc = false;
-    int ooc_lane_req = 262144, ooc_group_req = 128;  // requested chunk sizes (lanes, groups)
-    int lc_pos = 0, lc = 0, n_lc = 0, ecg = 0;        // positions / lanes per lane chunk, lane chunks, groups per group chunk
-    bool ooc_ready = false;
-    void* dl[2][4] = {};    // two slots of a lane chunk: the species' psi^1, psi^2; the primary's for the source
-    void* dgc[2] = {};      // two slots of a group chunk
-    cudaStream_t s_in = nullptr, s_out = nullptr;        // host-to-device / device-to-host copies
-    cudaEvent_t ev_in[2] = {}, ev_comp[2] = {}, ev_out[2] = {}, ev_pass = nullptr;
-    void* ooc_part = nullptr;                            // IDD partials of every lane chunk, both species
-    std::vector<void*> host_allocs;
-    double* lite_coef = nullptr;    // [Ng][2] lite step constants
-
-    BeamTables tables;
-    std::vector<double> raw_sigma;  // sigma_c as given, before the optional calibration
-    bool tables_loaded = false;
-    bool beam_ready = false;
-    int steps_done = 0;
-    bool secondary_zero = true;
-
-    // transport launch shape
-    int tr_ac = 16, tr_ty = 1, tr_tz = 1;
-    bool tr_inplace = true;
-    bool tr_plane_ok = false;   // a compiled whole-plane kernel exists for this plane
-    bool tr_plane = false;      // use it
-    int tr_plane_ac = 8;
-    bool tr_pairs_ok = false;   // angle pairs share direction signs (float whole planes)
-    bool tr_pairs = true;       // use the paired kernel where it applies
-    bool tr_cluster_ok = false; // a cluster kernel is compiled for this plane (float state)
-    int tr_cluster = 1;         // 0 off, 1 planes without a whole-plane kernel, 2 every supported plane
-    bool tr_tile_ok = false;    // the plane needs tiles: the unrolled tiled kernel applies
-    bool tr_tile = false;       // use it
-    int tr_tile_ac = 8;
-    int ang_slices = 4;
-    int energy_block = 128;
-
-    cudaGraphExec_t graph_exec = nullptr;
-    int graph_key = -1;
-    bool use_graphs = true;
-    // overlapped steps: the secondary half of step n (source, energy and
-    // transport of the secondary species, the step's IDD) runs on s_sec beside
-    // the primary half of step n+1; graph ovl_exec[p] serves steps of parity p
-    bool overlap = true;
-    bool pending_sec = false;  // the secondary half of step steps_done-1 is still owed
-    cudaStream_t s_sec = nullptr;
-    cudaEvent_t ev_fork = nullptr, ev_pread = nullptr, ev_join = nullptr;
-    // inside an overlapped body the T-A-T chains of psi^2 also get their own
-    // streams (one per species): s_f[k], forked / joined by ev_ff[k] / ev_fj[k]
-    bool split_tat = false;
-    bool split_chains = true;  // option: split the chains in overlapped bodies
-    cudaStream_t s_f[2] = {nullptr, nullptr};
-    cudaEvent_t ev_ff[2] = {nullptr, nullptr}, ev_fj[2] = {nullptr, nullptr};
-    cudaGraphExec_t ovl_exec[2] = {nullptr, nullptr};
-    bool profiling = false;
-    struct Pending {
-        int cls;
-        cudaEvent_t a, b;
-    };
-    std::vector<cudaEvent_t> ev_pool;
-    std::vector<Pending> pending;
-    double prof_ms[BFPN_KERNEL_CLASSES] = {};
-    int prof_n[BFPN_KERNEL_CLASSES] = {};
-    long long launches = 0;        // launches issued by host enqueue code
-    int kernels_per_step = 0;
-
-    std::string err;
-};
 
 namespace {
 
@@ -406,15 +275,25 @@ void choose_plane_transport(bfpn_ctx* c) {
     c->tr_tile_ok = !c->tr_plane_ok && !c->tr_inplace;
     c->tr_tile = c->tr_tile_ok;
     c->tr_cluster_ok = c->elem == 4 && transport_cluster_supported(c->Ny, c->Nz);
+    c->tr_stream_ok = c->elem == 4 && transport_stream_supported(c->Ny, c->NA);
+}
+
+// The row-streaming kernel runs this context's transport (it needs paired angles).
+bool stream_transport(const bfpn_ctx* c) {
+    if (!c->tr_stream_ok || !c->tr_pairs || !c->tr_pairs_ok) return false;
+    return c->tr_stream == 2 || (c->tr_stream == 1 && !c->tr_plane);
 }
 
 // The cluster kernel runs this context's transport (it needs paired angles).
 bool cluster_transport(const bfpn_ctx* c) {
+    if (stream_transport(c)) return false;
     if (!c->tr_cluster_ok || !c->tr_pairs || !c->tr_pairs_ok) return false;
     return c->tr_cluster == 2 || (c->tr_cluster == 1 && !c->tr_plane);
 }
 
-bool transport_in_place(const bfpn_ctx* c) { return c->tr_plane || c->tr_inplace || cluster_transport(c); }
+bool transport_in_place(const bfpn_ctx* c) {
+    return c->tr_plane || c->tr_inplace || cluster_transport(c) || stream_transport(c);
+}
 
 template <typename T>
 bfpn_status upload_as(bfpn_ctx* c, void* dst, const double* host, size_t n) {
@@ -488,6 +367,8 @@ cudaError_t enq_transport(bfpn_ctx* c, const void* in, void* out, double dt, boo
     a.preserve_sign = preserve_sign ? 1 : 0;
     a.pairs = (c->elem == 4 && c->tr_pairs && c->tr_pairs_ok) ? 1 : 0;
     if constexpr (sizeof(T) == 4) {
+        if (stream_transport(c))
+            return prof(c, BFPN_KERNEL_TRANSPORT, [&] { return launch_transport_stream(a, c->stream); });
         if (cluster_transport(c))
             return prof(c, BFPN_KERNEL_TRANSPORT, [&] { return launch_transport_cluster(a, c->stream); });
     }
@@ -1732,6 +1613,12 @@ bfpn_status bfpn_set_option(bfpn_ctx* c, int32_t option, int32_t value) {
             if (value < 1) return fail(c, BFPN_INVALID_ARG, "chunk sizes must be positive");
             (option == BFPN_OPT_LANE_CHUNK ? c->ooc_lane_req : c->ooc_group_req) = value;
             break;
+        case BFPN_OPT_STREAM_TRANSPORT:
+            if (value < 0 || value > 2) return fail(c, BFPN_INVALID_ARG, "stream transport: 0, 1 or 2");
+            if (value == 2 && !c->tr_stream_ok)
+                return fail(c, BFPN_INVALID_ARG, "no row-streaming transport for this plane size / precision");
+            c->tr_stream = value;
+            break;
         case BFPN_OPT_CLUSTER_TRANSPORT:
             if (value < 0 || value > 2) return fail(c, BFPN_INVALID_ARG, "cluster transport: 0, 1 or 2");
             if (value == 2 && !c->tr_cluster_ok)
@@ -2019,3 +1906,126 @@ int32_t bfpn_device_info(int32_t device, char* buf, int32_t buf_len) {
 }
 
 }  // extern "C"
+
+// ============================================================================
+// Per-slot step pieces for bundles (bundle.cu): the arguments enq_energy,
+// enq_transport and enq_angle would build for this context, the source on a
+// given stream, and the IDD finalisation.
+// ============================================================================
+namespace bfpn {
+
+std::string bundle_ready(const bfpn_ctx* c) {
+    if (!c) return "null context";
+    if (c->prec != BFPN_PREC_MIXED) return "a bundle holds mixed-precision beams";
+    if (c->lite || c->ooc) return "lite-memory and out-of-core beams run alone";
+    const unsigned fl = c->p.flags;
+    if (fl & (BFPN_FLAG_ENERGY_ONLY | BFPN_FLAG_PRIMARY_ONLY | BFPN_FLAG_NO_TRANSPORT | BFPN_FLAG_NO_ANGLE |
+              BFPN_FLAG_LEGACY_ENERGY))
+        return "a bundle runs the eq15 step with transport, angular diffusion and secondaries";
+    if (!c->tables_loaded || !c->beam_ready) return "load the tables and the initial beam first";
+    if (!(c->tr_pairs && c->tr_pairs_ok)) return "the angle pairs do not share direction signs";
+    if (!(stream_transport(c) || cluster_transport(c) || c->tr_plane))
+        return "no whole-plane, row-streaming or cluster transport kernel for this plane";
+    if (c->Nom != c->Nmu || c->Nom % 2 != 0 || c->Nom < 4 || c->Nom > 32 || c->Nom == 26 || c->Nom == 30)
+        return "the angular grid must be square with an even side in 4..24, 28 or 32";
+    if (c->nyz < angle_slots_tile(c->Nom)) return "the plane is smaller than one DST tile";
+    if (c->per_e % 4 != 0) return "Ny+1, Nz+1, Nmu, Nom give a lane count that is not a multiple of 4";
+    return "";
+}
+
+EnergyArgs<float> bundle_energy_args(bfpn_ctx* c, int species, bool with_source, double* partials) {
+    EnergyArgs<float> a;
+    a.F = as<float>(c->st[species][0]);
+    a.f = as<float>(c->st[species][1]);
+    a.src = with_source ? as<const float>(c->src) : nullptr;
+    a.coef = c->ecoef_half;
+    a.Ng = c->Ng;
+    a.lanes = c->per_e;
+    a.mode = (c->p.flags & BFPN_FLAG_EQ15_STRAGGLING) ? EMODE_EQ15_STRAG : EMODE_EQ15;
+    a.partials = partials;
+    a.dose_coef = c->dose_coef;
+    a.NA = c->NA;
+    a.Ny = c->Ny;
+    a.Nz = c->Nz;
+    a.trapezoidal = (c->p.flags & BFPN_FLAG_TRAPEZOIDAL_YZ) ? 1 : 0;
+    return a;
+}
+
+TransportArgs<float> bundle_transport_args(bfpn_ctx* c, int species, int coef, bool preserve_sign) {
+    TransportArgs<float> a;
+    a.in = as<const float>(c->st[species][coef]);
+    a.out = as<float>(c->st[species][coef]);
+    a.omega = as<const float>(c->omega);
+    a.Ny = c->Ny;
+    a.Nz = c->Nz;
+    a.NA = c->NA;
+    a.Ng = c->Ng;
+    a.dt = static_cast<float>(0.5 * c->d.dt);
+    a.dy = static_cast<float>(c->d.dy);
+    a.dz = static_cast<float>(c->d.dz);
+    a.tile_y = c->tr_ty;
+    a.tile_z = c->tr_tz;
+    a.preserve_sign = preserve_sign ? 1 : 0;
+    a.pairs = 1;
+    return a;
+}
+
+AngleArgs<float> bundle_angle_args(bfpn_ctx* c, int species, int coef, int* err) {
+    AngleArgs<float> a;
+    a.F = as<float>(c->st[species][coef]);
+    a.fac = as<const float>(c->fac_step);
+    a.sine_u = as<const float>(c->sine_u);
+    a.sine_v = as<const float>(c->sine_v);
+    a.Nom = c->Nom;
+    a.Nmu = c->Nmu;
+    a.nyz = c->nyz;
+    a.Ng = c->Ng;
+    a.slices_per_block = angle_slots_tile(c->Nom);
+    a.err = err;
+    a.pairs = 1;
+    return a;
+}
+
+cudaError_t bundle_source(bfpn_ctx* c, cudaStream_t s) {
+    cudaStream_t own = c->stream;
+    c->stream = s;
+    const cudaError_t e = enq_source<float>(c, nullptr);
+    c->stream = own;
+    return e;
+}
+
+double* bundle_partials(bfpn_ctx* c, int species) {
+    return species == 0 ? primary_partials(c, 0) : c->partials + 2 * static_cast<size_t>(c->n_part);
+}
+
+IddFinalArgs bundle_finalize_args(bfpn_ctx* c, bool secondary) {
+    IddFinalArgs f;
+    const int nP = energy_grid(c->per_e, c->energy_block);
+    f.p = bundle_partials(c, 0);
+    f.n = nP;
+    f.p2 = secondary ? bundle_partials(c, 1) : nullptr;
+    f.n2 = secondary ? nP : 0;
+    f.idd_scale = c->d.du * c->d.dv * c->d.dy * c->d.dz;
+    f.proxy_scale = c->d.dg;
+    f.hist_idd = c->hist_idd;
+    f.hist_proxy = c->hist_proxy;
+    f.counter = c->counter;
+    f.capacity = c->hist_cap;
+    return f;
+}
+
+bfpn_status bundle_reserve_history(bfpn_ctx* c, int n) { return ensure_history(c, c->steps_done + n); }
+
+int bundle_cluster_size(const bfpn_ctx* c) { return cluster_transport(c) ? transport_cluster_size(c->Ny + 1) : 0; }
+
+bool bundle_stream_transport(const bfpn_ctx* c) { return stream_transport(c); }
+
+std::string bundle_class_key(const bfpn_ctx* c) {
+    char buf[160];
+    std::snprintf(buf, sizeof buf, "plane %dx%d angles %dx%d %s %s", c->Ny + 1, c->Nz + 1, c->Nmu, c->Nom,
+                  stream_transport(c) ? "row-streaming" : cluster_transport(c) ? "cluster" : "whole-plane",
+                  (c->p.flags & BFPN_FLAG_EQ15_STRAGGLING) ? "eq15+straggling" : "eq15");
+    return buf;
+}
+
+}  // namespace bfpn

@@ -107,6 +107,63 @@ struct SourceArgs {
     double dg;
 };
 
+// ---- multi-slot launches (a bundle of beams of one shape class) ----------
+// One launch serves several slots: blocks (or work tiles) [begin[s],
+// begin[s+1]) belong to slot s and read that slot's argument struct from a
+// device array.  begin has nslots + 1 entries, begin[0] = 0.
+#ifdef __CUDACC__
+__device__ __forceinline__ int find_slot(const int* __restrict__ begin, int nslots, long long b) {
+    int lo = 0, hi = nslots - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(begin + mid) <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+#endif
+
+// Arguments of one slot's IDD finalisation (launch_finalize_idd's arguments).
+struct IddFinalArgs {
+    const double* p;
+    int n;
+    const double* p2;
+    int n2;
+    double idd_scale, proxy_scale;
+    double* hist_idd;
+    double* hist_proxy;
+    int* counter;
+    int capacity;
+};
+
+// Float state only.  args / begin are device arrays; blocks = begin[nslots].
+// Energy sweep: ring = the 4-lane ring kernel (lanes % 4 == 0, not legacy),
+// else the register kernel with `block` threads; every slot's grid is that
+// kernel's energy_grid of its lanes.
+cudaError_t launch_energy_slots(const EnergyArgs<float>* args, const int* begin, int nslots, int blocks, int mode,
+                                bool ring, int block, cudaStream_t s);
+// Transport of square planes of NP = Ny + 1 points, paired angles: the
+// whole-plane kernel with ang_chunk angles per block (NP a compiled plane
+// size; slot grid Ng * ceil(NA / ang_chunk)) or, for a compiled cluster size,
+// the cluster kernel (slot grid Ng * ceil(NA / 8) * cluster size).
+cudaError_t launch_transport_slots(const TransportArgs<float>* args, const int* begin, int nslots, int blocks,
+                                   int NP, int NA, int ang_chunk, bool cluster, cudaStream_t s);
+int transport_cluster_size(int NP);
+// Row-streaming transport (float state, paired angles, Ny + 1 <= 128, any Nz):
+// one block per (group, 8-angle chunk) plane walking the z rows, in place.
+cudaError_t launch_transport_stream(const TransportArgs<float>& a, cudaStream_t s);
+bool transport_stream_supported(int Ny, int NA);
+// The same over the slots of a bundle (slot grid Ng * ceil(NA / 8)).
+cudaError_t launch_transport_stream_slots(const TransportArgs<float>* args, const int* begin, int nslots, int blocks,
+                                          int Ny, int NA, cudaStream_t s);
+// Pipelined paired DST (Nom = Nmu = N even): work tiles of 2 * 128 / N slices;
+// tile_begin = tile offsets (slot s has ceil(Ng nyz / tile) tiles); stages 2 or 3.
+cudaError_t launch_angle_slots(const AngleArgs<float>* args, const int* tile_begin, int nslots, long long tiles,
+                               int N, int stages, cudaStream_t s);
+int angle_slots_tile(int N);
+// IDD finalisation, one block per slot (advance the counters).
+cudaError_t launch_finalize_idd_slots(const IddFinalArgs* args, int nslots, cudaStream_t s);
+
 // Launchers (kernels_*.cu).  All return the launch status.
 template <typename T> cudaError_t launch_energy(const EnergyArgs<T>& a, int block, cudaStream_t s);
 // Lite-memory primary step over psi^1 with fused IDD partials (psi^2 column 0);

@@ -71,8 +71,10 @@ __device__ __forceinline__ void energy_lane_update(const double* __restrict__ c,
     }
 }
 
-template <int MODE, typename T, int LPT, int D = 4, int NTH = 128, int MINB = (sizeof(T) == 4 ? 5 : 4)>
-__global__ void __launch_bounds__(NTH, MINB) energy_kernel(EnergyArgs<T> a) {
+// The sweep of block `bid` of one beam's lanes (the kernels below map their
+// blocks onto it: one beam, or the slots of a bundle).
+template <int MODE, typename T, int LPT, int D>
+__device__ __forceinline__ void energy_body(const EnergyArgs<T>& a, long long bid) {
     // D: groups prefetched ahead of use
     const long long L = a.lanes;
     const int Ng = a.Ng;
@@ -80,7 +82,7 @@ __global__ void __launch_bounds__(NTH, MINB) energy_kernel(EnergyArgs<T> a) {
     bool ok[LPT];
 #pragma unroll
     for (int j = 0; j < LPT; ++j) {
-        lane[j] = static_cast<long long>(blockIdx.x) * blockDim.x * LPT + threadIdx.x + j * blockDim.x;
+        lane[j] = bid * blockDim.x * LPT + threadIdx.x + j * blockDim.x;
         ok[j] = lane[j] < L;
     }
     const T* __restrict__ sp = a.src;
@@ -165,11 +167,23 @@ __global__ void __launch_bounds__(NTH, MINB) energy_kernel(EnergyArgs<T> a) {
                 accp += __shfl_down_sync(0xffffffffu, accp, o);
             }
             if (l == 0) {
-                a.partials[2 * blockIdx.x] = acc;
-                a.partials[2 * blockIdx.x + 1] = accp;
+                a.partials[2 * bid] = acc;
+                a.partials[2 * bid + 1] = accp;
             }
         }
     }
+}
+
+template <int MODE, typename T, int LPT, int D = 4, int NTH = 128, int MINB = (sizeof(T) == 4 ? 5 : 4)>
+__global__ void __launch_bounds__(NTH, MINB) energy_kernel(EnergyArgs<T> a) {
+    energy_body<MODE, T, LPT, D>(a, blockIdx.x);
+}
+
+template <int MODE, int LPT, int D = 4, int NTH = 128, int MINB = 5>
+__global__ void __launch_bounds__(NTH, MINB) energy_slots_kernel(const EnergyArgs<float>* __restrict__ args,
+                                                                  const int* __restrict__ begin, int nslots) {
+    const int s = find_slot(begin, nslots, blockIdx.x);
+    energy_body<MODE, float, LPT, D>(args[s], blockIdx.x - __ldg(begin + s));
 }
 
 // Float state, lanes a multiple of 4: each thread sweeps 4 consecutive lanes
@@ -182,12 +196,12 @@ __global__ void __launch_bounds__(NTH, MINB) energy_kernel(EnergyArgs<T> a) {
 constexpr int kEnergyRing = 8, kEnergyRingThreads = 64;
 
 template <int MODE, int D, int NTH>
-__global__ void __launch_bounds__(NTH) energy_ring_kernel(EnergyArgs<float> a) {
+__device__ __forceinline__ void energy_ring_body(const EnergyArgs<float>& a, long long bid) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float4* ring = reinterpret_cast<float4*>(smem_raw);  // [D][3][NTH]
     const long long L = a.lanes;
     const int Ng = a.Ng, tid = threadIdx.x;
-    const long long lane0 = (static_cast<long long>(blockIdx.x) * NTH + tid) * 4;
+    const long long lane0 = (bid * NTH + tid) * 4;
     const bool ok = lane0 < L;  // L % 4 == 0: the 4 lanes are all in or all out
     const float* __restrict__ sp = a.src;
     auto slot = [&](int k, int arr) { return ring + (k * 3 + arr) * NTH + tid; };
@@ -272,10 +286,22 @@ __global__ void __launch_bounds__(NTH) energy_ring_kernel(EnergyArgs<float> a) {
                 s0 += red[0][k];
                 s1 += red[1][k];
             }
-            a.partials[2 * blockIdx.x] = s0;
-            a.partials[2 * blockIdx.x + 1] = s1;
+            a.partials[2 * bid] = s0;
+            a.partials[2 * bid + 1] = s1;
         }
     }
+}
+
+template <int MODE, int D, int NTH>
+__global__ void __launch_bounds__(NTH) energy_ring_kernel(EnergyArgs<float> a) {
+    energy_ring_body<MODE, D, NTH>(a, blockIdx.x);
+}
+
+template <int MODE, int D, int NTH>
+__global__ void __launch_bounds__(NTH) energy_ring_slots_kernel(const EnergyArgs<float>* __restrict__ args,
+                                                                const int* __restrict__ begin, int nslots) {
+    const int s = find_slot(begin, nslots, blockIdx.x);
+    energy_ring_body<MODE, D, NTH>(args[s], blockIdx.x - __ldg(begin + s));
 }
 
 int energy_ring_grid(long long lanes) {
@@ -290,6 +316,29 @@ cudaError_t launch_energy_ring(const EnergyArgs<float>& a, cudaStream_t s) {
     const int grid = energy_ring_grid(a.lanes);
     if (a.mode == EMODE_EQ15) energy_ring_kernel<EMODE_EQ15, D, NTH><<<grid, NTH, smem, s>>>(a);
     else energy_ring_kernel<EMODE_EQ15_STRAG, D, NTH><<<grid, NTH, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_energy_slots(const EnergyArgs<float>* args, const int* begin, int nslots, int blocks, int mode,
+                                bool ring, int block, cudaStream_t s) {
+    if (nslots <= 0 || blocks <= 0) return cudaSuccess;
+    if (ring) {
+        if (mode == EMODE_LEGACY) return cudaErrorNotSupported;
+        constexpr int D = kEnergyRing, NTH = kEnergyRingThreads;
+        const size_t smem = static_cast<size_t>(D) * 3 * NTH * sizeof(float4);
+        if (mode == EMODE_EQ15) energy_ring_slots_kernel<EMODE_EQ15, D, NTH><<<blocks, NTH, smem, s>>>(args, begin, nslots);
+        else energy_ring_slots_kernel<EMODE_EQ15_STRAG, D, NTH><<<blocks, NTH, smem, s>>>(args, begin, nslots);
+        return cudaGetLastError();
+    }
+    if (block != 128) return cudaErrorNotSupported;
+    constexpr int LPT = kEnergyLanesPerThread;
+    switch (mode) {
+        case EMODE_EQ15: energy_slots_kernel<EMODE_EQ15, LPT><<<blocks, 128, 0, s>>>(args, begin, nslots); break;
+        case EMODE_EQ15_STRAG:
+            energy_slots_kernel<EMODE_EQ15_STRAG, LPT><<<blocks, 128, 0, s>>>(args, begin, nslots);
+            break;
+        default: energy_slots_kernel<EMODE_LEGACY, LPT><<<blocks, 128, 0, s>>>(args, begin, nslots); break;
+    }
     return cudaGetLastError();
 }
 
@@ -772,17 +821,33 @@ __device__ __forceinline__ float sign_or_zero(float fwd) {
     return __int_as_float(__float_as_int(st) | (__float_as_int(fwd) & static_cast<int>(0x80000000u)));
 }
 
-// superbee_diff for a pair: with s = sign_or_zero(fwd), b = s back and
-// |fwd| = s fwd (both exact), and the slope is s m; below eps s = 0 makes
-// b = |fwd| = 0 and so m = 0.
-__device__ __forceinline__ float2 superbee_diff2(float2 back, float2 fwd) {
-    const float2 s = make_float2(sign_or_zero(fwd.x), sign_or_zero(fwd.y));
-    const float2 b = __fmul2_rn(back, s), af = __fmul2_rn(fwd, s);
-    const float2 b2 = __fadd2_rn(b, b), af2 = __fadd2_rn(af, af);
+// min(|x|, |y|) carrying the sign bit sign(x) xor sign(y): negative exactly
+// when x and y have opposite signs.
+__device__ __forceinline__ float min_xorsign_abs(float x, float y) {
+    float d;
+    asm("min.xorsign.abs.f32 %0, %1, %2;" : "=f"(d) : "f"(x), "f"(y));
+    return d;
+}
+
+// max(x, y, z) in one instruction (sm_100).
+__device__ __forceinline__ float max3f(float x, float y, float z) {
+    float d;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(x), "f"(y), "f"(z));
+    return d;
+}
+
+// superbee_diff for a pair, from the two differences around the face and
+// their doubles (2 back is the previous face's 2 fwd, so each double is
+// formed once).  With b = sgn(fwd) back: min_xorsign_abs(2 back, fwd) is
+// min(2b, |fwd|) when back and fwd share a sign and negative otherwise (so is
+// min(2b, |fwd|) then, b being negative), and likewise min(back, 2 fwd) ~
+// min(b, 2|fwd|); m = max(0, both) is the scalar form's m value for value.
+// The slope is sign_or_zero(fwd) m: sgn(fwd) m, and 0 below eps.
+__device__ __forceinline__ float2 superbee_diff2(float2 back, float2 back2, float2 fwd, float2 fwd2) {
     float2 m;
-    m.x = fmaxf(0.f, fmaxf(fminf(b2.x, af.x), fminf(b.x, af2.x)));
-    m.y = fmaxf(0.f, fmaxf(fminf(b2.y, af.y), fminf(b.y, af2.y)));
-    return __fmul2_rn(m, s);
+    m.x = max3f(0.f, min_xorsign_abs(back2.x, fwd.x), min_xorsign_abs(back.x, fwd2.x));
+    m.y = max3f(0.f, min_xorsign_abs(back2.y, fwd.y), min_xorsign_abs(back.y, fwd2.y));
+    return __fmul2_rn(m, make_float2(sign_or_zero(fwd.x), sign_or_zero(fwd.y)));
 }
 
 template <int N, int S, int SY, bool HY, typename Emit>
@@ -796,6 +861,7 @@ __device__ __forceinline__ void walk_plane_line2(const float2* X, const float2* 
         for (int k = 1; k <= N && k <= kPrefetch; ++k) y[k] = Y[k * SY];
     }
     float2 fwd = sub2(x[1], x[0]);
+    float2 fwd2 = __fadd2_rn(fwd, fwd);
     float2 gp = x[0];
 #pragma unroll
     for (int j = 1; j < N; ++j) {
@@ -803,9 +869,10 @@ __device__ __forceinline__ void walk_plane_line2(const float2* X, const float2* 
         if constexpr (HY) {
             if (j + kPrefetch <= N) y[j + kPrefetch] = Y[(j + kPrefetch) * SY];
         }
-        const float2 back = fwd;
+        const float2 back = fwd, back2 = fwd2;
         fwd = sub2(x[j + 1], x[j]);
-        const float2 g = __ffma2_rn(h, superbee_diff2(back, fwd), x[j]);
+        fwd2 = __fadd2_rn(fwd, fwd);
+        const float2 g = __ffma2_rn(h, superbee_diff2(back, back2, fwd, fwd2), x[j]);
         emit(j, __fmul2_rn(wr, sub2(g, gp)), x[j], x[j - 1], HY ? y[j] : make_float2(0.f, 0.f));
         gp = g;
     }
@@ -817,14 +884,13 @@ __device__ __forceinline__ float2 max_lo2(float2 v, float lo) { return make_floa
 
 
 template <int NP, int AC>
-__global__ void __launch_bounds__((NP * AC / 2 + 31) / 32 * 32) transport_plane_f2_kernel(TransportArgs<float> a,
-                                                                                           int n_chunks) {
+__device__ __forceinline__ void transport_plane_f2_body(const TransportArgs<float>& a, int n_chunks, int bid) {
     constexpr int N = NP - 1, RP = NP | 1, A2 = AC / 2, RS = RP * A2, PL = NP * RS;  // in float2
     constexpr int NT = (NP * A2 + 31) / 32 * 32;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float2* Fs = reinterpret_cast<float2*>(smem_raw);
     float2* Ps = Fs + PL;
-    const int chunk = blockIdx.x % n_chunks, ek = blockIdx.x / n_chunks;
+    const int chunk = bid % n_chunks, ek = bid / n_chunks;
     const int NA = a.NA, a0 = chunk * AC;
     const size_t plane = static_cast<size_t>(ek) * NP * NP * NA + a0;
     const float* __restrict__ in = a.in + plane;
@@ -921,6 +987,20 @@ __global__ void __launch_bounds__((NP * AC / 2 + 31) / 32 * 32) transport_plane_
     }
 }
 
+template <int NP, int AC>
+__global__ void __launch_bounds__((NP * AC / 2 + 31) / 32 * 32) transport_plane_f2_kernel(TransportArgs<float> a,
+                                                                                           int n_chunks) {
+    transport_plane_f2_body<NP, AC>(a, n_chunks, blockIdx.x);
+}
+
+template <int NP, int AC>
+__global__ void __launch_bounds__((NP * AC / 2 + 31) / 32 * 32)
+    transport_plane_f2_slots_kernel(const TransportArgs<float>* __restrict__ args, const int* __restrict__ begin,
+                                    int nslots, int n_chunks) {
+    const int s = find_slot(begin, nslots, blockIdx.x);
+    transport_plane_f2_body<NP, AC>(args[s], n_chunks, blockIdx.x - __ldg(begin + s));
+}
+
 // ---------------------------------------------------------------------------
 // Planes too large for one block (float state, paired angles): a cluster of
 // CL CTAs holds one (group, 2*A2-angle chunk) plane, CTA r the z rows
@@ -960,13 +1040,16 @@ __device__ __forceinline__ void walk_get2(const Get& get, float2 wr, float2 h, c
     for (int k = 0; k < L && k < kPrefetch + 3; ++k) x[k] = get(k);
     float2 back = sub2(x[1], x[0]);
     float2 fwd = sub2(x[2], x[1]);
-    float2 gp = __ffma2_rn(h, superbee_diff2(back, fwd), x[1]);  // G(first - 1)
+    float2 back2 = __fadd2_rn(back, back), fwd2 = __fadd2_rn(fwd, fwd);
+    float2 gp = __ffma2_rn(h, superbee_diff2(back, back2, fwd, fwd2), x[1]);  // G(first - 1)
 #pragma unroll
     for (int i = 0; i + 4 <= L; ++i) {
         if (i + 3 + kPrefetch < L) x[i + 3 + kPrefetch] = get(i + 3 + kPrefetch);
         back = fwd;
+        back2 = fwd2;
         fwd = sub2(x[i + 3], x[i + 2]);
-        const float2 g = __ffma2_rn(h, superbee_diff2(back, fwd), x[i + 2]);
+        fwd2 = __fadd2_rn(fwd, fwd);
+        const float2 g = __ffma2_rn(h, superbee_diff2(back, back2, fwd, fwd2), x[i + 2]);
         emit(i, __fmul2_rn(wr, sub2(g, gp)), x[i + 1], x[i + 2]);
         gp = g;
     }
@@ -1009,8 +1092,7 @@ __device__ __forceinline__ void walk_band_column(const float2* Xb, int B, const 
 }
 
 template <int NP, int CL, int A2>
-__global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(ClusterPlane<NP, CL, A2>::NT)
-    transport_cluster_kernel(TransportArgs<float> a, int n_chunks) {
+__device__ __forceinline__ void transport_cluster_body(const TransportArgs<float>& a, int n_chunks, int bid) {
     using S = ClusterPlane<NP, CL, A2>;
     constexpr int N = S::N, BZ = S::BZ, RS = S::RS, AC = 2 * A2;
     namespace cg = cooperative_groups;
@@ -1019,7 +1101,7 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(ClusterPlane<NP, CL
     float2* Fs = reinterpret_cast<float2*>(smem_raw);
     float2* Ps = Fs + BZ * RS;
     const int rank = static_cast<int>(cluster.block_rank());
-    const int plane_id = blockIdx.x / CL;
+    const int plane_id = bid / CL;
     const int chunk = plane_id % n_chunks, ek = plane_id / n_chunks;
     const int z0 = rank * NP / CL, z1 = (rank + 1) * NP / CL, B = z1 - z0;
     const int NA = a.NA, a0 = chunk * AC;
@@ -1151,6 +1233,265 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(ClusterPlane<NP, CL
         walk_band_column<BZ, RS>(Ps + off, B, pb, pa, wrz, hz, sz, emit);
     }
     cluster.sync();  // no CTA leaves while a neighbour still reads its rows
+}
+
+template <int NP, int CL, int A2>
+__global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(ClusterPlane<NP, CL, A2>::NT)
+    transport_cluster_kernel(TransportArgs<float> a, int n_chunks) {
+    transport_cluster_body<NP, CL, A2>(a, n_chunks, blockIdx.x);
+}
+
+// Slot boundaries fall on cluster boundaries (every slot's grid is a
+// multiple of CL), so all CTAs of a cluster serve one slot.
+template <int NP, int CL, int A2>
+__global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(ClusterPlane<NP, CL, A2>::NT)
+    transport_cluster_slots_kernel(const TransportArgs<float>* __restrict__ args, const int* __restrict__ begin,
+                                   int nslots, int n_chunks) {
+    const int s = find_slot(begin, nslots, blockIdx.x);
+    transport_cluster_body<NP, CL, A2>(args[s], n_chunks, blockIdx.x - __ldg(begin + s));
+}
+
+// ---------------------------------------------------------------------------
+// Row-streaming transport (float state, paired angles), any plane with
+// Ny + 1 <= 128: one block per (group, 8-angle chunk) plane walks the z rows
+// once.  Thread (y, q) owns column y for angle pair q and keeps its z-stencil
+// in registers -- the last three rows of F, of the predictor P and of H, and
+// the face values G of the z-walk -- so the z-parts of both stages are line
+// walks with one limiter per cell and no memory traffic.  The y-parts need
+// the whole row: row i of F (staged by cp.async a few rows ahead into a ring)
+// and row i-2 of P sit in shared memory; each thread forms the y face value
+// at its own cell from its two neighbours, publishes it, and takes the
+// neighbour's after the barrier.  Iteration i runs stage 1 (predictor P and
+// H = F - dt/2 div F) on row i and stage 2 (H - dt/2 div P, clipped) on row
+// i-2, whose z-stencil needs P up to row i.  Two barriers per row, no halo
+// recomputed, no cluster; the per-cell arithmetic and its order are those of
+// the whole-plane kernel, so the states agree with it value for value.
+// Rows and columns beyond the plane repeat the edge value, as the
+// reference's clamped indices do.
+// ---------------------------------------------------------------------------
+constexpr int kStreamPairs = 4;            // angle pairs per block (8 angles, 32 bytes per position)
+constexpr int kStreamRing = 8;             // rows of F in the shared-memory ring
+constexpr int kStreamAhead = 4;            // rows copied ahead of the one a row's z-stencil needs
+constexpr int kStreamPRows = 4;            // rows of P kept in shared memory (rows i-2 .. i)
+constexpr int kStreamMaxThreads = 512;     // planes up to 128 points wide (80 registers: 2 blocks of 352 per SM at 81)
+
+size_t transport_stream_smem(int NPy) {
+    const size_t row = static_cast<size_t>(NPy) * kStreamPairs * sizeof(float2);
+    const size_t grow = static_cast<size_t>(NPy + 2) * kStreamPairs * sizeof(float2);
+    return (kStreamRing + kStreamPRows) * row + 2 * grow;
+}
+
+__device__ __forceinline__ void transport_stream_body(const TransportArgs<float>& a, int n_chunks, int bid) {
+    constexpr int A2 = kStreamPairs, AC = 2 * A2, RF = kStreamRing, PD = kStreamAhead, RP = kStreamPRows;
+    static_assert((RF & (RF - 1)) == 0 && (RP & (RP - 1)) == 0 && AC == 8, "ring sizes are powers of two");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int Ny = a.Ny, Nz = a.Nz, NPy = Ny + 1, NA = a.NA;
+    const int RS = NPy * A2;  // one row, in float2
+    float2* Fr = reinterpret_cast<float2*>(smem_raw);  // [RF][NPy][A2]
+    float2* Pr = Fr + RF * RS;                         // [RP][NPy][A2]
+    float2* GF = Pr + RP * RS;                         // [NPy + 2][A2]: G of F's y-walk, faces -1 .. N+1
+    float2* GP = GF + (NPy + 2) * A2;                  // same for P
+    const int chunk = bid % n_chunks, ek = bid / n_chunks, a0 = chunk * AC;
+    const size_t zs = static_cast<size_t>(NPy) * NA;  // one z row in the state
+    const size_t base = static_cast<size_t>(ek) * (Nz + 1) * zs + a0;
+    const int tid = threadIdx.x, q = tid % A2, y = tid / A2;
+    const bool act = y < NPy;
+
+    // this thread's 16-byte piece of every row: threads 0 .. 2 NPy - 1 copy position tid / 2, half tid % 2
+    const bool vec = NA % 4 == 0;
+    const bool loader = vec && tid < 2 * NPy;
+    const bool lok = loader && a0 + 4 * (tid & 1) < NA;
+    const float* lsrc = a.in + base + static_cast<size_t>(tid >> 1) * NA + 4 * (tid & 1);
+    float* ldst = reinterpret_cast<float*>(Fr) + (tid >> 1) * AC + 4 * (tid & 1);
+    auto fill = [&](int r) {  // row r of F into slot r % RF; one commit group per call, empty past the plane
+        if (r <= Nz) {
+            float* dst = ldst + (r & (RF - 1)) * (2 * RS);
+            if (loader) cp_async16(dst, lok ? lsrc + static_cast<size_t>(r) * zs : a.in, lok);
+            if (!vec) {
+                float* row = reinterpret_cast<float*>(Fr + (r & (RF - 1)) * RS);
+                const float* src = a.in + base + static_cast<size_t>(r) * zs;
+                for (int v = tid; v < NPy * AC; v += blockDim.x) {
+                    const int e = v % AC, p = v / AC;
+                    row[p * AC + e] = (a0 + e < NA) ? src[static_cast<size_t>(p) * NA + e] : 0.f;
+                }
+            }
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+
+    const bool ok0 = act && a0 + 2 * q < NA, ok1 = act && a0 + 2 * q + 1 < NA;  // output stores
+    const int g0 = min(a0 + 2 * q, NA - 1), g1 = min(a0 + 2 * q + 1, NA - 1);
+    const float wy0 = a.omega[2 * g0], wz0 = a.omega[2 * g0 + 1];
+    const float wy1 = a.omega[2 * g1], wz1 = a.omega[2 * g1 + 1];
+    const float2 wry = make_float2(wy0 / a.dy, wy1 / a.dy), wrz = make_float2(wz0 / a.dz, wz1 / a.dz);
+    const bool dny = wy0 < 0.f, dnz = wz0 < 0.f;
+    const float2 hy = dny ? make_float2(-0.5f, -0.5f) : make_float2(0.5f, 0.5f);
+    const float2 hz = dnz ? make_float2(-0.5f, -0.5f) : make_float2(0.5f, 0.5f);
+    const float2 ndt = make_float2(-a.dt, -a.dt), nhdt = make_float2(-0.5f * a.dt, -0.5f * a.dt);
+    const float lo = a.preserve_sign ? -INFINITY : 0.f;
+    const int yc = act ? y : 0;
+    const int own = yc * A2 + q;
+    const int offl = max(yc - 1, 0) * A2 + q, offr = min(yc + 1, Ny) * A2 + q;
+    // G index of the two faces of this cell's y-divergence (G is stored one face up)
+    const int ghi = own + (dny ? 2 * A2 : A2), glo = own + (dny ? A2 : 0);
+    const int gedge = yc == 0 ? q : (yc == Ny ? (NPy + 1) * A2 + q : -1);  // face beyond the plane
+    float* orow = a.out + base + static_cast<size_t>(yc) * NA + 2 * q;   // output row 0
+
+    // Threads past the plane (the last warp's padding) compute on row position
+    // yc = 0 like thread 0 but publish and store nothing.
+    auto y_face = [&](float2* G, const float2* row, float2 x) {
+        const float2 back = sub2(x, row[offl]), fwd = sub2(row[offr], x);
+        const float2 g = __ffma2_rn(hy, superbee_diff2(back, __fadd2_rn(back, back), fwd, __fadd2_rn(fwd, fwd)), x);
+        if (act) {
+            G[own + A2] = g;
+            if (gedge >= 0) G[gedge] = x;  // the faces beyond the plane equal the edge value
+        }
+    };
+
+    // registers: F rows i .. i+2, P rows j .. j+2 and H rows j .. i (j = i - 2), z faces
+    float2 f0, f1, f2, p0{}, p1{}, p2{}, h0{}, h1{}, h2{};
+    float2 gz_m{}, gz_0{}, zfwd{}, zfwd2{};   // z-walk of F: G(i-1), G(i), last difference
+    float2 pz_m{}, pz_0{}, pfwd{}, pfwd2{};   // z-walk of P: G(j-1), G(j)
+    int slot = 0, pslot = 0;                  // ring slots of row i of F and of P
+
+    // phase A of iteration i: the y faces of row i of F (stage 1) and of row j
+    // of P (stage 2); f2 = F(min(i+2, Nz)) (row Nz stays in its slot: nothing is
+    // copied past the plane)
+    auto phase_a = [&](int i, bool st1, bool st2) {
+        f2 = Fr[((slot + min(2, Nz - i)) & (RF - 1)) * RS + own];
+        if (st1) y_face(GF, Fr + slot * RS, f0);
+        if (st2) y_face(GP, Pr + ((pslot - 2) & (RP - 1)) * RS, p0);
+    };
+    // phase B, stage 1 on row i: z face i+1, predictor P(i) (also to shared
+    // memory for the y faces two rows on) and H(i)
+    auto stage1 = [&]() {
+        const float2 back = zfwd, back2 = zfwd2;
+        zfwd = sub2(f2, f1);
+        zfwd2 = __fadd2_rn(zfwd, zfwd);
+        const float2 gz_p = __ffma2_rn(hz, superbee_diff2(back, back2, zfwd, zfwd2), f1);
+        const float2 dz = __fmul2_rn(wrz, dnz ? sub2(gz_p, gz_0) : sub2(gz_0, gz_m));
+        gz_m = gz_0;
+        gz_0 = gz_p;
+        const float2 d = __fadd2_rn(__fmul2_rn(wry, sub2(GF[ghi], GF[glo])), dz);
+        p2 = max_lo2(__ffma2_rn(ndt, d, f0), lo);
+        h2 = __ffma2_rn(nhdt, d, f0);
+        if (act) Pr[pslot * RS + own] = p2;
+    };
+    // phase B, stage 2 on row j: z face j+1 from P rows j .. j+2, the output row
+    auto stage2 = [&]() {
+        const float2 back = pfwd, back2 = pfwd2;
+        pfwd = sub2(p2, p1);
+        pfwd2 = __fadd2_rn(pfwd, pfwd);
+        const float2 gp_p = __ffma2_rn(hz, superbee_diff2(back, back2, pfwd, pfwd2), p1);
+        const float2 dzp = __fmul2_rn(wrz, dnz ? sub2(gp_p, pz_0) : sub2(pz_0, pz_m));
+        pz_m = pz_0;
+        pz_0 = gp_p;
+        const float2 t = __ffma2_rn(nhdt, __fmul2_rn(wry, sub2(GP[ghi], GP[glo])), h0);
+        const float2 v = max_lo2(__ffma2_rn(nhdt, dzp, t), lo);
+        if (ok1) *reinterpret_cast<float2*>(orow) = v;
+        else if (ok0) *orow = v.x;
+        orow += zs;
+    };
+    auto slide = [&]() {  // P rows j+1 .. i, H rows i-1 .. i, F rows i+1 .. i+2
+        p0 = p1;
+        p1 = p2;
+        h0 = h1;
+        h1 = h2;
+        f0 = f1;
+        f1 = f2;
+        slot = (slot + 1) & (RF - 1);
+        pslot = (pslot + 1) & (RP - 1);
+    };
+    auto top = [&]() {
+        asm volatile("cp.async.wait_group %0;" ::"n"(PD - 1) : "memory");
+        __syncthreads();  // row i+2 of F, row i-1 of P and last iteration's face reads are done
+    };
+
+    for (int r = 0; r < PD + 2; ++r) fill(r);
+    // rows 0 and 1: stage 1 only
+    top();
+    f0 = Fr[own];
+    f1 = Fr[(min(1, Nz) & (RF - 1)) * RS + own];
+    gz_m = gz_0 = f0;  // faces -1 and 0 of a clamped column: the edge value
+    zfwd = sub2(f1, f0);
+    zfwd2 = __fadd2_rn(zfwd, zfwd);
+    for (int i = 0; i < 2; ++i) {
+        if (i > 0) top();
+        phase_a(i, i <= Nz, false);
+        __syncthreads();  // faces published; row i of F is free for the copy of row i+PD+2
+        fill(i + PD + 2);
+        if (i <= Nz) stage1();
+        else p2 = p1;
+        slide();
+    }
+    pz_m = pz_0 = p0;  // P rows 0 and 1 known: start the z-walk of P
+    pfwd = sub2(p1, p0);
+    pfwd2 = __fadd2_rn(pfwd, pfwd);
+    // rows 2 .. Nz: both stages
+#pragma unroll 2
+    for (int i = 2; i <= Nz; ++i) {
+        top();
+        phase_a(i, true, true);
+        __syncthreads();
+        fill(i + PD + 2);
+        stage1();
+        stage2();
+        slide();
+    }
+    // rows past the plane: stage 2 only
+    for (int i = max(Nz + 1, 2); i <= Nz + 2; ++i) {
+        top();
+        phase_a(i, false, true);
+        __syncthreads();
+        p2 = p1;  // rows past the plane repeat the last predictor row
+        stage2();
+        slide();
+    }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
+
+__global__ void __maxnreg__(80) transport_stream_kernel(TransportArgs<float> a, int n_chunks) {
+    transport_stream_body(a, n_chunks, blockIdx.x);
+}
+
+__global__ void __maxnreg__(80) transport_stream_slots_kernel(const TransportArgs<float>* __restrict__ args,
+                                                                      const int* __restrict__ begin, int nslots,
+                                                                      int n_chunks) {
+    const int s = find_slot(begin, nslots, blockIdx.x);
+    transport_stream_body(args[s], n_chunks, blockIdx.x - __ldg(begin + s));
+}
+
+int transport_stream_threads(int Ny) { return ((Ny + 1) * kStreamPairs + 31) / 32 * 32; }
+
+bool transport_stream_supported(int Ny, int NA) {
+    return NA % 2 == 0 && transport_stream_threads(Ny) <= kStreamMaxThreads &&
+           transport_stream_smem(Ny + 1) <= 200 * 1024;
+}
+
+cudaError_t launch_transport_stream(const TransportArgs<float>& a, cudaStream_t s) {
+    if (!a.pairs || !transport_stream_supported(a.Ny, a.NA)) return cudaErrorNotSupported;
+    const int n_chunks = (a.NA + 2 * kStreamPairs - 1) / (2 * kStreamPairs);
+    const size_t smem = transport_stream_smem(a.Ny + 1);
+    cudaError_t e = cudaFuncSetAttribute(transport_stream_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    const long long blocks = static_cast<long long>(a.Ng) * n_chunks;
+    if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+    transport_stream_kernel<<<static_cast<unsigned>(blocks), transport_stream_threads(a.Ny), smem, s>>>(a, n_chunks);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_transport_stream_slots(const TransportArgs<float>* args, const int* begin, int nslots, int blocks,
+                                          int Ny, int NA, cudaStream_t s) {
+    if (nslots <= 0 || blocks <= 0) return cudaSuccess;
+    if (!transport_stream_supported(Ny, NA)) return cudaErrorNotSupported;
+    const int n_chunks = (NA + 2 * kStreamPairs - 1) / (2 * kStreamPairs);
+    const size_t smem = transport_stream_smem(Ny + 1);
+    cudaError_t e = cudaFuncSetAttribute(transport_stream_slots_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    transport_stream_slots_kernel<<<blocks, transport_stream_threads(Ny), smem, s>>>(args, begin, nslots, n_chunks);
+    return cudaGetLastError();
 }
 
 // The packed kernel applies when NA is even (8-byte aligned pairs) and the
@@ -1446,6 +1787,68 @@ cudaError_t launch_transport_plane(const TransportArgs<T>& a, int ang_chunk, cud
         if (ang_chunk == 8) return launch_plane_ac<T, 8>(a, s);
     }
     return cudaErrorInvalidValue;
+}
+
+// ---- multi-slot transport --------------------------------------------------
+template <int NP, int AC>
+static cudaError_t launch_plane_f2_slots(const TransportArgs<float>* args, const int* begin, int nslots, int blocks,
+                                         int NA, cudaStream_t s) {
+    const int n_chunks = (NA + AC - 1) / AC;
+    const size_t smem = transport_plane_smem(NP, AC, sizeof(float));
+    auto kern = transport_plane_f2_slots_kernel<NP, AC>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    kern<<<blocks, (NP * AC / 2 + 31) / 32 * 32, smem, s>>>(args, begin, nslots, n_chunks);
+    return cudaGetLastError();
+}
+
+template <int NP, int CL>
+static cudaError_t launch_cluster_slots(const TransportArgs<float>* args, const int* begin, int nslots, int blocks,
+                                        int NA, cudaStream_t s) {
+    constexpr int A2 = 4, AC = 2 * A2;
+    using S = ClusterPlane<NP, CL, A2>;
+    if (blocks % CL != 0) return cudaErrorInvalidValue;
+    const int n_chunks = (NA + AC - 1) / AC;
+    auto kern = transport_cluster_slots_kernel<NP, CL, A2>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::smem));
+    if (e != cudaSuccess) return e;
+    kern<<<blocks, S::NT, S::smem, s>>>(args, begin, nslots, n_chunks);
+    return cudaGetLastError();
+}
+
+int transport_cluster_size(int NP) {
+    switch (NP) {
+#define BFPN_CASE(P, CL) \
+    case P: return CL;
+        BFPN_CLUSTER_PLANES(BFPN_CASE)
+#undef BFPN_CASE
+        default: return 0;
+    }
+}
+
+cudaError_t launch_transport_slots(const TransportArgs<float>* args, const int* begin, int nslots, int blocks,
+                                   int NP, int NA, int ang_chunk, bool cluster, cudaStream_t s) {
+    if (nslots <= 0 || blocks <= 0) return cudaSuccess;
+    if (NA % 2 != 0) return cudaErrorNotSupported;
+    if (cluster) {
+        switch (NP) {
+#define BFPN_CASE(P, CL) \
+    case P: return launch_cluster_slots<P, CL>(args, begin, nslots, blocks, NA, s);
+            BFPN_CLUSTER_PLANES(BFPN_CASE)
+#undef BFPN_CASE
+            default: return cudaErrorNotSupported;
+        }
+    }
+    switch (NP) {
+#define BFPN_CASE(P)                                                                            \
+    case P:                                                                                     \
+        if (ang_chunk == 8) return launch_plane_f2_slots<P, 8>(args, begin, nslots, blocks, NA, s); \
+        if (ang_chunk == 16) return launch_plane_f2_slots<P, 16>(args, begin, nslots, blocks, NA, s); \
+        return cudaErrorInvalidValue;
+        BFPN_PLANE_SIZES(BFPN_CASE)
+#undef BFPN_CASE
+        default: return cudaErrorNotSupported;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1812,27 +2215,62 @@ __device__ __forceinline__ void dst1_pair(const float (&c)[(N + 1) / 2], const f
 // The pipelined DST for float state with two lines per thread: rows r and
 // r + R/2 of a tile's R rows, then adjacent columns (mu, mu + 1) of a slice
 // (N even).  128 threads per block, 2 * 128 / N slices per tile.
-template <int N, int NST>
-__global__ void __launch_bounds__(128) angle_dst_pair_kernel(AngleArgs<float> a, SineTable<N, float> S,
-                                                             long long n_tiles) {
+// Where work tile t lies: its slices in the state (F), their count, the
+// first slice's index within its beam (for the group of each slice) and the
+// beam's factor table and positions per group.
+struct DstTile {
+    float* F;
+    int ns;
+    long long slice0;
+    const float* fac;
+    int nyz;
+};
+
+// Tiles of one beam: SL consecutive slices each.
+struct DstTilesOne {
+    const AngleArgs<float>& a;
+    int SL;
+    __device__ DstTile operator()(long long t) const {
+        const long long total = static_cast<long long>(a.Ng) * a.nyz;
+        const int ns = static_cast<int>(min(static_cast<long long>(SL), total - t * SL));
+        return DstTile{a.F + t * SL * a.Nom * a.Nmu, ns, t * SL, a.fac, a.nyz};
+    }
+};
+
+// Tiles of the slots of a bundle: slot s owns tiles [tile_begin[s], tile_begin[s+1]).
+struct DstTilesSlots {
+    const AngleArgs<float>* args;
+    const int* tile_begin;
+    int nslots, SL;
+    __device__ DstTile operator()(long long t) const {
+        const int s = find_slot(tile_begin, nslots, t);
+        const AngleArgs<float>& a = args[s];
+        const long long lt = t - __ldg(tile_begin + s);
+        const long long total = static_cast<long long>(a.Ng) * a.nyz;
+        const int ns = static_cast<int>(min(static_cast<long long>(SL), total - lt * SL));
+        return DstTile{a.F + lt * SL * a.Nom * a.Nmu, ns, lt * SL, a.fac, a.nyz};
+    }
+};
+
+template <int N, int NST, typename Tiles>
+__device__ __forceinline__ void angle_dst_pair_body(const Tiles& tiles, const SineTable<N, float>& S, int SL,
+                                                    long long n_tiles, int* err) {
     static_assert(N % 2 == 0, "column pairs need an even N");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t full[NST];
     __shared__ int go;
     constexpr int NA = N * N, NH = N / 2;
-    const int SL = a.slices_per_block, tid = threadIdx.x;
+    const int tid = threadIdx.x;
     const uint32_t stage_bytes = (static_cast<uint32_t>(SL) * NA * 4u + 127u) / 128u * 128u;
-    const long long total = static_cast<long long>(a.Ng) * a.nyz;
     auto tile_of = [&](int i) { return static_cast<long long>(blockIdx.x) + static_cast<long long>(i) * gridDim.x; };
-    auto nslices = [&](long long t) { return static_cast<int>(min(static_cast<long long>(SL), total - t * SL)); };
     auto buf = [&](int st) { return reinterpret_cast<float*>(smem_raw + st * stage_bytes); };
     int issued[NST] = {}, landed[NST] = {};
     auto issue = [&](int i) {
-        const long long t = tile_of(i);
+        const DstTile d = tiles(tile_of(i));
         const int st = i % NST;
-        const uint32_t bytes = static_cast<uint32_t>(nslices(t)) * NA * 4u;
+        const uint32_t bytes = static_cast<uint32_t>(d.ns) * NA * 4u;
         mbar_expect_tx(&full[st], bytes);
-        bulk_copy_g2s(buf(st), a.F + t * SL * NA, bytes, &full[st]);
+        bulk_copy_g2s(buf(st), d.F, bytes, &full[st]);
         ++issued[st];
     };
     if (tid == 0) {
@@ -1894,7 +2332,8 @@ __global__ void __launch_bounds__(128) angle_dst_pair_kernel(AngleArgs<float> a,
         __syncthreads();
         if (!go) break;
         float* X = buf(st);
-        const int ns = nslices(t), half = ns * NH;  // row pairs = column pairs = ns * N / 2
+        const DstTile d = tiles(t);
+        const int ns = d.ns, half = ns * NH;  // row pairs = column pairs = ns * N / 2
         if (tid < half) {  // forward u on rows tid and tid + half
             load_rows(X + tid * N, X + (tid + half) * N);
             dst1_pair<N>(c, x, y);
@@ -1907,8 +2346,8 @@ __global__ void __launch_bounds__(128) angle_dst_pair_kernel(AngleArgs<float> a,
 #pragma unroll
             for (int k = 0; k < N; ++k) x[k] = C[k * NH];
             dst1_pair<N>(c, x, y);
-            const long long ek = (t * SL + sl) / a.nyz;
-            const float2* __restrict__ fac = reinterpret_cast<const float2*>(a.fac + ek * NA + mu);
+            const long long ek = (d.slice0 + sl) / d.nyz;
+            const float2* __restrict__ fac = reinterpret_cast<const float2*>(d.fac + ek * NA + mu);
 #pragma unroll
             for (int k = 0; k < N; ++k) y[k] = __fmul2_rn(y[k], __ldg(fac + k * NH));
             dst1_pair<N>(c, y, x);
@@ -1924,18 +2363,32 @@ __global__ void __launch_bounds__(128) angle_dst_pair_kernel(AngleArgs<float> a,
         __syncthreads();
         if (tid == 0) {
             fence_proxy_async_smem();
-            bulk_copy_s2g(a.F + t * SL * NA, X, static_cast<uint32_t>(ns) * NA * 4u);
+            bulk_copy_s2g(d.F, X, static_cast<uint32_t>(ns) * NA * 4u);
             bulk_commit();
         }
     }
     if (tid == 0) {
         if (!go) {
-            atomicExch(a.err, 3);
+            atomicExch(err, 3);
             for (int st = 0; st < NST; ++st)
                 if (issued[st] > landed[st]) mbar_wait(&full[st], (issued[st] - 1) & 1);
         }
         bulk_wait<0>();
     }
+}
+
+template <int N, int NST>
+__global__ void __launch_bounds__(128) angle_dst_pair_kernel(AngleArgs<float> a, SineTable<N, float> S,
+                                                             long long n_tiles) {
+    angle_dst_pair_body<N, NST>(DstTilesOne{a, a.slices_per_block}, S, a.slices_per_block, n_tiles, a.err);
+}
+
+// The slots' tiles in one persistent launch; the error word is slot 0's.
+template <int N, int NST>
+__global__ void __launch_bounds__(128) angle_dst_pair_slots_kernel(const AngleArgs<float>* __restrict__ args,
+                                                                   const int* __restrict__ tile_begin, int nslots,
+                                                                   SineTable<N, float> S, int SL, long long n_tiles) {
+    angle_dst_pair_body<N, NST>(DstTilesSlots{args, tile_begin, nslots, SL}, S, SL, n_tiles, args[0].err);
 }
 
 template <int N, typename T>
@@ -2016,6 +2469,46 @@ cudaError_t launch_angle(const AngleArgs<T>& a, cudaStream_t s) {
         }
     }
     return launch_angle_generic(a, s);
+}
+
+// ---- multi-slot DST ---------------------------------------------------------
+int angle_slots_tile(int N) { return 256 / N; }
+
+template <int N, int NST>
+static cudaError_t launch_angle_slots_n(const AngleArgs<float>* args, const int* tile_begin, int nslots,
+                                        long long tiles, cudaStream_t s) {
+    SineTable<N, float> S;
+    for (int k = 1; k <= (N + 1) / 2; ++k)
+        S.c[k - 1] = static_cast<float>(std::sin(3.14159265358979323846 * k / (N + 1)));
+    const int SL = angle_slots_tile(N);
+    const size_t stage = (static_cast<size_t>(SL) * N * N * 4 + 127) / 128 * 128;
+    auto pk = angle_dst_pair_slots_kernel<N, NST>;
+    cudaError_t e = cudaFuncSetAttribute(pk, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(NST * stage));
+    if (e != cudaSuccess) return e;
+    int dev = 0, sms = 0, per_sm = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pk, 128, NST * stage)) != cudaSuccess) return e;
+    const long long grid = std::min<long long>(tiles, static_cast<long long>(sms) * std::max(per_sm, 1));
+    pk<<<static_cast<unsigned>(grid), 128, NST * stage, s>>>(args, tile_begin, nslots, S, SL, tiles);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_angle_slots(const AngleArgs<float>* args, const int* tile_begin, int nslots, long long tiles,
+                               int N, int stages, cudaStream_t s) {
+    if (nslots <= 0 || tiles <= 0) return cudaSuccess;
+    if (stages != 2 && stages != 3) return cudaErrorInvalidValue;
+    switch (N) {
+#define BFPN_DST_SLOTS(n)                                                                   \
+    case n:                                                                                 \
+        return stages == 2 ? launch_angle_slots_n<n, 2>(args, tile_begin, nslots, tiles, s) \
+                           : launch_angle_slots_n<n, 3>(args, tile_begin, nslots, tiles, s);
+        BFPN_DST_SLOTS(4) BFPN_DST_SLOTS(6) BFPN_DST_SLOTS(8) BFPN_DST_SLOTS(10) BFPN_DST_SLOTS(12)
+        BFPN_DST_SLOTS(14) BFPN_DST_SLOTS(16) BFPN_DST_SLOTS(18) BFPN_DST_SLOTS(20) BFPN_DST_SLOTS(22)
+        BFPN_DST_SLOTS(24) BFPN_DST_SLOTS(28) BFPN_DST_SLOTS(32)
+#undef BFPN_DST_SLOTS
+        default: return cudaErrorNotSupported;
+    }
 }
 
 template <typename T>
@@ -2126,6 +2619,45 @@ __global__ void __launch_bounds__(1024) finalize_idd_kernel(const double* __rest
             if (advance) *counter = c + 1;
         }
     }
+}
+
+// One block per slot of a bundle: launch_finalize_idd's reduction with the slot's arguments.
+__global__ void __launch_bounds__(1024) finalize_idd_slots_kernel(const IddFinalArgs* __restrict__ args) {
+    const IddFinalArgs& f = args[blockIdx.x];
+    double a = 0.0, b = 0.0;
+    for (int i = threadIdx.x; i < f.n; i += blockDim.x) { a += f.p[2 * i]; b += f.p[2 * i + 1]; }
+    for (int i = threadIdx.x; i < f.n2; i += blockDim.x) a += f.p2[2 * i];
+    __shared__ double red[2][32];
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_down_sync(0xffffffffu, a, o);
+        b += __shfl_down_sync(0xffffffffu, b, o);
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) { red[0][w] = a; red[1][w] = b; }
+    __syncthreads();
+    if (w == 0) {
+        const int nw = blockDim.x >> 5;
+        a = (l < nw) ? red[0][l] : 0.0;
+        b = (l < nw) ? red[1][l] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_down_sync(0xffffffffu, a, o);
+            b += __shfl_down_sync(0xffffffffu, b, o);
+        }
+        if (l == 0) {
+            const int c = *f.counter;
+            if (c >= 0 && c < f.capacity) {
+                f.hist_idd[c] = a * f.idd_scale;
+                f.hist_proxy[c] = b * f.proxy_scale;
+            }
+            *f.counter = c + 1;
+        }
+    }
+}
+
+cudaError_t launch_finalize_idd_slots(const IddFinalArgs* args, int nslots, cudaStream_t s) {
+    if (nslots <= 0) return cudaSuccess;
+    finalize_idd_slots_kernel<<<nslots, 1024, 0, s>>>(args);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_finalize_idd(const double* partials, int n, const double* partials2, int n2, double idd_scale,

@@ -1,13 +1,24 @@
 // Multi-beam batching and serving on top of the single-beam C ABI.
 //
 // The reference runs one beam per process (main.cu:344-348).  A treatment plan
-// or a dose engine needs many independent beams, each small enough that one
-// beam rarely fills a B200: this layer keeps a thread-safe queue of beam
-// requests and serves it with worker threads, each owning one solver context
-// (its own stream and CUDA graph) on one device, so several beams run
-// concurrently per GPU and across GPUs.  A worker keeps its context between
-// requests of the same shape (grid, flags, precision) and only reloads the
-// tables and the beam; a request of another shape replaces the context.
+// or a dose engine needs many independent beams, most too small to fill a
+// B200 alone.  This layer keeps a thread-safe queue of beam requests and
+// serves it two ways:
+//
+// - continuous batching: requests that a bundle can hold (mixed precision,
+//   the eq15 step, square angular grids; bfpn_bundle_accepts) go to one
+//   scheduler thread per device.  It admits them FIFO into bundles by shape
+//   class -- each admission checks the beam's device footprint against the
+//   free memory first -- and advances every bundle a time slice of depth
+//   steps per round, the bundles of different classes on their own streams at
+//   once.  Beams that arrive while others run join at the next round; a
+//   finished beam's results are collected and its slot and memory freed at
+//   once.  Results equal the beam run alone up to the order of the IDD
+//   partial sums.
+// - worker threads for everything else, each owning one solver context (its
+//   own stream and CUDA graph) on one device, kept between requests of the
+//   same shape (grid, flags, precision) with only the tables and the beam
+//   reloaded; results equal a single-context run bit for bit.
 //
 // bfpn_server_submit copies the request's tables, so callers may free them at
 // once.  Results stay with the server until bfpn_server_wait collects them.
@@ -24,6 +35,7 @@
 #include <mutex>
 #include <string>
 #include <thread>
+#include <map>
 #include <unordered_map>
 #include <vector>
 
@@ -56,6 +68,7 @@ struct Job {
     std::string error;
     std::vector<double> idd, proxy;
     int32_t device = -1;
+    bool bundled = false;  // served by a bundle scheduler
     Clock::time_point submitted, started, finished;
 };
 
@@ -72,11 +85,15 @@ struct bfpn_server {
     std::mutex mu;
     std::condition_variable cv_work;  // workers: a job was queued, or shutdown
     std::condition_variable cv_done;  // waiters: a job finished
-    std::deque<std::shared_ptr<Job>> queue;
+    std::condition_variable cv_bundle;  // schedulers: a bundle job was queued, or shutdown
+    std::deque<std::shared_ptr<Job>> queue;         // jobs for the context workers
+    std::deque<std::shared_ptr<Job>> bundle_queue;  // jobs for the bundle schedulers
     std::unordered_map<uint64_t, std::shared_ptr<Job>> jobs;
     uint64_t next_ticket = 1;
     bool stopping = false;
+    bool batching = true;
     std::vector<std::thread> workers;
+    std::vector<std::thread> schedulers;
     std::vector<int> busy_per_device;  // indexed by position in `devices`
     std::vector<int32_t> devices;
 };
@@ -154,11 +171,160 @@ void worker_main(bfpn_server* s, int dev_slot) {
     if (ctx) bfpn_destroy(ctx);
 }
 
+// ---- continuous batching ----------------------------------------------------
+
+// Shape class of a bundle-eligible beam: kernels depend on the plane, the
+// angular grid, the energy model and the clipping of psi^1.
+std::string class_key(const Job& j) {
+    const uint32_t fl = j.phys.flags & (BFPN_FLAG_EQ15_STRAGGLING | BFPN_FLAG_NO_SPATIAL_CLIPPING);
+    return std::to_string(j.grid.Ny) + "x" + std::to_string(j.grid.Nz) + "/" + std::to_string(j.grid.Nmu) + "x" +
+           std::to_string(j.grid.Nom) + "/" + std::to_string(fl);
+}
+
+constexpr int kBundleSlots = 64;
+constexpr double kSliceMs = 40.0;  // target length of one round of bundle steps
+
+struct LiveBundle {
+    bfpn_bundle* b = nullptr;
+    std::map<int, std::shared_ptr<Job>> slots;  // running jobs by slot
+    double ms_per_step = 1.0;                     // running estimate (host clock, concurrent rounds)
+};
+
+void finish(bfpn_server* s, const std::shared_ptr<Job>& j, bfpn_status st, const std::string& err) {
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        j->status = st;
+        if (st != BFPN_OK) j->error = err;
+        j->finished = Clock::now();
+        j->done = true;
+    }
+    s->cv_done.notify_all();
+}
+
+void scheduler_main(bfpn_server* s, int dev_slot) {
+    const int32_t device = s->devices[dev_slot];
+    std::map<std::string, LiveBundle> live;
+    for (;;) {
+        bool any_running = false;
+        for (auto& kv : live) any_running = any_running || !kv.second.slots.empty();
+        // 1. admit queued jobs FIFO while they fit (a job that does not fit waits at the head)
+        for (;;) {
+            std::shared_ptr<Job> j;
+            {
+                std::unique_lock<std::mutex> lk(s->mu);
+                if (!any_running)
+                    s->cv_bundle.wait(lk, [&] { return s->stopping || !s->bundle_queue.empty(); });
+                if (s->bundle_queue.empty()) {
+                    if (s->stopping && !any_running) {
+                        lk.unlock();
+                        for (auto& kv : live) bfpn_bundle_destroy(kv.second.b);
+                        return;
+                    }
+                    break;
+                }
+                j = s->bundle_queue.front();
+                s->bundle_queue.pop_front();
+            }
+            LiveBundle& lb = live[class_key(*j)];
+            bfpn_status st = BFPN_OK;
+            if (!lb.b) st = bfpn_bundle_create(device, kBundleSlots, &lb.b);
+            int32_t slot = -1;
+            bfpn_beam beam{j->grid, j->phys, j->precision, j->nsteps, j->mu.data(), j->mu_rows, j->sigma.data(),
+                           j->sigma_rows};
+            if (st == BFPN_OK && static_cast<int>(lb.slots.size()) < kBundleSlots)
+                st = bfpn_bundle_admit(lb.b, &beam, &slot);
+            else if (st == BFPN_OK)
+                st = BFPN_OOM;  // every slot taken: wait like a beam that does not fit
+            if (st == BFPN_OK) {
+                {
+                    std::lock_guard<std::mutex> lk(s->mu);
+                    j->started = Clock::now();
+                    j->device = device;
+                }
+                lb.slots[slot] = j;
+                any_running = true;
+                continue;
+            }
+            if (st == BFPN_OOM && any_running) {  // wait for running beams to free memory
+                std::lock_guard<std::mutex> lk(s->mu);
+                s->bundle_queue.push_front(j);
+                break;
+            }
+            if (st == BFPN_INVALID_ARG) {  // a bundle cannot hold it after all: a context worker serves it
+                {
+                    std::lock_guard<std::mutex> lk(s->mu);
+                    j->bundled = false;
+                    s->queue.push_back(j);
+                }
+                s->cv_work.notify_one();
+                continue;
+            }
+            finish(s, j, st, std::string("bundle admit: ") + bfpn_bundle_last_error(lb.b));
+        }
+        if (!any_running) continue;
+        // 2. one round: every bundle with running beams advances a time slice, concurrently
+        const auto t0 = Clock::now();
+        std::vector<std::pair<LiveBundle*, int>> stepped;
+        for (auto& kv : live) {
+            LiveBundle& lb = kv.second;
+            if (lb.slots.empty()) continue;
+            const int n = std::max(1, std::min(512, static_cast<int>(kSliceMs / std::max(lb.ms_per_step, 1e-3))));
+            bfpn_status st = bfpn_bundle_step(lb.b, n);
+            if (st != BFPN_OK) {
+                const std::string err = std::string("bundle step: ") + bfpn_bundle_last_error(lb.b);
+                for (auto& sj : lb.slots) finish(s, sj.second, st, err);
+                lb.slots.clear();
+                bfpn_bundle_destroy(lb.b);
+                lb.b = nullptr;
+                continue;
+            }
+            stepped.emplace_back(&lb, n);
+        }
+        // 3. wait, then collect the finished beams
+        for (auto& [lb, n] : stepped) {
+            bfpn_status st = bfpn_bundle_sync(lb->b);
+            const double ms = ms_between(t0, Clock::now());
+            lb->ms_per_step = 0.5 * lb->ms_per_step + 0.5 * ms / n;
+            for (auto it = lb->slots.begin(); it != lb->slots.end();) {
+                int32_t done = 0, total = 0;
+                bfpn_bundle_slot(lb->b, it->first, &done, &total);
+                if (st == BFPN_OK && done < total) {
+                    ++it;
+                    continue;
+                }
+                std::shared_ptr<Job> j = it->second;
+                bfpn_status cs = st;
+                if (cs == BFPN_OK) {
+                    j->idd.assign(static_cast<size_t>(j->nsteps), 0.0);
+                    j->proxy.assign(static_cast<size_t>(j->nsteps), 0.0);
+                    cs = bfpn_bundle_collect(lb->b, it->first, j->idd.data(), j->proxy.data(), j->nsteps);
+                }
+                finish(s, j, cs, std::string("bundle: ") + bfpn_bundle_last_error(lb->b));
+                it = lb->slots.erase(it);
+            }
+            if (st != BFPN_OK) {  // the bundle's state is suspect: drop it
+                bfpn_bundle_destroy(lb->b);
+                lb->b = nullptr;
+            }
+        }
+        for (auto it = live.begin(); it != live.end();)
+            it = (it->second.b == nullptr) ? live.erase(it) : std::next(it);
+    }
+}
+
 }  // namespace
 
 extern "C" {
 
 const char* bfpn_server_last_error(void) { return g_server_error.c_str(); }
+
+bfpn_status bfpn_server_set_batching(bfpn_server* s, int32_t on) {
+    if (!s) return server_fail(BFPN_INVALID_ARG, "null server");
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->next_ticket != 1) return server_fail(BFPN_NOT_READY, "set batching before the first submit");
+    s->batching = on != 0;
+    return BFPN_OK;
+}
 
 bfpn_status bfpn_server_create(const int32_t* devices, int32_t n_devices, int32_t workers_per_device,
                                bfpn_server** out) {
@@ -175,8 +341,10 @@ bfpn_status bfpn_server_create(const int32_t* devices, int32_t n_devices, int32_
     auto* s = new bfpn_server();
     s->devices = devs;
     s->busy_per_device.assign(devs.size(), 0);
-    for (size_t k = 0; k < devs.size(); ++k)
+    for (size_t k = 0; k < devs.size(); ++k) {
         for (int w = 0; w < workers_per_device; ++w) s->workers.emplace_back(worker_main, s, static_cast<int>(k));
+        s->schedulers.emplace_back(scheduler_main, s, static_cast<int>(k));
+    }
     *out = s;
     return BFPN_OK;
 }
@@ -203,10 +371,12 @@ bfpn_status bfpn_server_submit(bfpn_server* s, const bfpn_beam* beam, uint64_t* 
         j->ticket = s->next_ticket++;
         j->submitted = Clock::now();
         s->jobs[j->ticket] = j;
-        s->queue.push_back(j);
+        j->bundled = s->batching && bfpn_bundle_accepts(beam) == BFPN_OK;
+        (j->bundled ? s->bundle_queue : s->queue).push_back(j);
         *ticket = j->ticket;
     }
-    s->cv_work.notify_one();
+    if (j->bundled) s->cv_bundle.notify_all();
+    else s->cv_work.notify_one();
     return BFPN_OK;
 }
 
@@ -256,7 +426,9 @@ bfpn_status bfpn_server_destroy(bfpn_server* s) {
         s->stopping = true;
     }
     s->cv_work.notify_all();
+    s->cv_bundle.notify_all();
     for (auto& t : s->workers) t.join();
+    for (auto& t : s->schedulers) t.join();
     delete s;
     return BFPN_OK;
 }

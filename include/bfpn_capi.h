@@ -282,7 +282,14 @@ int32_t bfpn_source_groups(bfpn_ctx* ctx);
  *   only; 0 runs everything one kernel after the other.  Applies when graphs
  *   are on and the transport is in place (whole-plane or cluster kernels);
  *   every bfpn_step / bfpn_step_async call still ends on whole steps.  Same
- *   kernels on the same inputs: the same values. */
+ *   kernels on the same inputs: the same values.
+ * BFPN_OPT_STREAM_TRANSPORT: 1 (default) runs the mixed-precision transport
+ *   of planes without a whole-plane kernel (Ny + 1 <= 128, any Nz, paired
+ *   angles) with the row-streaming kernel: one block per (group, 8-angle)
+ *   plane walks the z rows, the z-stencil in registers and one row of the
+ *   y-stencil in shared memory, in place; 2 also uses it where a whole-plane
+ *   kernel exists; 0 leaves those planes to the cluster / tiled kernels.
+ *   Same values as the whole-plane kernel. */
 enum {
     BFPN_OPT_TENSOR_CORES = 0,
     BFPN_OPT_CUDA_GRAPHS = 1,
@@ -291,7 +298,8 @@ enum {
     BFPN_OPT_CLUSTER_TRANSPORT = 4,
     BFPN_OPT_LANE_CHUNK = 5,
     BFPN_OPT_ENERGY_CHUNK = 6,
-    BFPN_OPT_STEP_OVERLAP = 7
+    BFPN_OPT_STEP_OVERLAP = 7,
+    BFPN_OPT_STREAM_TRANSPORT = 8
 };
 bfpn_status bfpn_set_option(bfpn_ctx* ctx, int32_t option, int32_t value);
 
@@ -324,12 +332,14 @@ bfpn_status bfpn_spot_plane(bfpn_ctx* ctx, double* plane);
 
 /* ---- multi-beam batching and serving ------------------------------------
  * The reference runs one beam per process (main.cu:344-348).  These calls
- * serve many independent beams: a thread-safe queue of requests worked by
- * threads that each own one context (stream + CUDA graph) on one device, so
- * several beams run at once per GPU and across GPUs.  A worker keeps its
- * context between requests of the same shape and only reloads tables and
- * beam.  Each beam's IDD / proxy history is the same as bfpn_step on a fresh
- * context would give. */
+ * serve many independent beams from a thread-safe queue.  Requests a bundle
+ * can hold are batched continuously (bfpn_server_set_batching); the others
+ * are worked by threads that each own one context (stream + CUDA graph) on
+ * one device, so several beams run at once per GPU and across GPUs; such a
+ * worker keeps its context between requests of the same shape and only
+ * reloads tables and beam.  A worker-served beam's IDD / proxy history is the
+ * one bfpn_step on a fresh context gives; a batched beam's equals it up to
+ * the order of the IDD partial sums. */
 typedef struct bfpn_beam {
     bfpn_grid grid;
     bfpn_phys phys;
@@ -354,6 +364,14 @@ typedef struct bfpn_server bfpn_server;
  * device 0). */
 bfpn_status bfpn_server_create(const int32_t* devices, int32_t n_devices, int32_t workers_per_device,
                                bfpn_server** out);
+/* Continuous batching (default on): requests a bundle can hold
+ * (bfpn_bundle_accepts) are served by one scheduler thread per device that
+ * admits them FIFO into bundles of their shape class, each admission checked
+ * against free device memory by the beam's footprint, and advances all
+ * bundles together in rounds of depth steps; beams join and leave between
+ * rounds.  Off: every request goes to the context workers.  Call before the
+ * first submit (BFPN_NOT_READY otherwise). */
+bfpn_status bfpn_server_set_batching(bfpn_server* server, int32_t on);
 /* Queue one beam; thread-safe.  *ticket identifies it for poll / wait. */
 bfpn_status bfpn_server_submit(bfpn_server* server, const bfpn_beam* beam, uint64_t* ticket);
 /* 1 finished (success or failure), 0 queued or running, -1 unknown ticket. */
@@ -373,6 +391,64 @@ const char* bfpn_server_last_error(void);
 bfpn_status bfpn_batch_run(const bfpn_beam* beams, int32_t n, const int32_t* devices, int32_t n_devices,
                            int32_t workers_per_device, double* const* idd_out, double* const* proxy_out,
                            bfpn_status* status_out);
+
+/* ---- bundles: beams of one shape class advanced together ---------------
+ * No counterpart in the reference, which runs one beam per process
+ * (main.cu:344-348).  A bundle holds up to max_slots mixed-precision beams
+ * whose kernels share one shape class -- the same Ny+1 = Nz+1 plane, square
+ * Nmu = Nom angular grid and energy model -- and advances all of them with
+ * one launch per operator per depth step: the energy sweep, the transport
+ * half-steps and the DST of both state arrays of every slot each run as a
+ * single kernel over a device table of per-slot arguments; each slot's
+ * secondary source runs on a parallel graph branch.  Slots keep their own Ng,
+ * tables, beam, depth-step count and IDD history, and join or leave at any
+ * step (continuous batching).  The step of the current slot set is one CUDA
+ * graph.  Kernel variants (angles per transport block, DST ring stages,
+ * energy kernel form) are timed per shape class on the bundle's first steps
+ * and the fastest kept for the process (autotuning); all variants compute the
+ * same states.  Each beam's IDD history equals its single-context run up to
+ * the order of the IDD partial sums. */
+typedef struct bfpn_bundle bfpn_bundle;
+
+enum {
+    BFPN_BUNDLE_OPT_AUTOTUNE = 1,          /* 1 (default) tune on first use, 0 use the defaults / settings below */
+    BFPN_BUNDLE_OPT_TRANSPORT_ANGLES = 2,  /* 8 or 16 angles per whole-plane transport block (turns tuning off) */
+    BFPN_BUNDLE_OPT_DST_STAGES = 3,        /* 2 or 3 DST ring stages (turns tuning off) */
+    BFPN_BUNDLE_OPT_ENERGY_RING = 4        /* 1 ring energy kernel, 0 register kernel (turns tuning off) */
+};
+
+/* BFPN_OK when a bundle can hold the beam (host-side check of its precision,
+ * flags and grid; bfpn_bundle_admit may still refuse it for memory), else
+ * BFPN_INVALID_ARG with the reason in bfpn_bundle_last_error(NULL). */
+bfpn_status bfpn_bundle_accepts(const bfpn_beam* beam);
+bfpn_status bfpn_bundle_create(int32_t device, int32_t max_slots, bfpn_bundle** out);
+bfpn_status bfpn_bundle_set_option(bfpn_bundle* bundle, int32_t option, int32_t value);
+/* Admit one beam (precision must be BFPN_PREC_MIXED): checks its footprint
+ * (bfpn_footprint_bytes) against the device's free memory less 512 MiB
+ * (BFPN_OOM when it does not fit, nothing allocated), builds its context
+ * (tables, initial beam) and gives it a free slot (*slot).  The first beam
+ * fixes the shape class; a beam of another class gets BFPN_INVALID_ARG. */
+bfpn_status bfpn_bundle_admit(bfpn_bundle* bundle, const bfpn_beam* beam, int32_t* slot);
+/* Enqueue up to nsteps depth steps of every slot that has steps left (each
+ * stops at its own nsteps) on the bundle's stream; returns without waiting. */
+bfpn_status bfpn_bundle_step(bfpn_bundle* bundle, int32_t nsteps);
+/* Wait for the enqueued steps; BFPN_TIMEOUT if a kernel's bounded wait ran out. */
+bfpn_status bfpn_bundle_sync(bfpn_bundle* bundle);
+/* Slots that still have steps to run. */
+int32_t bfpn_bundle_running(const bfpn_bundle* bundle);
+/* Steps enqueued so far and steps requested of a slot (-1 / 0 when empty). */
+bfpn_status bfpn_bundle_slot(const bfpn_bundle* bundle, int32_t slot, int32_t* steps_done, int32_t* nsteps);
+/* Copy a finished slot's IDD / proxy histories (capacity >= its nsteps; either
+ * may be NULL), then free the slot and its device memory. */
+bfpn_status bfpn_bundle_collect(bfpn_bundle* bundle, int32_t slot, double* idd, double* proxy, int32_t capacity);
+/* The tuning choice of the bundle's shape class as one line of text; returns
+ * its length, or -1. */
+int32_t bfpn_bundle_tuning(const bfpn_bundle* bundle, char* buf, int32_t buf_len);
+/* cudaStream_t of the bundle. */
+void* bfpn_bundle_stream(bfpn_bundle* bundle);
+bfpn_status bfpn_bundle_destroy(bfpn_bundle* bundle);
+/* Message of the bundle's last failure (NULL: the last failure on this thread). */
+const char* bfpn_bundle_last_error(const bfpn_bundle* bundle);
 
 /* ---- integrated depth dose without device allocation -------------------
  * No counterpart in the reference: its IDD (computeIntegratedDepthDose +

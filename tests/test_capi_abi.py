@@ -161,3 +161,14 @@ def test_streaming_and_lite_memory_are_exclusive():
     bad = dataclasses.replace(cfg, streaming_full=True)
     with pytest.raises(capi.BfpnError, match="mutually exclusive"):
         capi.Context(bad.grid(), bad.phys(), capi.PREC_FP64)
+
+
+def test_bundle_without_device_fails_cleanly():
+    """No GPU here: creating a bundle reports NO_DEVICE with a message."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    with pytest.raises(capi.BfpnError, match="no such device"):
+        capi.Bundle(device=0, max_slots=4)
+    with pytest.raises(capi.BfpnError, match="bad arguments"):
+        capi.Bundle(device=0, max_slots=0)

@@ -99,3 +99,52 @@ def test_batch_run_matches_direct_runs():
     for (cfg, prec, mu, sig, n, _), (idd, prox) in zip(reqs, out):
         d_idd, d_prox = direct(cfg, prec, mu, sig, n)
         assert np.array_equal(idd, d_idd) and np.array_equal(prox, d_prox)
+
+
+def _alone_mixed(r):
+    ctx = Context(r.cfg.grid(), r.cfg.phys(), capi.PREC_MIXED)
+    ctx.load_tables(r.mu, r.sigma)
+    ctx.init_beam()
+    idd, _ = ctx.step(r.nsteps)
+    ctx.close()
+    return idd
+
+
+def test_continuous_batching_solo_equals_mix():
+    """Bundle-eligible requests of three shape classes, submitted while
+    earlier ones run: every served IDD equals the beam run alone on a context
+    and the beam served alone, within 1e-6 of its peak."""
+    import time
+
+    from bfpn_gpu_b200 import beams
+
+    pool = [r for r in beams.uneven_beams(24, seed=5, ny_choices=(16, 24, 32), na_choices=(12, 16))][:7]
+    for r in pool:
+        r.nsteps = min(r.nsteps, 45)
+        assert capi.bundle_accepts(r.beam())
+    with capi.Server(workers_per_device=1) as srv:
+        tickets = []
+        for k, r in enumerate(pool):
+            tickets.append(srv.submit(r.beam()))
+            if k in (1, 4):
+                time.sleep(0.05)  # later requests arrive while the first run
+        mix = [srv.wait(t, r.nsteps) for t, r in zip(tickets, pool)]
+    with capi.Server(workers_per_device=1) as srv:
+        solo = srv.wait(srv.submit(pool[0].beam()), pool[0].nsteps)[0]
+    for r, (idd, _, info) in zip(pool, mix):
+        ref = _alone_mixed(r)
+        assert info["steps"] == r.nsteps
+        assert np.abs(idd - ref).max() <= 1e-6 * np.abs(ref).max()
+    assert np.abs(solo - mix[0][0]).max() <= 1e-6 * np.abs(solo).max()
+
+
+def test_batching_off_serves_bit_identical_results():
+    from bfpn_gpu_b200 import beams
+
+    r = beams.uneven_beams(4, seed=9, ny_choices=(16,), na_choices=(12,))[0]
+    r.nsteps = min(r.nsteps, 20)
+    with capi.Server(workers_per_device=1, batching=False) as srv:
+        idd = srv.wait(srv.submit(r.beam()), r.nsteps)[0]
+        with pytest.raises(capi.BfpnError):
+            srv.set_batching(True)  # only before the first submit
+    assert np.array_equal(idd, _alone_mixed(r))
