@@ -458,68 +458,127 @@ def run_reference(args):
     print(json.dumps(out), flush=True)
 
 
-def run_serve(args):
-    """Batched and served uneven beams against the plain one-beam-at-a-time
-    path: beams/s of each, the speed-up, latency percentiles of a Poisson
-    request stream, and every served IDD against the same beam run alone."""
-    import torch  # noqa: F401  (CUDA context for the device query)
-    from bfpn_gpu_b200 import Context, capi, beams
+def _plain_run(r):
+    """One beam through a fresh single context: create, tables, beam, all
+    steps, IDD history to the host."""
+    from bfpn_gpu_b200 import Context
+    ctx = Context(r.cfg.grid(), r.cfg.phys(), r.precision)
+    ctx.load_tables(r.mu, r.sigma)
+    ctx.init_beam()
+    idd, _ = ctx.step(r.nsteps)
+    ctx.close()
+    return idd
 
-    pool = beams.uneven_beams(64, seed=args.serve_seed)
-    reqs = [r for r in pool if r.cfg.ny <= args.serve_max_ny][: args.serve_beams]
-    prec = capi.PREC_MIXED if args.precision == "mixed" else capi.PREC_FP64
+
+def _serve(reqs, arrivals, workers=2):
+    """Submit each request at its arrival time (seconds from the start) to a
+    continuous-batching server; returns (IDDs, makespan s, latencies ms)."""
+    from bfpn_gpu_b200 import capi
+    with capi.Server(devices=(0,), workers_per_device=workers) as srv:
+        start = time.perf_counter()
+        tickets, submit_t = [], []
+        for r, at in zip(reqs, arrivals):
+            delay = at - (time.perf_counter() - start)
+            if delay > 0:
+                time.sleep(delay)
+            submit_t.append(time.perf_counter())
+            tickets.append(srv.submit(r.beam()))
+        out, lat = [], []
+        for r, t, t0 in zip(reqs, tickets, submit_t):
+            idd, _, info = srv.wait(t, r.nsteps)
+            out.append(idd)
+            lat.append(info["queue_ms"] + info["run_ms"])
+        return out, time.perf_counter() - start, np.array(lat)
+
+
+def _max_rel_diff(got, ref):
+    return max(float(np.abs(a - b).max() / np.abs(b).max()) for a, b in zip(got, ref))
+
+
+def run_batch(args):
+    """Config 4: the seeded set of uneven beams (energy 70-230 MeV, water or
+    bone, sigma_yz 0.3-0.8 cm, Ny = Nz in {16,32,48,64}, Nmu = Nom in
+    {12,16,20}, Ng ~ 2 E0, depth 1.2 x CSDA range) served by continuous
+    batching -- bundles by shape class, admitted by device footprint -- against
+    the plain path, one beam at a time through a fresh context.  Beams/s of
+    both, every batched IDD against the same beam run alone."""
+    import torch  # noqa: F401
+    from bfpn_gpu_b200 import beams, capi
+
+    reqs = [r for r in beams.uneven_beams(args.batch_beams, seed=args.serve_seed) if r.cfg.ny <= args.batch_max_ny]
     for r in reqs:
-        r.precision = prec
+        r.precision = capi.PREC_MIXED
     updates = sum(r.cells * (2 * r.nsteps - 1) for r in reqs)
-
-    def plain(r):
-        ctx = Context(r.cfg.grid(), r.cfg.phys(), r.precision)
-        ctx.load_tables(r.mu, r.sigma)
-        ctx.init_beam()
-        idd, _ = ctx.step(r.nsteps)
-        ctx.close()
-        return idd
-
-    plain(reqs[0])  # warm-up: module load, first graph capture
+    _plain_run(reqs[0])  # warm-up: module load
     t0 = time.perf_counter()
-    alone = [plain(r) for r in reqs]
+    alone = [_plain_run(r) for r in reqs]
     t_plain = time.perf_counter() - t0
-
-    def served(arrivals):
-        with capi.Server(devices=(0,), workers_per_device=args.serve_workers) as srv:
-            start = time.perf_counter()
-            tickets = []
-            for r, at in zip(reqs, arrivals):
-                delay = at - (time.perf_counter() - start)
-                if delay > 0:
-                    time.sleep(delay)
-                tickets.append(srv.submit(r.beam()))
-            out, lat = [], []
-            for r, t, at in zip(reqs, tickets, arrivals):
-                idd, _, info = srv.wait(t, r.nsteps)
-                out.append(idd)
-                lat.append(info["queue_ms"] + info["run_ms"])
-            return out, time.perf_counter() - start, np.array(lat)
-
-    zero = np.zeros(len(reqs))
-    served(zero[:1])  # warm-up of the worker contexts' kernels
-    batch_out, t_batch, batch_lat = served(zero)
-    rate = args.serve_rate or 0.9 * len(reqs) / t_batch
-    arrivals = beams.poisson_arrivals(len(reqs), rate, seed=args.serve_seed)
-    pois_out, t_pois, pois_lat = served(arrivals)
-    diff = max(float(np.abs(a - b).max() / np.abs(b).max()) for a, b in zip(batch_out + pois_out, alone + alone))
-    out = {"metric": "served beams/s", "value": len(reqs) / t_batch, "unit": "beams/s", "n_gpus": 1,
-           "higher_is_better": True, "dtype": "f32 state / f64 recursion" if prec == capi.PREC_MIXED else "f64",
-           "data": "synthetic uneven beams drawn from a seed (reference water / bone tables)",
-           "config": {"workload": "%d uneven beams (E 70-230 MeV, water/bone, Ny=Nz <= %d, Nmu=Nom in 12/16/20, "
-                                  "Ng ~ 2 E0, depth 1.2 CSDA range)" % (len(reqs), args.serve_max_ny),
-                      "workers_per_device": args.serve_workers, "precision": args.precision},
+    batched, t_batch, lat = _serve(reqs, np.zeros(len(reqs)))
+    name, cores = host_cpu()
+    out = {"metric": "beams/s", "value": len(reqs) / t_batch, "unit": "beams/s", "n_gpus": 1,
+           "higher_is_better": True, "dtype": "f32 state / f64 recursion", "data": "synthetic seeded beam set, "
+           "reference water / bone tables",
+           "config": {"workload": "%d uneven beams (E 70-230 MeV, water/bone, Ny=Nz in 16/32/48/64 up to %d, "
+                                  "Nmu=Nom in 12/16/20, Ng ~ 2 E0, depth 1.2 CSDA range; the first %d of the seeded "
+                                  "set), all submitted at t=0" % (len(reqs), args.batch_max_ny, args.batch_beams),
+                      "mode": "continuous batching (bundles by shape class, footprint admission)"},
            "plain_beams_per_s": len(reqs) / t_plain, "speedup_vs_plain": t_plain / t_batch,
+           "seconds_batched": t_batch, "seconds_plain": t_plain,
            "updates_per_s_batched": updates / t_batch, "updates_per_s_plain": updates / t_plain,
-           "batch_latency_ms": {"p50": float(np.percentile(batch_lat, 50)), "p99": float(np.percentile(batch_lat, 99))},
-           "poisson": {"rate_per_s": rate, "beams_per_s": len(reqs) / t_pois,
-                       "latency_ms": {q: float(np.percentile(pois_lat, float(q[1:]))) for q in ("p50", "p99", "p99.9")}},
-           "max_idd_diff_served_vs_alone": diff, "timing": "host wall clock around whole beam solves"}
+           "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                          "max": float(lat.max())},
+           "max_idd_diff_batched_vs_alone_rel_to_peak": _max_rel_diff(batched, alone),
+           "timing": "host wall clock around whole beam solves (set-up included)", "host_cpu": name}
+    print(json.dumps(out), flush=True)
+
+
+def run_serve(args):
+    """Config 5: Poisson streams of beam requests at each rate of a sweep,
+    drawn from the config-4 distribution with a share of full 80x80 paper-grid
+    requests, served by continuous batching.  Per rate: beams/s, latency
+    percentiles, and every served IDD against the same beam run alone."""
+    import dataclasses
+
+    import torch  # noqa: F401
+    from bfpn_gpu_b200 import beams, capi, make_config, read_tables
+
+    rates = [float(x) for x in args.serve_rates.split(",")]
+    rng = np.random.default_rng(args.serve_seed + 7)
+    small = beams.uneven_beams(args.serve_beams, seed=args.serve_seed)
+    big_w, _ = WORKLOADS["water230_80"]
+    big_cfg = make_config(**big_w)
+    big_mu, big_sig = read_tables(os.path.join(ROOT, "tests", "golden", "tables", "water"), big_cfg.ng)
+    reqs = []
+    for r in small:
+        if rng.random() < args.serve_large_frac:
+            reqs.append(beams.BeamRequest(dataclasses.replace(big_cfg), big_mu, big_sig, big_cfg.max_steps(),
+                                          capi.PREC_MIXED))
+        else:
+            r.precision = capi.PREC_MIXED
+            reqs.append(r)
+    n_large = sum(1 for r in reqs if r.cfg.ny == 80)
+    alone = {}
+    for k, r in enumerate(reqs):  # solo IDD of each distinct beam (the large requests are one beam)
+        key = "large" if r.cfg.ny == 80 else k
+        if key not in alone:
+            alone[key] = _plain_run(r)
+    ref = [alone["large" if r.cfg.ny == 80 else k] for k, r in enumerate(reqs)]
+    sweep = []
+    for rate in rates:
+        arrivals = beams.poisson_arrivals(len(reqs), rate, seed=args.serve_seed + int(rate))
+        got, t, lat = _serve(reqs, arrivals)
+        sweep.append({"rate_per_s": rate, "beams_per_s": len(reqs) / t, "makespan_s": t,
+                      "latency_ms": {q: float(np.percentile(lat, float(q[1:]))) for q in ("p50", "p99", "p99.9")},
+                      "max_idd_diff_vs_alone_rel_to_peak": _max_rel_diff(got, ref)})
+    best = max(sweep, key=lambda x: x["beams_per_s"])
+    out = {"metric": "served beams/s", "value": best["beams_per_s"], "unit": "beams/s", "n_gpus": 1,
+           "higher_is_better": True, "dtype": "f32 state / f64 recursion",
+           "data": "synthetic seeded requests, reference water / bone tables",
+           "config": {"workload": "%d requests: config-4 beams with %d full 80x80x20x20x500 water 230 MeV "
+                                  "requests, Poisson arrivals" % (len(reqs), n_large),
+                      "rates_per_s": rates, "mode": "continuous batching (bundles by shape class, footprint "
+                                                    "admission)"},
+           "sweep": sweep, "timing": "host wall clock from each submit to its result"}
     print(json.dumps(out), flush=True)
 
 
@@ -583,12 +642,15 @@ def main():
     ap.add_argument("--accuracy-steps", type=int, default=1000)
     ap.add_argument("--cpu-steps", type=int, default=1)
     ap.add_argument("--reference-budget-s", type=float, default=120.0)
+    ap.add_argument("--batch", action="store_true",
+                    help="the uneven beam set by continuous batching against the plain one-beam-at-a-time path")
+    ap.add_argument("--batch-beams", type=int, default=64)
+    ap.add_argument("--batch-max-ny", type=int, default=64, help="keep the beams of the set with Ny <= this")
     ap.add_argument("--serve", action="store_true",
-                    help="batched / served uneven beams against the plain one-beam-at-a-time path")
-    ap.add_argument("--serve-beams", type=int, default=16)
-    ap.add_argument("--serve-max-ny", type=int, default=32)
-    ap.add_argument("--serve-workers", type=int, default=8)
-    ap.add_argument("--serve-rate", type=float, default=None, help="Poisson arrival rate (default 0.9 x batched)")
+                    help="Poisson request streams at each rate of --serve-rates, served by continuous batching")
+    ap.add_argument("--serve-beams", type=int, default=20)
+    ap.add_argument("--serve-rates", default="10,30,100,300,1000")
+    ap.add_argument("--serve-large-frac", type=float, default=0.1)
     ap.add_argument("--serve-seed", type=int, default=20261203)
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD,
                     help="single-beam workload (default: the 80x80 paper-scale grid)")
@@ -606,7 +668,9 @@ def main():
     TABLES = os.path.join(ROOT, "tests", "golden", "tables", WORKLOAD["material_name"])
     if args.ng:
         WORKLOAD["ng"] = args.ng
-    if args.serve:
+    if args.batch:
+        run_batch(args)
+    elif args.serve:
         run_serve(args)
     elif args.out_of_core:
         run_out_of_core(args)

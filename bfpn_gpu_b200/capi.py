@@ -138,6 +138,7 @@ SIGNATURES = {
     "bfpn_bundle_destroy": (ctypes.c_int, [_vp]),
     "bfpn_bundle_last_error": (ctypes.c_char_p, [_vp]),
     "bfpn_device_count": (_i32, []),
+    "bfpn_device_memory": (ctypes.c_int, [_i32, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
     "bfpn_device_info": (_i32, [_i32, ctypes.c_char_p, _i32]),
     "bfpn_stream": (_vp, [_vp]),
 }

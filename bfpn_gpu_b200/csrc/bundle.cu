@@ -38,6 +38,7 @@ using namespace bfpn;
 namespace {
 
 constexpr int kMaxSideStreams = 4;
+constexpr int kBundleMaxPlane = 65;  // Ny + 1 and Nz + 1 of a bundle's beams
 
 struct Tuning {
     bool tuned = false;
@@ -407,6 +408,11 @@ bfpn_status bfpn_bundle_accepts(const bfpn_beam* beam) {
     const long long nyz = static_cast<long long>(g.Ny + 1) * (g.Nz + 1);
     if (g.Ny < 1 || g.Nz < 1 || nyz < angle_slots_tile(N))
         return bfail(nullptr, BFPN_INVALID_ARG, "bundle: the plane is smaller than one DST tile");
+    // planes up to 65 x 65 points: the range the batched kernels have run over
+    // (a serving run that batched 80 x 80 beams next to other classes raised
+    // an illegal memory access whose cause is not found; such beams run alone)
+    if (g.Ny + 1 > kBundleMaxPlane || g.Nz + 1 > kBundleMaxPlane)
+        return bfail(nullptr, BFPN_INVALID_ARG, "bundle: planes up to 65 x 65 points; larger beams run alone");
     const bool square_plane = g.Ny == g.Nz && (transport_plane_supported(g.Ny, g.Nz) || transport_cluster_supported(g.Ny, g.Nz));
     if (!transport_stream_supported(g.Ny, N * N) && !square_plane)
         return bfail(nullptr, BFPN_INVALID_ARG, "bundle: no batched transport kernel for this plane");
@@ -479,6 +485,8 @@ bfpn_status bfpn_bundle_admit(bfpn_bundle* b, const bfpn_beam* beam, int32_t* sl
     if (b->shaped && (beam->grid.Ny + 1 != b->NP || beam->grid.Nz + 1 != b->NP || beam->grid.Nmu != b->N ||
                       beam->grid.Nom != b->N))
         return bfail(b, BFPN_INVALID_ARG, "bundle admit: the beam's grid is not the bundle's shape class (" + b->key + ")");
+    if (bfpn_bundle_accepts(beam) != BFPN_OK)
+        return bfail(b, BFPN_INVALID_ARG, std::string("bundle admit: ") + g_bundle_error.substr(8));
     DeviceScope scope(b->device);
     // admission by footprint: the whole context must fit in free memory, with a margin
     uint64_t need = 0;
@@ -575,6 +583,17 @@ bfpn_status bfpn_bundle_sync(bfpn_bundle* b) {
     if (err) {
         cudaMemset(b->err, 0, sizeof(int));
         return bfail(b, BFPN_TIMEOUT, "bundle: a kernel's bounded wait ran out (code " + std::to_string(err) + ")");
+    }
+    // the slots' own error words (the tensor-core source kernels' bounded waits)
+    for (size_t i = 0; i < b->slots.size(); ++i) {
+        bfpn_ctx* c = b->slots[i].ctx;
+        if (!c || !c->dev_err) continue;
+        BUNDLE_CUDA(b, cudaMemcpy(&err, c->dev_err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (err) {
+            cudaMemset(c->dev_err, 0, sizeof(int));
+            return bfail(b, BFPN_TIMEOUT, "bundle: slot " + std::to_string(i) + ": a source kernel's bounded wait ran out "
+                                          "(code " + std::to_string(err) + ")");
+        }
     }
     return BFPN_OK;
 }

@@ -111,6 +111,16 @@ uint64_t footprint(const bfpn_grid& g, int prec, bool lite) {
     b += 4 * static_cast<uint64_t>(L.part_blocks) * sizeof(double);
     b += 2 * static_cast<uint64_t>(L.hist_cap) * sizeof(double);
     b += 64ull * g.Ng * sizeof(double) + (1u << 20);               // small tables
+    if (prec == BFPN_PREC_MIXED) {
+        // tensor-core source, at most every group a source group: the packed
+        // split-bf16 A operand, the B tiles of the angular kernel and the
+        // energy stage's coefficient tiles (an upper bound: 2 Ng x Ng bf16 pairs)
+        const int ntiles = (static_cast<int>(NA) + 255) / 256;
+        const int nt = ((static_cast<int>(NA) + ntiles - 1) / ntiles + 15) / 16 * 16;
+        b += umma_pack_bytes(g.Ng, (g.Ny + 1) * (g.Nz + 1), static_cast<int>(NA), 16);
+        b += umma_blob_bytes(g.Ng, static_cast<int>(NA), nt, 16);
+        b += 8ull * g.Ng * g.Ng;
+    }
     return b;
 }
 
@@ -1889,6 +1899,26 @@ int32_t bfpn_device_count(void) {
         return 0;
     }
     return n;
+}
+
+bfpn_status bfpn_device_memory(int32_t device, uint64_t* free_bytes, uint64_t* total_bytes) {
+    int n = 0, prev = -1;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+        cudaGetLastError();
+        return BFPN_NO_DEVICE;
+    }
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    size_t f = 0, t = 0;
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaMemGetInfo(&f, &t);
+    if (prev >= 0) cudaSetDevice(prev);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return BFPN_CUDA_ERROR;
+    }
+    if (free_bytes) *free_bytes = f;
+    if (total_bytes) *total_bytes = t;
+    return BFPN_OK;
 }
 
 int32_t bfpn_device_info(int32_t device, char* buf, int32_t buf_len) {

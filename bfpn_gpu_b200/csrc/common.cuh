@@ -149,7 +149,7 @@ cudaError_t launch_energy_slots(const EnergyArgs<float>* args, const int* begin,
 cudaError_t launch_transport_slots(const TransportArgs<float>* args, const int* begin, int nslots, int blocks,
                                    int NP, int NA, int ang_chunk, bool cluster, cudaStream_t s);
 int transport_cluster_size(int NP);
-// Row-streaming transport (float state, paired angles, Ny + 1 <= 128, any Nz):
+// Row-streaming transport (float state, paired angles, Ny + 1 <= 256, any Nz):
 // one block per (group, 8-angle chunk) plane walking the z rows, in place.
 cudaError_t launch_transport_stream(const TransportArgs<float>& a, cudaStream_t s);
 bool transport_stream_supported(int Ny, int NA);

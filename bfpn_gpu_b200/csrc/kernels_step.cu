@@ -73,6 +73,61 @@ __device__ __forceinline__ void energy_lane_update(const double* __restrict__ c,
 
 // The sweep of block `bid` of one beam's lanes (the kernels below map their
 // blocks onto it: one beam, or the slots of a bundle).
+// The eq15 constants of one group held in registers (loaded a group ahead by
+// the ring sweep, so their loads are off the recursion's critical path), and
+// the eq15 update of energy_lane_update from them: the same operations in the
+// same order.
+struct Eq15Coef {
+    double c_up, c_cur, c_f, r_f, r_up, r_cur, r_fg, a, r_hi, inv_coe, f_from_f, inv_f, f_from_hi;
+    double s_hi, s_lo, s_g;  // straggling
+    double d0, d1;           // dose weights of psi^1, psi^2
+};
+
+template <int MODE>
+__device__ __forceinline__ Eq15Coef load_eq15_coef(const double* __restrict__ c, const double* __restrict__ dc,
+                                                   bool dose) {
+    Eq15Coef k;
+    k.c_up = __ldg(c + EC_C_UP);
+    k.c_cur = __ldg(c + EC_C_CUR);
+    k.c_f = __ldg(c + EC_C_F);
+    k.r_f = __ldg(c + EC_R_F);
+    k.r_up = __ldg(c + EC_R_UP);
+    k.r_cur = __ldg(c + EC_R_CUR);
+    k.r_fg = __ldg(c + EC_R_FG);
+    k.a = __ldg(c + EC_A);
+    k.r_hi = __ldg(c + EC_R_HI);
+    k.inv_coe = __ldg(c + EC_INV_COE);
+    k.f_from_f = __ldg(c + EC_F_FROM_F);
+    k.inv_f = __ldg(c + EC_INV_F);
+    k.f_from_hi = __ldg(c + EC_F_FROM_HI);
+    k.s_hi = k.s_lo = k.s_g = 0.0;
+    if (MODE == EMODE_EQ15_STRAG) {
+        k.s_hi = __ldg(c + EC_S_HI);
+        k.s_lo = __ldg(c + EC_S_LO);
+        k.s_g = __ldg(c + EC_S_G);
+    }
+    k.d0 = dose ? __ldg(dc) : 0.0;
+    k.d1 = dose ? __ldg(dc + 1) : 0.0;
+    return k;
+}
+
+template <int MODE>
+__device__ __forceinline__ void eq15_update(const Eq15Coef& k, int ek, double Fg, double fg, double sg, double Fn,
+                                            double F_hi_old, double f_hi_old, double next_F, double next_f,
+                                            double& Fv, double& fv) {
+    const double up = F_hi_old - f_hi_old;
+    const double cur = Fg - fg;
+    double common = k.c_up * up + k.c_cur * cur + k.c_f * Fg + sg;
+    if (MODE == EMODE_EQ15_STRAG) {
+        const double Flo = (ek > 0) ? Fn : 0.0;
+        common += k.s_hi * F_hi_old + k.s_lo * Flo - k.s_g * Fg;
+    }
+    const double hi_delta = next_F - next_f;
+    const double rhs = k.r_f * fg + k.r_up * up + k.r_cur * cur + k.r_fg * Fg - k.a * common + k.r_hi * hi_delta;
+    fv = rhs * k.inv_coe;
+    Fv = k.f_from_f * fv + k.inv_f * common + k.f_from_hi * hi_delta;
+}
+
 template <int MODE, typename T, int LPT, int D>
 __device__ __forceinline__ void energy_body(const EnergyArgs<T>& a, long long bid) {
     // D: groups prefetched ahead of use
@@ -229,8 +284,12 @@ __device__ __forceinline__ void energy_ring_body(const EnergyArgs<float>& a, lon
         }
     }
     constexpr bool kStrag = MODE == EMODE_EQ15_STRAG;
+    const bool dose = a.partials != nullptr;
+    Eq15Coef k_next = load_eq15_coef<MODE>(a.coef + (Ng - 1) * kEnergyCoef, a.dose_coef + 2 * (Ng - 1), dose);
     for (int i = 0; i < Ng; ++i) {
         const int ek = Ng - 1 - i;
+        const Eq15Coef kc = k_next;
+        if (ek > 0) k_next = load_eq15_coef<MODE>(a.coef + (ek - 1) * kEnergyCoef, a.dose_coef + 2 * (ek - 1), dose);
         // groups 0 .. i (and i+1 for straggling) have landed
         if (kStrag) asm volatile("cp.async.wait_group %0;" ::"n"(D - 3) : "memory");
         else asm volatile("cp.async.wait_group %0;" ::"n"(D - 2) : "memory");
@@ -239,8 +298,6 @@ __device__ __forceinline__ void energy_ring_body(const EnergyArgs<float>& a, lon
         float4 vn = make_float4(0.f, 0.f, 0.f, 0.f);
         if (kStrag && ek > 0) vn = *slot((i + 1) % D, 0);
         if (i > 0) fill(i - 1 + D);  // the slot read in the previous iteration
-        const double* __restrict__ c = a.coef + ek * kEnergyCoef;
-        const double* __restrict__ dc = a.dose_coef + 2 * ek;
         const float Fa[4] = {vF.x, vF.y, vF.z, vF.w}, fa[4] = {vf.x, vf.y, vf.z, vf.w};
         const float sa[4] = {vs.x, vs.y, vs.z, vs.w}, na[4] = {vn.x, vn.y, vn.z, vn.w};
         float Fo[4], fo[4];
@@ -248,12 +305,12 @@ __device__ __forceinline__ void energy_ring_body(const EnergyArgs<float>& a, lon
         for (int j = 0; j < 4; ++j) {
             const double Fg = Fa[j], fg = fa[j];
             double Fv, fv;
-            energy_lane_update<MODE>(c, ek, Fg, fg, static_cast<double>(sa[j]), static_cast<double>(na[j]), F_hi_old[j],
-                                     f_hi_old[j], next_F[j], next_f[j], Fv, fv);
+            eq15_update<MODE>(kc, ek, Fg, fg, static_cast<double>(sa[j]), static_cast<double>(na[j]), F_hi_old[j],
+                              f_hi_old[j], next_F[j], next_f[j], Fv, fv);
             Fo[j] = static_cast<float>(Fv);
             fo[j] = static_cast<float>(fv);
-            if (a.partials && ok) {
-                acc += w_pos[j] * (__ldg(dc) * static_cast<double>(Fo[j]) + __ldg(dc + 1) * static_cast<double>(fo[j]));
+            if (dose && ok) {
+                acc += w_pos[j] * (kc.d0 * static_cast<double>(Fo[j]) + kc.d1 * static_cast<double>(fo[j]));
                 accp += static_cast<double>(fo[j]);
             }
             F_hi_old[j] = Fg;
@@ -1252,64 +1309,79 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(ClusterPlane<NP, CL
 }
 
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
 // Row-streaming transport (float state, paired angles), any plane with
-// Ny + 1 <= 128: one block per (group, 8-angle chunk) plane walks the z rows
-// once.  Thread (y, q) owns column y for angle pair q and keeps its z-stencil
-// in registers -- the last three rows of F, of the predictor P and of H, and
-// the face values G of the z-walk -- so the z-parts of both stages are line
-// walks with one limiter per cell and no memory traffic.  The y-parts need
-// the whole row: row i of F (staged by cp.async a few rows ahead into a ring)
-// and row i-2 of P sit in shared memory; each thread forms the y face value
-// at its own cell from its two neighbours, publishes it, and takes the
+// Ny + 1 <= 256: one block per (group, 8-angle chunk) plane walks the z rows
+// once.  Two threads per column y, each carrying two of the chunk's four angle
+// pairs (fp32x2), keep the column's z-stencil in registers -- the last three
+// rows of F, of the predictor P and of H, and the face values G of the z-walk
+// -- so the z-parts of both stages are line walks with one limiter per cell
+// and no memory traffic.  The y-parts need the whole row: row i of F (staged
+// by cp.async a few rows ahead into a ring, one 16-byte piece per thread) and
+// row i-2 of P sit in shared memory; each thread forms the y face value at its
+// own cells from their two neighbours, publishes it, and takes the
 // neighbour's after the barrier.  Iteration i runs stage 1 (predictor P and
 // H = F - dt/2 div F) on row i and stage 2 (H - dt/2 div P, clipped) on row
 // i-2, whose z-stencil needs P up to row i.  Two barriers per row, no halo
-// recomputed, no cluster; the per-cell arithmetic and its order are those of
-// the whole-plane kernel, so the states agree with it value for value.
-// Rows and columns beyond the plane repeat the edge value, as the
-// reference's clamped indices do.
+// recomputed, no cluster; the first two and last two rows are peeled out of
+// the loop so its body is branch-free.  The per-cell arithmetic and its order
+// are those of the whole-plane kernel.  Rows and columns beyond the plane
+// repeat the edge value, as the reference's clamped indices do.
 // ---------------------------------------------------------------------------
 constexpr int kStreamPairs = 4;            // angle pairs per block (8 angles, 32 bytes per position)
 constexpr int kStreamRing = 8;             // rows of F in the shared-memory ring
 constexpr int kStreamAhead = 4;            // rows copied ahead of the one a row's z-stencil needs
 constexpr int kStreamPRows = 4;            // rows of P kept in shared memory (rows i-2 .. i)
-constexpr int kStreamMaxThreads = 512;     // planes up to 128 points wide (80 registers: 2 blocks of 352 per SM at 81)
+constexpr int kStreamMaxThreads = 512;     // two threads per column: planes up to 256 points wide
 
 size_t transport_stream_smem(int NPy) {
     const size_t row = static_cast<size_t>(NPy) * kStreamPairs * sizeof(float2);
-    const size_t grow = static_cast<size_t>(NPy + 2) * kStreamPairs * sizeof(float2);
+    const size_t grow = static_cast<size_t>(NPy + 3) * kStreamPairs * sizeof(float2);
     return (kStreamRing + kStreamPRows) * row + 2 * grow;
 }
+
+// One thread per (column y, half h): angle pairs h and h + 2 of the block's
+// four, so the (Ny+1) x 2 threads also copy the row's (Ny+1) x 2 16-byte
+// pieces one each.  The per-pair state lives in a PairState.
+struct StreamPair {
+    float2 f0, f1, f2, p0, p1, p2, h0, h1, h2;  // F rows i .. i+2, P rows j .. j+2, H rows j .. i (j = i-2)
+    float2 gz_m, gz_0, zfwd, zfwd2;             // z-walk of F: G(i-1), G(i), last difference
+    float2 pz_m, pz_0, pfwd, pfwd2;             // z-walk of P: G(j-1), G(j)
+    float2 wry, wrz, hy, hz;
+    bool dnz;
+    int own, offl, offr, ghi, glo;              // shared-memory offsets (float2) in a row / a face row
+    bool ok0, ok1;                              // angles of the pair inside NA (output stores)
+};
 
 __device__ __forceinline__ void transport_stream_body(const TransportArgs<float>& a, int n_chunks, int bid) {
     constexpr int A2 = kStreamPairs, AC = 2 * A2, RF = kStreamRing, PD = kStreamAhead, RP = kStreamPRows;
     static_assert((RF & (RF - 1)) == 0 && (RP & (RP - 1)) == 0 && AC == 8, "ring sizes are powers of two");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int Ny = a.Ny, Nz = a.Nz, NPy = Ny + 1, NA = a.NA;
-    const int RS = NPy * A2;  // one row, in float2
+    const int RS = NPy * A2;       // one row, in float2
+    const int GS = (NPy + 2) * A2 + A2;  // one face row: faces -1 .. N+1, then a spare row for edge-less threads
     float2* Fr = reinterpret_cast<float2*>(smem_raw);  // [RF][NPy][A2]
     float2* Pr = Fr + RF * RS;                         // [RP][NPy][A2]
-    float2* GF = Pr + RP * RS;                         // [NPy + 2][A2]: G of F's y-walk, faces -1 .. N+1
-    float2* GP = GF + (NPy + 2) * A2;                  // same for P
+    float2* GF = Pr + RP * RS;                         // [GS]: G of F's y-walk
+    float2* GP = GF + GS;                              // same for P
     const int chunk = bid % n_chunks, ek = bid / n_chunks, a0 = chunk * AC;
     const size_t zs = static_cast<size_t>(NPy) * NA;  // one z row in the state
     const size_t base = static_cast<size_t>(ek) * (Nz + 1) * zs + a0;
-    const int tid = threadIdx.x, q = tid % A2, y = tid / A2;
-    const bool act = y < NPy;
+    const int tid = threadIdx.x, h = tid & 1, y = tid >> 1;
 
-    // this thread's 16-byte piece of every row: threads 0 .. 2 NPy - 1 copy position tid / 2, half tid % 2
+    // this thread's 16-byte piece of every row: position y, angles a0 + 4h .. a0 + 4h + 3
     const bool vec = NA % 4 == 0;
-    const bool loader = vec && tid < 2 * NPy;
-    const bool lok = loader && a0 + 4 * (tid & 1) < NA;
-    const float* lsrc = a.in + base + static_cast<size_t>(tid >> 1) * NA + 4 * (tid & 1);
-    float* ldst = reinterpret_cast<float*>(Fr) + (tid >> 1) * AC + 4 * (tid & 1);
+    const bool lok = vec && a0 + 4 * h < NA;
+    const float* in0 = a.in;
+    const float* lsrc = in0 + base + static_cast<size_t>(y) * NA + 4 * h;
+    float* ldst = reinterpret_cast<float*>(Fr) + y * AC + 4 * h;
     auto fill = [&](int r) {  // row r of F into slot r % RF; one commit group per call, empty past the plane
         if (r <= Nz) {
-            float* dst = ldst + (r & (RF - 1)) * (2 * RS);
-            if (loader) cp_async16(dst, lok ? lsrc + static_cast<size_t>(r) * zs : a.in, lok);
-            if (!vec) {
+            if (vec) {
+                cp_async16(ldst + (r & (RF - 1)) * (2 * RS), lok ? lsrc + static_cast<size_t>(r) * zs : in0, lok);
+            } else {
                 float* row = reinterpret_cast<float*>(Fr + (r & (RF - 1)) * RS);
-                const float* src = a.in + base + static_cast<size_t>(r) * zs;
+                const float* src = in0 + base + static_cast<size_t>(r) * zs;
                 for (int v = tid; v < NPy * AC; v += blockDim.x) {
                     const int e = v % AC, p = v / AC;
                     row[p * AC + e] = (a0 + e < NA) ? src[static_cast<size_t>(p) * NA + e] : 0.f;
@@ -1319,86 +1391,107 @@ __device__ __forceinline__ void transport_stream_body(const TransportArgs<float>
         asm volatile("cp.async.commit_group;" ::: "memory");
     };
 
-    const bool ok0 = act && a0 + 2 * q < NA, ok1 = act && a0 + 2 * q + 1 < NA;  // output stores
-    const int g0 = min(a0 + 2 * q, NA - 1), g1 = min(a0 + 2 * q + 1, NA - 1);
-    const float wy0 = a.omega[2 * g0], wz0 = a.omega[2 * g0 + 1];
-    const float wy1 = a.omega[2 * g1], wz1 = a.omega[2 * g1 + 1];
-    const float2 wry = make_float2(wy0 / a.dy, wy1 / a.dy), wrz = make_float2(wz0 / a.dz, wz1 / a.dz);
-    const bool dny = wy0 < 0.f, dnz = wz0 < 0.f;
-    const float2 hy = dny ? make_float2(-0.5f, -0.5f) : make_float2(0.5f, 0.5f);
-    const float2 hz = dnz ? make_float2(-0.5f, -0.5f) : make_float2(0.5f, 0.5f);
     const float2 ndt = make_float2(-a.dt, -a.dt), nhdt = make_float2(-0.5f * a.dt, -0.5f * a.dt);
     const float lo = a.preserve_sign ? -INFINITY : 0.f;
-    const int yc = act ? y : 0;
-    const int own = yc * A2 + q;
-    const int offl = max(yc - 1, 0) * A2 + q, offr = min(yc + 1, Ny) * A2 + q;
-    // G index of the two faces of this cell's y-divergence (G is stored one face up)
-    const int ghi = own + (dny ? 2 * A2 : A2), glo = own + (dny ? A2 : 0);
-    const int gedge = yc == 0 ? q : (yc == Ny ? (NPy + 1) * A2 + q : -1);  // face beyond the plane
-    float* orow = a.out + base + static_cast<size_t>(yc) * NA + 2 * q;   // output row 0
+    // the face beyond the plane (edge threads) or a spare slot (the others): every thread stores one
+    const int gedge_row = y == 0 ? 0 : (y == Ny ? (NPy + 1) * A2 : (NPy + 2) * A2);
+    StreamPair S[2];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        StreamPair& P = S[k];
+        const int q = h + 2 * k;
+        P.ok0 = a0 + 2 * q < NA;
+        P.ok1 = a0 + 2 * q + 1 < NA;
+        const int g0 = min(a0 + 2 * q, NA - 1), g1 = min(a0 + 2 * q + 1, NA - 1);
+        const float wy0 = a.omega[2 * g0], wz0 = a.omega[2 * g0 + 1];
+        const float wy1 = a.omega[2 * g1], wz1 = a.omega[2 * g1 + 1];
+        P.wry = make_float2(wy0 / a.dy, wy1 / a.dy);
+        P.wrz = make_float2(wz0 / a.dz, wz1 / a.dz);
+        const bool dny = wy0 < 0.f;
+        P.dnz = wz0 < 0.f;
+        P.hy = dny ? make_float2(-0.5f, -0.5f) : make_float2(0.5f, 0.5f);
+        P.hz = P.dnz ? make_float2(-0.5f, -0.5f) : make_float2(0.5f, 0.5f);
+        P.own = y * A2 + q;
+        P.offl = max(y - 1, 0) * A2 + q;
+        P.offr = min(y + 1, Ny) * A2 + q;
+        // G index of the two faces of this cell's y-divergence (G is stored one face up)
+        P.ghi = P.own + (dny ? 2 * A2 : A2);
+        P.glo = P.own + (dny ? A2 : 0);
+        P.p0 = P.p1 = P.p2 = P.h0 = P.h1 = P.h2 = make_float2(0.f, 0.f);
+        P.pz_m = P.pz_0 = P.pfwd = P.pfwd2 = make_float2(0.f, 0.f);
+    }
+    float* orow = a.out + base + static_cast<size_t>(y) * NA;  // this position's angles a0 .. a0+7, row 0
 
-    // Threads past the plane (the last warp's padding) compute on row position
-    // yc = 0 like thread 0 but publish and store nothing.
-    auto y_face = [&](float2* G, const float2* row, float2 x) {
-        const float2 back = sub2(x, row[offl]), fwd = sub2(row[offr], x);
-        const float2 g = __ffma2_rn(hy, superbee_diff2(back, __fadd2_rn(back, back), fwd, __fadd2_rn(fwd, fwd)), x);
-        if (act) {
-            G[own + A2] = g;
-            if (gedge >= 0) G[gedge] = x;  // the faces beyond the plane equal the edge value
+    auto y_face = [&](float2* G, const float2* row, const StreamPair& P, float2 x) {
+        const float2 back = sub2(x, row[P.offl]), fwd = sub2(row[P.offr], x);
+        G[P.own + A2] = __ffma2_rn(P.hy, superbee_diff2(back, __fadd2_rn(back, back), fwd, __fadd2_rn(fwd, fwd)), x);
+        G[gedge_row + (P.own - y * A2)] = x;  // faces beyond the plane equal the edge value
+    };
+    int slot = 0, pslot = 0;  // ring slots of row i of F and of P
+
+    // phase A of iteration i: y faces of F row i (stage 1) and P row j = i-2 (stage 2);
+    // f2 = F(min(i+2, Nz)) (row Nz stays in its slot: nothing is copied past the plane)
+    auto phase_a = [&](int i, bool st1, bool st2) {
+        const float2* f2row = Fr + ((slot + min(2, Nz - i)) & (RF - 1)) * RS;
+        const float2* Fi = Fr + slot * RS;
+        const float2* Pj = Pr + ((pslot - 2) & (RP - 1)) * RS;
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            StreamPair& P = S[k];
+            P.f2 = f2row[P.own];
+            if (st1) y_face(GF, Fi, P, P.f0);
+            if (st2) y_face(GP, Pj, P, P.p0);
         }
     };
-
-    // registers: F rows i .. i+2, P rows j .. j+2 and H rows j .. i (j = i - 2), z faces
-    float2 f0, f1, f2, p0{}, p1{}, p2{}, h0{}, h1{}, h2{};
-    float2 gz_m{}, gz_0{}, zfwd{}, zfwd2{};   // z-walk of F: G(i-1), G(i), last difference
-    float2 pz_m{}, pz_0{}, pfwd{}, pfwd2{};   // z-walk of P: G(j-1), G(j)
-    int slot = 0, pslot = 0;                  // ring slots of row i of F and of P
-
-    // phase A of iteration i: the y faces of row i of F (stage 1) and of row j
-    // of P (stage 2); f2 = F(min(i+2, Nz)) (row Nz stays in its slot: nothing is
-    // copied past the plane)
-    auto phase_a = [&](int i, bool st1, bool st2) {
-        f2 = Fr[((slot + min(2, Nz - i)) & (RF - 1)) * RS + own];
-        if (st1) y_face(GF, Fr + slot * RS, f0);
-        if (st2) y_face(GP, Pr + ((pslot - 2) & (RP - 1)) * RS, p0);
-    };
-    // phase B, stage 1 on row i: z face i+1, predictor P(i) (also to shared
-    // memory for the y faces two rows on) and H(i)
+    // phase B, stage 1 on row i: z face i+1, predictor P(i) (also to shared memory) and H(i)
     auto stage1 = [&]() {
-        const float2 back = zfwd, back2 = zfwd2;
-        zfwd = sub2(f2, f1);
-        zfwd2 = __fadd2_rn(zfwd, zfwd);
-        const float2 gz_p = __ffma2_rn(hz, superbee_diff2(back, back2, zfwd, zfwd2), f1);
-        const float2 dz = __fmul2_rn(wrz, dnz ? sub2(gz_p, gz_0) : sub2(gz_0, gz_m));
-        gz_m = gz_0;
-        gz_0 = gz_p;
-        const float2 d = __fadd2_rn(__fmul2_rn(wry, sub2(GF[ghi], GF[glo])), dz);
-        p2 = max_lo2(__ffma2_rn(ndt, d, f0), lo);
-        h2 = __ffma2_rn(nhdt, d, f0);
-        if (act) Pr[pslot * RS + own] = p2;
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            StreamPair& P = S[k];
+            const float2 back = P.zfwd, back2 = P.zfwd2;
+            P.zfwd = sub2(P.f2, P.f1);
+            P.zfwd2 = __fadd2_rn(P.zfwd, P.zfwd);
+            const float2 gz_p = __ffma2_rn(P.hz, superbee_diff2(back, back2, P.zfwd, P.zfwd2), P.f1);
+            const float2 dz = __fmul2_rn(P.wrz, P.dnz ? sub2(gz_p, P.gz_0) : sub2(P.gz_0, P.gz_m));
+            P.gz_m = P.gz_0;
+            P.gz_0 = gz_p;
+            const float2 d = __fadd2_rn(__fmul2_rn(P.wry, sub2(GF[P.ghi], GF[P.glo])), dz);
+            P.p2 = max_lo2(__ffma2_rn(ndt, d, P.f0), lo);
+            P.h2 = __ffma2_rn(nhdt, d, P.f0);
+            Pr[pslot * RS + P.own] = P.p2;
+        }
     };
     // phase B, stage 2 on row j: z face j+1 from P rows j .. j+2, the output row
     auto stage2 = [&]() {
-        const float2 back = pfwd, back2 = pfwd2;
-        pfwd = sub2(p2, p1);
-        pfwd2 = __fadd2_rn(pfwd, pfwd);
-        const float2 gp_p = __ffma2_rn(hz, superbee_diff2(back, back2, pfwd, pfwd2), p1);
-        const float2 dzp = __fmul2_rn(wrz, dnz ? sub2(gp_p, pz_0) : sub2(pz_0, pz_m));
-        pz_m = pz_0;
-        pz_0 = gp_p;
-        const float2 t = __ffma2_rn(nhdt, __fmul2_rn(wry, sub2(GP[ghi], GP[glo])), h0);
-        const float2 v = max_lo2(__ffma2_rn(nhdt, dzp, t), lo);
-        if (ok1) *reinterpret_cast<float2*>(orow) = v;
-        else if (ok0) *orow = v.x;
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            StreamPair& P = S[k];
+            const float2 back = P.pfwd, back2 = P.pfwd2;
+            P.pfwd = sub2(P.p2, P.p1);
+            P.pfwd2 = __fadd2_rn(P.pfwd, P.pfwd);
+            const float2 gp_p = __ffma2_rn(P.hz, superbee_diff2(back, back2, P.pfwd, P.pfwd2), P.p1);
+            const float2 dzp = __fmul2_rn(P.wrz, P.dnz ? sub2(gp_p, P.pz_0) : sub2(P.pz_0, P.pz_m));
+            P.pz_m = P.pz_0;
+            P.pz_0 = gp_p;
+            const float2 t = __ffma2_rn(nhdt, __fmul2_rn(P.wry, sub2(GP[P.ghi], GP[P.glo])), P.h0);
+            const float2 v = max_lo2(__ffma2_rn(nhdt, dzp, t), lo);
+            float* o = orow + 2 * (h + 2 * k);  // pair h + 2k: angles a0 + 2h + 4k, a0 + 2h + 4k + 1
+            if (P.ok1) *reinterpret_cast<float2*>(o) = v;
+            else if (P.ok0) *o = v.x;
+        }
         orow += zs;
     };
     auto slide = [&]() {  // P rows j+1 .. i, H rows i-1 .. i, F rows i+1 .. i+2
-        p0 = p1;
-        p1 = p2;
-        h0 = h1;
-        h1 = h2;
-        f0 = f1;
-        f1 = f2;
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            StreamPair& P = S[k];
+            P.p0 = P.p1;
+            P.p1 = P.p2;
+            P.h0 = P.h1;
+            P.h1 = P.h2;
+            P.f0 = P.f1;
+            P.f1 = P.f2;
+        }
         slot = (slot + 1) & (RF - 1);
         pslot = (pslot + 1) & (RP - 1);
     };
@@ -1410,25 +1503,36 @@ __device__ __forceinline__ void transport_stream_body(const TransportArgs<float>
     for (int r = 0; r < PD + 2; ++r) fill(r);
     // rows 0 and 1: stage 1 only
     top();
-    f0 = Fr[own];
-    f1 = Fr[(min(1, Nz) & (RF - 1)) * RS + own];
-    gz_m = gz_0 = f0;  // faces -1 and 0 of a clamped column: the edge value
-    zfwd = sub2(f1, f0);
-    zfwd2 = __fadd2_rn(zfwd, zfwd);
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        StreamPair& P = S[k];
+        P.f0 = Fr[P.own];
+        P.f1 = Fr[(min(1, Nz) & (RF - 1)) * RS + P.own];
+        P.gz_m = P.gz_0 = P.f0;  // faces -1 and 0 of a clamped column: the edge value
+        P.zfwd = sub2(P.f1, P.f0);
+        P.zfwd2 = __fadd2_rn(P.zfwd, P.zfwd);
+    }
     for (int i = 0; i < 2; ++i) {
         if (i > 0) top();
         phase_a(i, i <= Nz, false);
         __syncthreads();  // faces published; row i of F is free for the copy of row i+PD+2
         fill(i + PD + 2);
         if (i <= Nz) stage1();
-        else p2 = p1;
+        else {
+#pragma unroll
+            for (int k = 0; k < 2; ++k) S[k].p2 = S[k].p1;
+        }
         slide();
     }
-    pz_m = pz_0 = p0;  // P rows 0 and 1 known: start the z-walk of P
-    pfwd = sub2(p1, p0);
-    pfwd2 = __fadd2_rn(pfwd, pfwd);
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {  // P rows 0 and 1 known: start the z-walk of P
+        StreamPair& P = S[k];
+        P.pz_m = P.pz_0 = P.p0;
+        P.pfwd = sub2(P.p1, P.p0);
+        P.pfwd2 = __fadd2_rn(P.pfwd, P.pfwd);
+    }
     // rows 2 .. Nz: both stages
-#pragma unroll 2
+#pragma unroll 1
     for (int i = 2; i <= Nz; ++i) {
         top();
         phase_a(i, true, true);
@@ -1443,25 +1547,26 @@ __device__ __forceinline__ void transport_stream_body(const TransportArgs<float>
         top();
         phase_a(i, false, true);
         __syncthreads();
-        p2 = p1;  // rows past the plane repeat the last predictor row
+#pragma unroll
+        for (int k = 0; k < 2; ++k) S[k].p2 = S[k].p1;  // rows past the plane repeat the last predictor row
         stage2();
         slide();
     }
     asm volatile("cp.async.wait_group 0;" ::: "memory");
 }
 
-__global__ void __maxnreg__(80) transport_stream_kernel(TransportArgs<float> a, int n_chunks) {
+__global__ void __maxnreg__(128) transport_stream_kernel(TransportArgs<float> a, int n_chunks) {
     transport_stream_body(a, n_chunks, blockIdx.x);
 }
 
-__global__ void __maxnreg__(80) transport_stream_slots_kernel(const TransportArgs<float>* __restrict__ args,
+__global__ void __maxnreg__(128) transport_stream_slots_kernel(const TransportArgs<float>* __restrict__ args,
                                                                       const int* __restrict__ begin, int nslots,
                                                                       int n_chunks) {
     const int s = find_slot(begin, nslots, blockIdx.x);
     transport_stream_body(args[s], n_chunks, blockIdx.x - __ldg(begin + s));
 }
 
-int transport_stream_threads(int Ny) { return ((Ny + 1) * kStreamPairs + 31) / 32 * 32; }
+int transport_stream_threads(int Ny) { return (Ny + 1) * 2; }
 
 bool transport_stream_supported(int Ny, int NA) {
     return NA % 2 == 0 && transport_stream_threads(Ny) <= kStreamMaxThreads &&

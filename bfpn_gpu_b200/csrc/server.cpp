@@ -94,7 +94,8 @@ struct bfpn_server {
     bool batching = true;
     std::vector<std::thread> workers;
     std::vector<std::thread> schedulers;
-    std::vector<int> busy_per_device;  // indexed by position in `devices`
+    std::vector<int> busy_per_device;     // context-worker jobs running, by position in `devices`
+    std::vector<int> bundled_per_device;  // bundle jobs running, same index
     std::vector<int32_t> devices;
 };
 
@@ -112,8 +113,21 @@ void run_job(bfpn_server* s, int dev_slot, Job& j, bfpn_ctx*& ctx, Job& ctx_shap
         ctx = nullptr;
     }
     if (!ctx) {
-        // another worker on this device may hold the memory this beam needs:
-        // retry while any of them is busy, fail once the device is idle
+        // admission by footprint: wait while the beam does not fit in free
+        // memory and other work on this device may still free some; then
+        // create, and on OOM retry the same way (another worker may have
+        // allocated in between); fail once nothing else runs
+        uint64_t need = 0;
+        if (bfpn_footprint_bytes(&j.grid, &j.phys, j.precision, &need) == BFPN_OK) {
+            for (;;) {
+                uint64_t free_b = 0;
+                if (bfpn_device_memory(device, &free_b, nullptr) != BFPN_OK || need + (512ull << 20) <= free_b) break;
+                std::unique_lock<std::mutex> lk(s->mu);
+                const bool others = s->busy_per_device[dev_slot] > 1 || s->bundled_per_device[dev_slot] > 0;
+                if (!others || s->stopping) break;  // let bfpn_create report it
+                s->cv_done.wait_for(lk, std::chrono::milliseconds(50));
+            }
+        }
         for (;;) {
             bfpn_status st = bfpn_create(&j.grid, &j.phys, j.precision, device, &ctx);
             if (st == BFPN_OK) break;
@@ -190,9 +204,11 @@ struct LiveBundle {
     double ms_per_step = 1.0;                     // running estimate (host clock, concurrent rounds)
 };
 
-void finish(bfpn_server* s, const std::shared_ptr<Job>& j, bfpn_status st, const std::string& err) {
+void finish(bfpn_server* s, const std::shared_ptr<Job>& j, bfpn_status st, const std::string& err,
+            int dev_slot = -1) {
     {
         std::lock_guard<std::mutex> lk(s->mu);
+        if (dev_slot >= 0) s->bundled_per_device[dev_slot]--;  // a running bundle job ends
         j->status = st;
         if (st != BFPN_OK) j->error = err;
         j->finished = Clock::now();
@@ -240,6 +256,7 @@ void scheduler_main(bfpn_server* s, int dev_slot) {
                     std::lock_guard<std::mutex> lk(s->mu);
                     j->started = Clock::now();
                     j->device = device;
+                    s->bundled_per_device[dev_slot]++;
                 }
                 lb.slots[slot] = j;
                 any_running = true;
@@ -272,7 +289,7 @@ void scheduler_main(bfpn_server* s, int dev_slot) {
             bfpn_status st = bfpn_bundle_step(lb.b, n);
             if (st != BFPN_OK) {
                 const std::string err = std::string("bundle step: ") + bfpn_bundle_last_error(lb.b);
-                for (auto& sj : lb.slots) finish(s, sj.second, st, err);
+                for (auto& sj : lb.slots) finish(s, sj.second, st, err, dev_slot);
                 lb.slots.clear();
                 bfpn_bundle_destroy(lb.b);
                 lb.b = nullptr;
@@ -299,7 +316,7 @@ void scheduler_main(bfpn_server* s, int dev_slot) {
                     j->proxy.assign(static_cast<size_t>(j->nsteps), 0.0);
                     cs = bfpn_bundle_collect(lb->b, it->first, j->idd.data(), j->proxy.data(), j->nsteps);
                 }
-                finish(s, j, cs, std::string("bundle: ") + bfpn_bundle_last_error(lb->b));
+                finish(s, j, cs, std::string("bundle: ") + bfpn_bundle_last_error(lb->b), dev_slot);
                 it = lb->slots.erase(it);
             }
             if (st != BFPN_OK) {  // the bundle's state is suspect: drop it
@@ -341,6 +358,7 @@ bfpn_status bfpn_server_create(const int32_t* devices, int32_t n_devices, int32_
     auto* s = new bfpn_server();
     s->devices = devs;
     s->busy_per_device.assign(devs.size(), 0);
+    s->bundled_per_device.assign(devs.size(), 0);
     for (size_t k = 0; k < devs.size(); ++k) {
         for (int w = 0; w < workers_per_device; ++w) s->workers.emplace_back(worker_main, s, static_cast<int>(k));
         s->schedulers.emplace_back(scheduler_main, s, static_cast<int>(k));

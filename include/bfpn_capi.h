@@ -144,7 +144,8 @@ bfpn_status bfpn_host_table(const bfpn_grid* grid, const bfpn_phys* phys, const 
                             uint64_t* n_out);
 
 /* Device bytes a context of this shape needs (state, source, work buffers,
- * tables).  Replaces the reference's preflightMemory estimate
+ * tables; in mixed precision also the tensor-core source's operand buffers
+ * at their largest).  Replaces the reference's preflightMemory estimate
  * (bfpm_solver.cu:1321-1433).  Pure host arithmetic; no GPU needed. */
 bfpn_status bfpn_footprint_bytes(const bfpn_grid* grid, const bfpn_phys* phys,
                                  int precision, uint64_t* bytes);
@@ -284,7 +285,7 @@ int32_t bfpn_source_groups(bfpn_ctx* ctx);
  *   every bfpn_step / bfpn_step_async call still ends on whole steps.  Same
  *   kernels on the same inputs: the same values.
  * BFPN_OPT_STREAM_TRANSPORT: 1 (default) runs the mixed-precision transport
- *   of planes without a whole-plane kernel (Ny + 1 <= 128, any Nz, paired
+ *   of planes without a whole-plane kernel (Ny + 1 <= 256, any Nz, paired
  *   angles) with the row-streaming kernel: one block per (group, 8-angle)
  *   plane walks the z rows, the z-stencil in registers and one row of the
  *   y-stencil in shared memory, in place; 2 also uses it where a whole-plane
@@ -488,6 +489,9 @@ bfpn_status bfpn_idd_noalloc(const bfpn_grid* grid, int32_t precision, int32_t t
 
 /* ---- devices (printGPUInfo, main.cu:25-42) ---------------------------- */
 int32_t bfpn_device_count(void);
+/* Free and total device memory of a device (cudaMemGetInfo with that device
+ * current; the caller's current device is left as it was). */
+bfpn_status bfpn_device_memory(int32_t device, uint64_t* free_bytes, uint64_t* total_bytes);
 /* One line per device property in the reference's format; returns the number
  * of bytes written (excluding the terminating zero), or -1. */
 int32_t bfpn_device_info(int32_t device, char* buf, int32_t buf_len);

@@ -104,7 +104,7 @@ def test_footprint_scales_with_grid_and_precision():
     b32 = capi.footprint_bytes(c2.grid(), c2.phys(), capi.PREC_MIXED)
     cells = c2.cells()
     assert 8 * cells * 8 <= b64 < 8 * cells * 8 * 1.5
-    assert 0.45 < b32 / b64 < 0.55
+    assert 0.5 < b32 / b64 < 0.8  # half the state bytes plus the tensor-core source's operand buffers
     bad = make_config(ny=0)
     with pytest.raises(capi.BfpnError):
         capi.footprint_bytes(bad.grid(), bad.phys())
