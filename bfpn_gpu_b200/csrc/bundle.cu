@@ -514,6 +514,8 @@ bfpn_status bfpn_bundle_admit(bfpn_bundle* b, const bfpn_beam* beam, int32_t* sl
     if ((st = bfpn_init_beam(c)) != BFPN_OK) return undo(st, bfpn_last_error(c));
     const std::string why = bundle_ready(c);
     if (!why.empty()) return undo(BFPN_INVALID_ARG, why);
+    // a beam whose tensor-core source buffers did not fit waits for memory like one that does not fit at all
+    if (!bundle_tc_source(c)) return undo(BFPN_OOM, "no room for the tensor-core source buffers");
     const std::string key = bundle_class_key(c);
     const int mode = (c->p.flags & BFPN_FLAG_EQ15_STRAGGLING) ? EMODE_EQ15_STRAG : EMODE_EQ15;
     const bool no_clip = (c->p.flags & BFPN_FLAG_NO_SPATIAL_CLIPPING) != 0;

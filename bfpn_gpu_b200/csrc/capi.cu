@@ -1963,6 +1963,10 @@ std::string bundle_ready(const bfpn_ctx* c) {
     return "";
 }
 
+bool bundle_tc_source(const bfpn_ctx* c) {
+    return c && (c->n_groups == 0 || (c->use_umma && c->ablob && c->bblob && c->eblob));
+}
+
 EnergyArgs<float> bundle_energy_args(bfpn_ctx* c, int species, bool with_source, double* partials) {
     EnergyArgs<float> a;
     a.F = as<float>(c->st[species][0]);

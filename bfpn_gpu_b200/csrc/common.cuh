@@ -137,6 +137,13 @@ struct IddFinalArgs {
 };
 
 // Float state only.  args / begin are device arrays; blocks = begin[nslots].
+// Dynamic shared memory: raise `func`'s limit, once per device, to the most
+// the device allows a block (never lowered afterwards), and check that `need`
+// fits.  The limit is a process-wide property of the function; setting it per
+// launch to that launch's size let a thread lower it between another
+// thread's capture of a larger launch and that graph's replay.
+cudaError_t allow_dynamic_smem(const void* func, size_t need);
+
 // Energy sweep: ring = the 4-lane ring kernel (lanes % 4 == 0, not legacy),
 // else the register kernel with `block` threads; every slot's grid is that
 // kernel's energy_grid of its lanes.

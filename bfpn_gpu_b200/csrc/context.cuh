@@ -154,6 +154,10 @@ namespace bfpn {
 // Per-slot pieces of a depth step, for bundle.cu (capi.cu).  Float state.
 // A context qualifies for a bundle when bundle_ready is empty.
 std::string bundle_ready(const bfpn_ctx* c);
+// The slot's secondary source runs on the tensor-core kernels (its operand
+// buffers were allocated); a context that fell back to the CUDA-core source
+// for lack of memory does not enter a bundle.
+bool bundle_tc_source(const bfpn_ctx* c);
 EnergyArgs<float> bundle_energy_args(bfpn_ctx* c, int species, bool with_source, double* partials);
 TransportArgs<float> bundle_transport_args(bfpn_ctx* c, int species, int coef, bool preserve_sign);
 AngleArgs<float> bundle_angle_args(bfpn_ctx* c, int species, int coef, int* err);

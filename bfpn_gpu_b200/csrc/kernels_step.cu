@@ -14,8 +14,34 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <type_traits>
+#include <utility>
 
 namespace bfpn {
+
+cudaError_t allow_dynamic_smem(const void* func, size_t need) {
+    static std::mutex m;
+    static std::map<std::pair<const void*, int>, size_t> limit;  // (function, device) -> bytes allowed
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(m);
+    auto it = limit.find({func, dev});
+    if (it == limit.end()) {
+        cudaFuncAttributes fa{};
+        int optin = 0;
+        if ((e = cudaFuncGetAttributes(&fa, func)) != cudaSuccess) return e;
+        if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev)) != cudaSuccess) return e;
+        const size_t allow = optin > static_cast<int>(fa.sharedSizeBytes) ? optin - fa.sharedSizeBytes : 0;
+        if ((e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(allow))) !=
+            cudaSuccess)
+            return e;
+        it = limit.emplace(std::make_pair(func, dev), allow).first;
+    }
+    return need <= it->second ? cudaSuccess : cudaErrorInvalidValue;
+}
 
 template <typename T>
 cudaError_t launch_angle_generic(const AngleArgs<T>& a, cudaStream_t s);
@@ -672,7 +698,7 @@ static cudaError_t launch_transport_ac(const TransportArgs<T>& a, cudaStream_t s
     const int n_chunks = (a.NA + AC - 1) / AC;
     const size_t smem = transport_smem(Ny1, Nz1, a.tile_y, a.tile_z, AC, sizeof(T));
     auto kern = transport_kernel<T, AC>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    cudaError_t e = allow_dynamic_smem(reinterpret_cast<const void*>(kern), smem);
     if (e != cudaSuccess) return e;
     const long long blocks = static_cast<long long>(a.Ng) * n_chunks * tiles_y * tiles_z;
     if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
@@ -1330,28 +1356,38 @@ __global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(ClusterPlane<NP, CL
 // ---------------------------------------------------------------------------
 constexpr int kStreamPairs = 4;            // angle pairs per block (8 angles, 32 bytes per position)
 constexpr int kStreamRing = 8;             // rows of F in the shared-memory ring
-constexpr int kStreamAhead = 4;            // rows copied ahead of the one a row's z-stencil needs
+constexpr int kStreamAhead = 5;            // rows copied ahead of the one a row's z-stencil needs
 constexpr int kStreamPRows = 4;            // rows of P kept in shared memory (rows i-2 .. i)
-constexpr int kStreamMaxThreads = 512;     // two threads per column: planes up to 256 points wide
+constexpr int kStreamPT = 2;               // angle pairs per thread
+constexpr int kStreamTPC = kStreamPairs / kStreamPT;  // threads per column
+constexpr int kStreamMaxThreads = 256 * kStreamTPC;   // planes up to 256 points wide
+// register cap: two blocks per SM at the 81-point plane either way
+constexpr int kStreamMaxReg = kStreamPT == 2 ? 168 : 88;
 
 size_t transport_stream_smem(int NPy) {
     const size_t row = static_cast<size_t>(NPy) * kStreamPairs * sizeof(float2);
     const size_t grow = static_cast<size_t>(NPy + 3) * kStreamPairs * sizeof(float2);
-    return (kStreamRing + kStreamPRows) * row + 2 * grow;
+    return (kStreamRing + kStreamPRows) * row + 4 * grow;  // face rows of F and P, double-buffered
 }
 
-// One thread per (column y, half h): angle pairs h and h + 2 of the block's
-// four, so the (Ny+1) x 2 threads also copy the row's (Ny+1) x 2 16-byte
-// pieces one each.  The per-pair state lives in a PairState.
+// kStreamTPC threads per column y: thread (y, t) carries angle pairs t,
+// t + kStreamTPC, ... of the block's four; threads t < 2 also copy the row's
+// 16-byte pieces, one each.  The z-stencil of a pair lives in three-slot register
+// rotations indexed by row mod 3; the row loop is unrolled by three so every
+// slot index is a compile-time constant and the rotation costs no moves.
 struct StreamPair {
-    float2 f0, f1, f2, p0, p1, p2, h0, h1, h2;  // F rows i .. i+2, P rows j .. j+2, H rows j .. i (j = i-2)
-    float2 gz_m, gz_0, zfwd, zfwd2;             // z-walk of F: G(i-1), G(i), last difference
-    float2 pz_m, pz_0, pfwd, pfwd2;             // z-walk of P: G(j-1), G(j)
+    float2 f[3];              // F row r in f[r % 3] (rows i .. i+2 at iteration i)
+    float2 p[3], hh[3];       // predictor P and H row r in [r % 3] (rows i-2 .. i)
+    float2 gz[3], zf[3], zf2[3];  // z-walk of F: face value of cell c in gz[c % 3]; F(i+2) - F(i+1) and its double in [i % 3]
+    float2 pz[3], pf[3], pf2[3];  // z-walk of P: face value of cell c in pz[c % 3]; P(i) - P(i-1) and its double in [i % 3]
     float2 wry, wrz, hy, hz;
     bool dnz;
     int own, offl, offr, ghi, glo;              // shared-memory offsets (float2) in a row / a face row
-    bool ok0, ok1;                              // angles of the pair inside NA (output stores)
+    bool ok1, ok_half;                          // both angles of the pair inside NA; only the first
 };
+
+template <int V>
+using IntC = std::integral_constant<int, V>;
 
 __device__ __forceinline__ void transport_stream_body(const TransportArgs<float>& a, int n_chunks, int bid) {
     constexpr int A2 = kStreamPairs, AC = 2 * A2, RF = kStreamRing, PD = kStreamAhead, RP = kStreamPRows;
@@ -1362,23 +1398,24 @@ __device__ __forceinline__ void transport_stream_body(const TransportArgs<float>
     const int GS = (NPy + 2) * A2 + A2;  // one face row: faces -1 .. N+1, then a spare row for edge-less threads
     float2* Fr = reinterpret_cast<float2*>(smem_raw);  // [RF][NPy][A2]
     float2* Pr = Fr + RF * RS;                         // [RP][NPy][A2]
-    float2* GF = Pr + RP * RS;                         // [GS]: G of F's y-walk
-    float2* GP = GF + GS;                              // same for P
+    float2* Gb = Pr + RP * RS;                         // [2][F, P][GS]: G of the y-walks, by row parity
     const int chunk = bid % n_chunks, ek = bid / n_chunks, a0 = chunk * AC;
     const size_t zs = static_cast<size_t>(NPy) * NA;  // one z row in the state
     const size_t base = static_cast<size_t>(ek) * (Nz + 1) * zs + a0;
-    const int tid = threadIdx.x, h = tid & 1, y = tid >> 1;
+    constexpr int PT = kStreamPT, TPC = kStreamTPC;
+    const int tid = threadIdx.x, h = tid % TPC, y = tid / TPC;
 
-    // this thread's 16-byte piece of every row: position y, angles a0 + 4h .. a0 + 4h + 3
+    // this thread's 16-byte piece of every row (threads h < 2): position y, angles a0 + 4h .. a0 + 4h + 3
     const bool vec = NA % 4 == 0;
-    const bool lok = vec && a0 + 4 * h < NA;
+    const bool lcp = h < 2;
+    const bool lok = vec && lcp && a0 + 4 * h < NA;
     const float* in0 = a.in;
-    const float* lsrc = in0 + base + static_cast<size_t>(y) * NA + 4 * h;
-    float* ldst = reinterpret_cast<float*>(Fr) + y * AC + 4 * h;
+    const float* lsrc = in0 + base + static_cast<size_t>(y) * NA + 4 * (h & 1);
+    float* ldst = reinterpret_cast<float*>(Fr) + y * AC + 4 * (h & 1);
     auto fill = [&](int r) {  // row r of F into slot r % RF; one commit group per call, empty past the plane
         if (r <= Nz) {
             if (vec) {
-                cp_async16(ldst + (r & (RF - 1)) * (2 * RS), lok ? lsrc + static_cast<size_t>(r) * zs : in0, lok);
+                if (lcp) cp_async16(ldst + (r & (RF - 1)) * (2 * RS), lok ? lsrc + static_cast<size_t>(r) * zs : in0, lok);
             } else {
                 float* row = reinterpret_cast<float*>(Fr + (r & (RF - 1)) * RS);
                 const float* src = in0 + base + static_cast<size_t>(r) * zs;
@@ -1395,13 +1432,13 @@ __device__ __forceinline__ void transport_stream_body(const TransportArgs<float>
     const float lo = a.preserve_sign ? -INFINITY : 0.f;
     // the face beyond the plane (edge threads) or a spare slot (the others): every thread stores one
     const int gedge_row = y == 0 ? 0 : (y == Ny ? (NPy + 1) * A2 : (NPy + 2) * A2);
-    StreamPair S[2];
+    StreamPair S[PT];
 #pragma unroll
-    for (int k = 0; k < 2; ++k) {
+    for (int k = 0; k < PT; ++k) {
         StreamPair& P = S[k];
-        const int q = h + 2 * k;
-        P.ok0 = a0 + 2 * q < NA;
+        const int q = h + TPC * k;
         P.ok1 = a0 + 2 * q + 1 < NA;
+        P.ok_half = a0 + 2 * q < NA && !P.ok1;
         const int g0 = min(a0 + 2 * q, NA - 1), g1 = min(a0 + 2 * q + 1, NA - 1);
         const float wy0 = a.omega[2 * g0], wz0 = a.omega[2 * g0 + 1];
         const float wy1 = a.omega[2 * g1], wz1 = a.omega[2 * g1 + 1];
@@ -1417,8 +1454,8 @@ __device__ __forceinline__ void transport_stream_body(const TransportArgs<float>
         // G index of the two faces of this cell's y-divergence (G is stored one face up)
         P.ghi = P.own + (dny ? 2 * A2 : A2);
         P.glo = P.own + (dny ? A2 : 0);
-        P.p0 = P.p1 = P.p2 = P.h0 = P.h1 = P.h2 = make_float2(0.f, 0.f);
-        P.pz_m = P.pz_0 = P.pfwd = P.pfwd2 = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int r = 0; r < 3; ++r) P.p[r] = P.hh[r] = make_float2(0.f, 0.f);
     }
     float* orow = a.out + base + static_cast<size_t>(y) * NA;  // this position's angles a0 .. a0+7, row 0
 
@@ -1427,146 +1464,137 @@ __device__ __forceinline__ void transport_stream_body(const TransportArgs<float>
         G[P.own + A2] = __ffma2_rn(P.hy, superbee_diff2(back, __fadd2_rn(back, back), fwd, __fadd2_rn(fwd, fwd)), x);
         G[gedge_row + (P.own - y * A2)] = x;  // faces beyond the plane equal the edge value
     };
-    int slot = 0, pslot = 0;  // ring slots of row i of F and of P
-
-    // phase A of iteration i: y faces of F row i (stage 1) and P row j = i-2 (stage 2);
-    // f2 = F(min(i+2, Nz)) (row Nz stays in its slot: nothing is copied past the plane)
-    auto phase_a = [&](int i, bool st1, bool st2) {
-        const float2* f2row = Fr + ((slot + min(2, Nz - i)) & (RF - 1)) * RS;
-        const float2* Fi = Fr + slot * RS;
-        const float2* Pj = Pr + ((pslot - 2) & (RP - 1)) * RS;
+    // Iteration i (R = i mod 3).  Phase A: y faces of F row i (stage 1) and of
+    // P row j = i-2 (stage 2) into the face rows of parity i, and F row
+    // min(i+2, Nz) into the rotation (row Nz stays in its ring slot: nothing is
+    // copied past the plane).  Then this thread's copy of row i+3 is waited
+    // for and the block meets once: faces published, F row i+3 and P row i-1
+    // visible.  Phase B: stage 1 on row i (z face of cell i+1, P(i) -- also
+    // to shared memory -- and H(i)), stage 2 on row j (z face of cell j+1 from
+    // P rows j .. i, the output row).  One barrier per row suffices: a face
+    // row of parity i is rewritten only at iteration i+2, after every thread
+    // has passed barrier i+1 and so finished iteration i; the F slot refilled
+    // at iteration i held row i-2 and the P slot written held row i-4, both
+    // last read before barrier i-1.  A row of F past the plane is not walked:
+    // P(i) repeats the last predictor row.  FILL: issue the copy of row
+    // i+PD+2 (every iteration that walks F).
+    auto iter = [&](auto Rc, auto S1c, auto S2c, auto FILLc, int i) {
+        constexpr int R = decltype(Rc)::value, R1 = (R + 1) % 3, R2 = (R + 2) % 3;
+        constexpr bool st1 = decltype(S1c)::value != 0, st2 = decltype(S2c)::value != 0;
+        constexpr bool do_fill = decltype(FILLc)::value != 0;
+        float2* GF = Gb + (i & 1) * (2 * GS);
+        float2* GP = GF + GS;
+        const float2* Fi = Fr + (i & (RF - 1)) * RS;
+        const float2* f2row = Fr + ((i + min(2, Nz - i)) & (RF - 1)) * RS;
+        const float2* Pj = Pr + ((i - 2) & (RP - 1)) * RS;
 #pragma unroll
-        for (int k = 0; k < 2; ++k) {
+        for (int k = 0; k < PT; ++k) {
             StreamPair& P = S[k];
-            P.f2 = f2row[P.own];
-            if (st1) y_face(GF, Fi, P, P.f0);
-            if (st2) y_face(GP, Pj, P, P.p0);
+            if (st1) {
+                P.f[R2] = f2row[P.own];
+                y_face(GF, Fi, P, P.f[R]);
+            }
+            if (st2) y_face(GP, Pj, P, P.p[R1]);
         }
-    };
-    // phase B, stage 1 on row i: z face i+1, predictor P(i) (also to shared memory) and H(i)
-    auto stage1 = [&]() {
+        asm volatile("cp.async.wait_group %0;" ::"n"(PD - 2) : "memory");  // row i+3 of F landed
+        __syncthreads();
+        if (do_fill) fill(i + PD + 2);
+        float2* Pw = Pr + (i & (RP - 1)) * RS;
 #pragma unroll
-        for (int k = 0; k < 2; ++k) {
+        for (int k = 0; k < PT; ++k) {
             StreamPair& P = S[k];
-            const float2 back = P.zfwd, back2 = P.zfwd2;
-            P.zfwd = sub2(P.f2, P.f1);
-            P.zfwd2 = __fadd2_rn(P.zfwd, P.zfwd);
-            const float2 gz_p = __ffma2_rn(P.hz, superbee_diff2(back, back2, P.zfwd, P.zfwd2), P.f1);
-            const float2 dz = __fmul2_rn(P.wrz, P.dnz ? sub2(gz_p, P.gz_0) : sub2(P.gz_0, P.gz_m));
-            P.gz_m = P.gz_0;
-            P.gz_0 = gz_p;
-            const float2 d = __fadd2_rn(__fmul2_rn(P.wry, sub2(GF[P.ghi], GF[P.glo])), dz);
-            P.p2 = max_lo2(__ffma2_rn(ndt, d, P.f0), lo);
-            P.h2 = __ffma2_rn(nhdt, d, P.f0);
-            Pr[pslot * RS + P.own] = P.p2;
+            if (st1) {
+                const float2 back = P.zf[R2], back2 = P.zf2[R2];
+                P.zf[R] = sub2(P.f[R2], P.f[R1]);
+                P.zf2[R] = __fadd2_rn(P.zf[R], P.zf[R]);
+                const float2 gz_p = __ffma2_rn(P.hz, superbee_diff2(back, back2, P.zf[R], P.zf2[R]), P.f[R1]);
+                const float2 dz = __fmul2_rn(P.wrz, P.dnz ? sub2(gz_p, P.gz[R]) : sub2(P.gz[R], P.gz[R2]));
+                P.gz[R1] = gz_p;
+                const float2 d = __fadd2_rn(__fmul2_rn(P.wry, sub2(GF[P.ghi], GF[P.glo])), dz);
+                P.p[R] = max_lo2(__ffma2_rn(ndt, d, P.f[R]), lo);
+                P.hh[R] = __ffma2_rn(nhdt, d, P.f[R]);
+                Pw[P.own] = P.p[R];
+            } else {
+                P.p[R] = P.p[R2];
+            }
         }
-    };
-    // phase B, stage 2 on row j: z face j+1 from P rows j .. j+2, the output row
-    auto stage2 = [&]() {
+        if (st2) {
 #pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            StreamPair& P = S[k];
-            const float2 back = P.pfwd, back2 = P.pfwd2;
-            P.pfwd = sub2(P.p2, P.p1);
-            P.pfwd2 = __fadd2_rn(P.pfwd, P.pfwd);
-            const float2 gp_p = __ffma2_rn(P.hz, superbee_diff2(back, back2, P.pfwd, P.pfwd2), P.p1);
-            const float2 dzp = __fmul2_rn(P.wrz, P.dnz ? sub2(gp_p, P.pz_0) : sub2(P.pz_0, P.pz_m));
-            P.pz_m = P.pz_0;
-            P.pz_0 = gp_p;
-            const float2 t = __ffma2_rn(nhdt, __fmul2_rn(P.wry, sub2(GP[P.ghi], GP[P.glo])), P.h0);
-            const float2 v = max_lo2(__ffma2_rn(nhdt, dzp, t), lo);
-            float* o = orow + 2 * (h + 2 * k);  // pair h + 2k: angles a0 + 2h + 4k, a0 + 2h + 4k + 1
-            if (P.ok1) *reinterpret_cast<float2*>(o) = v;
-            else if (P.ok0) *o = v.x;
+            for (int k = 0; k < PT; ++k) {
+                StreamPair& P = S[k];
+                const float2 back = P.pf[R2], back2 = P.pf2[R2];
+                P.pf[R] = sub2(P.p[R], P.p[R2]);
+                P.pf2[R] = __fadd2_rn(P.pf[R], P.pf[R]);
+                const float2 gp_p = __ffma2_rn(P.hz, superbee_diff2(back, back2, P.pf[R], P.pf2[R]), P.p[R2]);
+                const float2 dzp = __fmul2_rn(P.wrz, P.dnz ? sub2(gp_p, P.pz[R1]) : sub2(P.pz[R1], P.pz[R]));
+                P.pz[R2] = gp_p;
+                const float2 t = __ffma2_rn(nhdt, __fmul2_rn(P.wry, sub2(GP[P.ghi], GP[P.glo])), P.hh[R1]);
+                const float2 v = max_lo2(__ffma2_rn(nhdt, dzp, t), lo);
+                float* o = orow + 2 * (h + TPC * k);  // pair h + TPC k
+                if (P.ok1) *reinterpret_cast<float2*>(o) = v;
+                if (P.ok_half) *o = v.x;
+            }
+            orow += zs;
         }
-        orow += zs;
-    };
-    auto slide = [&]() {  // P rows j+1 .. i, H rows i-1 .. i, F rows i+1 .. i+2
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            StreamPair& P = S[k];
-            P.p0 = P.p1;
-            P.p1 = P.p2;
-            P.h0 = P.h1;
-            P.h1 = P.h2;
-            P.f0 = P.f1;
-            P.f1 = P.f2;
-        }
-        slot = (slot + 1) & (RF - 1);
-        pslot = (pslot + 1) & (RP - 1);
-    };
-    auto top = [&]() {
-        asm volatile("cp.async.wait_group %0;" ::"n"(PD - 1) : "memory");
-        __syncthreads();  // row i+2 of F, row i-1 of P and last iteration's face reads are done
     };
 
     for (int r = 0; r < PD + 2; ++r) fill(r);
-    // rows 0 and 1: stage 1 only
-    top();
+    // rows 0 and 1: stage 1 only (row 1 is past a one-row plane when Nz = 0)
+    asm volatile("cp.async.wait_group %0;" ::"n"(PD - 1) : "memory");  // rows 0 .. 2 landed
+    __syncthreads();
 #pragma unroll
-    for (int k = 0; k < 2; ++k) {
+    for (int k = 0; k < PT; ++k) {
         StreamPair& P = S[k];
-        P.f0 = Fr[P.own];
-        P.f1 = Fr[(min(1, Nz) & (RF - 1)) * RS + P.own];
-        P.gz_m = P.gz_0 = P.f0;  // faces -1 and 0 of a clamped column: the edge value
-        P.zfwd = sub2(P.f1, P.f0);
-        P.zfwd2 = __fadd2_rn(P.zfwd, P.zfwd);
+        P.f[0] = Fr[P.own];
+        P.f[1] = Fr[(min(1, Nz) & (RF - 1)) * RS + P.own];
+        P.gz[2] = P.gz[0] = P.f[0];  // faces of cells -1 and 0 of a clamped column: the edge value
+        P.zf[2] = sub2(P.f[1], P.f[0]);
+        P.zf2[2] = __fadd2_rn(P.zf[2], P.zf[2]);
     }
-    for (int i = 0; i < 2; ++i) {
-        if (i > 0) top();
-        phase_a(i, i <= Nz, false);
-        __syncthreads();  // faces published; row i of F is free for the copy of row i+PD+2
-        fill(i + PD + 2);
-        if (i <= Nz) stage1();
-        else {
+    iter(IntC<0>(), IntC<1>(), IntC<0>(), IntC<1>(), 0);
+    if (Nz >= 1) iter(IntC<1>(), IntC<1>(), IntC<0>(), IntC<1>(), 1);
+    else iter(IntC<1>(), IntC<0>(), IntC<0>(), IntC<1>(), 1);
 #pragma unroll
-            for (int k = 0; k < 2; ++k) S[k].p2 = S[k].p1;
-        }
-        slide();
-    }
-#pragma unroll
-    for (int k = 0; k < 2; ++k) {  // P rows 0 and 1 known: start the z-walk of P
+    for (int k = 0; k < PT; ++k) {  // P rows 0 and 1 known: start the z-walk of P
         StreamPair& P = S[k];
-        P.pz_m = P.pz_0 = P.p0;
-        P.pfwd = sub2(P.p1, P.p0);
-        P.pfwd2 = __fadd2_rn(P.pfwd, P.pfwd);
+        P.pz[2] = P.pz[0] = P.p[0];  // faces of cells -1 and 0
+        P.pf[1] = sub2(P.p[1], P.p[0]);
+        P.pf2[1] = __fadd2_rn(P.pf[1], P.pf[1]);
     }
-    // rows 2 .. Nz: both stages
+    // rows 2 .. Nz: both stages, three rows per trip so the rotations stay in place
+    int i = 2;
+    if (i <= Nz) iter(IntC<2>(), IntC<1>(), IntC<1>(), IntC<1>(), i++);
 #pragma unroll 1
-    for (int i = 2; i <= Nz; ++i) {
-        top();
-        phase_a(i, true, true);
-        __syncthreads();
-        fill(i + PD + 2);
-        stage1();
-        stage2();
-        slide();
+    for (; i + 2 <= Nz; i += 3) {
+        iter(IntC<0>(), IntC<1>(), IntC<1>(), IntC<1>(), i);
+        iter(IntC<1>(), IntC<1>(), IntC<1>(), IntC<1>(), i + 1);
+        iter(IntC<2>(), IntC<1>(), IntC<1>(), IntC<1>(), i + 2);
     }
-    // rows past the plane: stage 2 only
-    for (int i = max(Nz + 1, 2); i <= Nz + 2; ++i) {
-        top();
-        phase_a(i, false, true);
-        __syncthreads();
-#pragma unroll
-        for (int k = 0; k < 2; ++k) S[k].p2 = S[k].p1;  // rows past the plane repeat the last predictor row
-        stage2();
-        slide();
+    if (i <= Nz) iter(IntC<0>(), IntC<1>(), IntC<1>(), IntC<1>(), i++);
+    if (i <= Nz) iter(IntC<1>(), IntC<1>(), IntC<1>(), IntC<1>(), i++);
+    // rows past the plane: stage 2 only (the rows' phase is known only at run time)
+    for (; i <= Nz + 2; ++i) {
+        switch (i % 3) {
+            case 0: iter(IntC<0>(), IntC<0>(), IntC<1>(), IntC<0>(), i); break;
+            case 1: iter(IntC<1>(), IntC<0>(), IntC<1>(), IntC<0>(), i); break;
+            default: iter(IntC<2>(), IntC<0>(), IntC<1>(), IntC<0>(), i); break;
+        }
     }
     asm volatile("cp.async.wait_group 0;" ::: "memory");
 }
 
-__global__ void __maxnreg__(128) transport_stream_kernel(TransportArgs<float> a, int n_chunks) {
+__global__ void __maxnreg__(kStreamMaxReg) transport_stream_kernel(TransportArgs<float> a, int n_chunks) {
     transport_stream_body(a, n_chunks, blockIdx.x);
 }
 
-__global__ void __maxnreg__(128) transport_stream_slots_kernel(const TransportArgs<float>* __restrict__ args,
+__global__ void __maxnreg__(kStreamMaxReg) transport_stream_slots_kernel(const TransportArgs<float>* __restrict__ args,
                                                                       const int* __restrict__ begin, int nslots,
                                                                       int n_chunks) {
     const int s = find_slot(begin, nslots, blockIdx.x);
     transport_stream_body(args[s], n_chunks, blockIdx.x - __ldg(begin + s));
 }
 
-int transport_stream_threads(int Ny) { return (Ny + 1) * 2; }
+int transport_stream_threads(int Ny) { return (Ny + 1) * kStreamTPC; }
 
 bool transport_stream_supported(int Ny, int NA) {
     return NA % 2 == 0 && transport_stream_threads(Ny) <= kStreamMaxThreads &&
@@ -1577,8 +1605,7 @@ cudaError_t launch_transport_stream(const TransportArgs<float>& a, cudaStream_t 
     if (!a.pairs || !transport_stream_supported(a.Ny, a.NA)) return cudaErrorNotSupported;
     const int n_chunks = (a.NA + 2 * kStreamPairs - 1) / (2 * kStreamPairs);
     const size_t smem = transport_stream_smem(a.Ny + 1);
-    cudaError_t e = cudaFuncSetAttribute(transport_stream_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(smem));
+    cudaError_t e = allow_dynamic_smem(reinterpret_cast<const void*>(transport_stream_kernel), smem);
     if (e != cudaSuccess) return e;
     const long long blocks = static_cast<long long>(a.Ng) * n_chunks;
     if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
@@ -1592,8 +1619,7 @@ cudaError_t launch_transport_stream_slots(const TransportArgs<float>* args, cons
     if (!transport_stream_supported(Ny, NA)) return cudaErrorNotSupported;
     const int n_chunks = (NA + 2 * kStreamPairs - 1) / (2 * kStreamPairs);
     const size_t smem = transport_stream_smem(Ny + 1);
-    cudaError_t e = cudaFuncSetAttribute(transport_stream_slots_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(smem));
+    cudaError_t e = allow_dynamic_smem(reinterpret_cast<const void*>(transport_stream_slots_kernel), smem);
     if (e != cudaSuccess) return e;
     transport_stream_slots_kernel<<<blocks, transport_stream_threads(Ny), smem, s>>>(args, begin, nslots, n_chunks);
     return cudaGetLastError();
@@ -1618,7 +1644,7 @@ static cudaError_t launch_plane_np(const TransportArgs<T>& a, cudaStream_t s) {
     const int n_chunks = (a.NA + AC - 1) / AC;
     const size_t smem = transport_plane_smem(NP, AC, sizeof(T));
     auto kern = transport_plane_kernel<T, NP, AC>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    cudaError_t e = allow_dynamic_smem(reinterpret_cast<const void*>(kern), smem);
     if (e != cudaSuccess) return e;
     const long long blocks = static_cast<long long>(a.Ng) * n_chunks;
     if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
@@ -1768,7 +1794,7 @@ static cudaError_t launch_tile_ac(const TransportArgs<T>& a, cudaStream_t s) {
     const int n_chunks = (a.NA + AC - 1) / AC;
     const size_t smem = transport_tile_smem(R, AC, sizeof(T));
     auto kern = transport_tile_kernel<T, R, AC>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    cudaError_t e = allow_dynamic_smem(reinterpret_cast<const void*>(kern), smem);
     if (e != cudaSuccess) return e;
     const long long blocks = static_cast<long long>(a.Ng) * n_chunks * tiles_y * tiles_z;
     if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
@@ -1810,7 +1836,7 @@ static cudaError_t launch_cluster_np(const TransportArgs<float>& a, cudaStream_t
     using S = ClusterPlane<NP, CL, A2>;
     const int n_chunks = (a.NA + AC - 1) / AC;
     auto kern = transport_cluster_kernel<NP, CL, A2>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::smem));
+    cudaError_t e = allow_dynamic_smem(reinterpret_cast<const void*>(kern), S::smem);
     if (e != cudaSuccess) return e;
     const long long blocks = static_cast<long long>(a.Ng) * n_chunks * CL;
     if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
@@ -1860,7 +1886,7 @@ static cudaError_t launch_plane_f2_np(const TransportArgs<float>& a, cudaStream_
     const int n_chunks = (a.NA + AC - 1) / AC;
     const size_t smem = transport_plane_smem(NP, AC, sizeof(float));
     auto kern = transport_plane_f2_kernel<NP, AC>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    cudaError_t e = allow_dynamic_smem(reinterpret_cast<const void*>(kern), smem);
     if (e != cudaSuccess) return e;
     const long long blocks = static_cast<long long>(a.Ng) * n_chunks;
     if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
@@ -1901,7 +1927,7 @@ static cudaError_t launch_plane_f2_slots(const TransportArgs<float>* args, const
     const int n_chunks = (NA + AC - 1) / AC;
     const size_t smem = transport_plane_smem(NP, AC, sizeof(float));
     auto kern = transport_plane_f2_slots_kernel<NP, AC>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    cudaError_t e = allow_dynamic_smem(reinterpret_cast<const void*>(kern), smem);
     if (e != cudaSuccess) return e;
     kern<<<blocks, (NP * AC / 2 + 31) / 32 * 32, smem, s>>>(args, begin, nslots, n_chunks);
     return cudaGetLastError();
@@ -1915,7 +1941,7 @@ static cudaError_t launch_cluster_slots(const TransportArgs<float>* args, const 
     if (blocks % CL != 0) return cudaErrorInvalidValue;
     const int n_chunks = (NA + AC - 1) / AC;
     auto kern = transport_cluster_slots_kernel<NP, CL, A2>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::smem));
+    cudaError_t e = allow_dynamic_smem(reinterpret_cast<const void*>(kern), S::smem);
     if (e != cudaSuccess) return e;
     kern<<<blocks, S::NT, S::smem, s>>>(args, begin, nslots, n_chunks);
     return cudaGetLastError();
@@ -2513,8 +2539,7 @@ static cudaError_t launch_angle_dst(const AngleArgs<T>& a, cudaStream_t s) {
             const long long tiles2 = (total + SL2 - 1) / SL2;
             const size_t stage = (static_cast<size_t>(SL2) * N * N * 4 + 127) / 128 * 128;
             auto pk = angle_dst_pair_kernel<N, NST>;
-            cudaError_t e = cudaFuncSetAttribute(pk, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 static_cast<int>(NST * stage));
+            cudaError_t e = allow_dynamic_smem(reinterpret_cast<const void*>(pk), NST * stage);
             if (e != cudaSuccess) return e;
             int dev = 0, sms = 0, per_sm = 0;
             if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
@@ -2533,8 +2558,7 @@ static cudaError_t launch_angle_dst(const AngleArgs<T>& a, cudaStream_t s) {
         constexpr int NST = 2;
         const size_t stage = (static_cast<size_t>(SL) * N * N * sizeof(T) + 127) / 128 * 128;
         auto pk = angle_dst_pipe_kernel<N, T, NST>;
-        cudaError_t e = cudaFuncSetAttribute(pk, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             static_cast<int>(NST * stage));
+        cudaError_t e = allow_dynamic_smem(reinterpret_cast<const void*>(pk), NST * stage);
         if (e != cudaSuccess) return e;
         int dev = 0, sms = 0, per_sm = 0;
         if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
@@ -2549,7 +2573,7 @@ static cudaError_t launch_angle_dst(const AngleArgs<T>& a, cudaStream_t s) {
     }
     const size_t smem = (static_cast<size_t>(SL) * N * (N + 1) + 2 * static_cast<size_t>(N) * N) * sizeof(T);
     auto kern = angle_dst_kernel<N, T>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    cudaError_t e = allow_dynamic_smem(reinterpret_cast<const void*>(kern), smem);
     if (e != cudaSuccess) return e;
     AngleArgs<T> b = a;
     b.slices_per_block = SL;
@@ -2588,7 +2612,7 @@ static cudaError_t launch_angle_slots_n(const AngleArgs<float>* args, const int*
     const int SL = angle_slots_tile(N);
     const size_t stage = (static_cast<size_t>(SL) * N * N * 4 + 127) / 128 * 128;
     auto pk = angle_dst_pair_slots_kernel<N, NST>;
-    cudaError_t e = cudaFuncSetAttribute(pk, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(NST * stage));
+    cudaError_t e = allow_dynamic_smem(reinterpret_cast<const void*>(pk), NST * stage);
     if (e != cudaSuccess) return e;
     int dev = 0, sms = 0, per_sm = 0;
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
@@ -2622,7 +2646,7 @@ cudaError_t launch_angle_generic(const AngleArgs<T>& a, cudaStream_t s) {
     const size_t smem = (static_cast<size_t>(a.Nom) * a.Nom + static_cast<size_t>(a.Nmu) * a.Nmu
                          + 2 * static_cast<size_t>(a.slices_per_block) * NA) * sizeof(T);
     auto kern = angle_kernel<T>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    cudaError_t e = allow_dynamic_smem(reinterpret_cast<const void*>(kern), smem);
     if (e != cudaSuccess) return e;
     const long long total = static_cast<long long>(a.Ng) * a.nyz;
     const long long blocks = (total + a.slices_per_block - 1) / a.slices_per_block;

@@ -369,7 +369,7 @@ cudaError_t launch_source_angular_pipe(const float* P1, const float* P2, uint8_t
     // at most two CTAs per SM when each holds 256 tensor-memory columns (512 per SM)
     if (NT > 128) smem = std::max<size_t>(smem, 80 * 1024);
     auto kern = source_angular_umma_pipe_kernel<16>;
-    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    e = allow_dynamic_smem(reinterpret_cast<const void*>(kern), smem);
     if (e != cudaSuccess) return e;
     dim3 grid(n_ntiles, n_mt, n_groups);
     if (grid.y > 65535 || grid.z > 65535) return cudaErrorInvalidConfiguration;
@@ -593,8 +593,7 @@ cudaError_t launch_source_energy_umma(const uint8_t* q, const uint8_t* eblob, co
     a.n_eg = a.nsg;
     a.nst = energy_umma_stages(emax_cols, &a.stage_bytes);
     const size_t smem = energy_umma_smem(emax_cols);
-    cudaError_t e = cudaFuncSetAttribute(source_energy_umma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(smem));
+    cudaError_t e = allow_dynamic_smem(reinterpret_cast<const void*>(source_energy_umma_kernel), smem);
     if (e != cudaSuccess) return e;
     source_energy_umma_kernel<<<static_cast<unsigned>(n_lt * n_et), 128, smem, s>>>(a);
     return cudaGetLastError();

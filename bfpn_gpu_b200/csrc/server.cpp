@@ -262,10 +262,14 @@ void scheduler_main(bfpn_server* s, int dev_slot) {
                 any_running = true;
                 continue;
             }
-            if (st == BFPN_OOM && any_running) {  // wait for running beams to free memory
-                std::lock_guard<std::mutex> lk(s->mu);
-                s->bundle_queue.push_front(j);
-                break;
+            if (st == BFPN_OOM) {
+                // wait for running beams -- bundled, or on this device's context workers -- to free memory
+                std::unique_lock<std::mutex> lk(s->mu);
+                if (any_running || s->busy_per_device[dev_slot] > 0) {
+                    s->bundle_queue.push_front(j);
+                    if (!any_running) s->cv_done.wait_for(lk, std::chrono::milliseconds(50));
+                    break;
+                }
             }
             if (st == BFPN_INVALID_ARG) {  // a bundle cannot hold it after all: a context worker serves it
                 {
