@@ -210,10 +210,15 @@ def job_throughput(world, updates_per_step_per_rank, steps, max_ms):
     return world * updates_per_step_per_rank * steps / (max_ms / 1e3)
 
 
-def kernel_bytes(cls, cells, elem, n_groups, nyz, NA):
+def kernel_bytes(cls, cells, elem, n_groups, nyz, NA, fused=False):
     """Algorithmic bytes (hbm) or flops (tensor) of one launch of a kernel class."""
     if cls == "energy":
-        return "hbm", 4.5 * cells * elem  # F, f read + write; the secondary's two launches also read the source
+        # F, f read + written; the secondary's launches also read the source (2 of the 4 separate passes, 2
+        # of the 3 when the primary's passes are fused)
+        return "hbm", (5.0 if fused else 4.5) * cells * elem
+    if cls == "energy_fused":
+        # F, f read + written once for two half-steps, the source groups' split-bf16 operand written
+        return "hbm", 4.0 * cells * elem + 8.0 * nyz * NA * n_groups
     if cls == "transport":
         return "hbm", 2.0 * cells * elem
     if cls == "angle":
@@ -277,19 +282,20 @@ def run_ours(args):
     # per-kernel device times, eager launches bracketed by CUDA events
     ctx.set_profiling(True)
     ctx.kernel_profile(reset=True)
-    prof_steps = 2
+    prof_steps = 8  # one call: its first step opens and its last closes separately when the passes are fused
     ctx.step(prof_steps, fetch=False)
     prof = ctx.kernel_profile()
     ctx.set_profiling(False)
     nyz = (cfg.ny + 1) * (cfg.nz + 1)
     NA = cfg.nmu * cfg.nom
     n_groups = ctx.source_groups()
+    fused = prof.get("energy_fused", (0.0, 0))[1] > 0
     pk, pk_kind = peaks()
     per_kernel = {}
     for cls, (tot, n) in prof.items():
         if n == 0:
             continue
-        bound, work = kernel_bytes(cls, cells, elem, n_groups, nyz, NA)
+        bound, work = kernel_bytes(cls, cells, elem, n_groups, nyz, NA, fused)
         avg = tot / n
         entry = {"launches_per_step": n / prof_steps, "ms_per_launch": avg, "share": tot / sum(v[0] for v in prof.values())}
         if work > 0:
@@ -299,7 +305,7 @@ def run_ours(args):
                 entry["achieved_TFLOPs"] = work / (avg / 1e3) / 1e12
         per_kernel[cls] = entry
     dom = max(prof.items(), key=lambda kv: kv[1][0])[0]
-    bound, work = kernel_bytes(dom, cells, elem, n_groups, nyz, NA)
+    bound, work = kernel_bytes(dom, cells, elem, n_groups, nyz, NA, fused)
     avg_s = prof[dom][0] / prof[dom][1] / 1e3
     per_cell = NCU_DRAM_BYTES_PER_CELL.get(WORKLOAD_KEY, {}).get(dom) if prec == capi.PREC_MIXED else None
     traffic = per_cell * cells if per_cell and args.ng is None else None  # bytes per launch
@@ -566,7 +572,9 @@ def run_serve(args):
     sweep = []
     for rate in rates:
         arrivals = beams.poisson_arrivals(len(reqs), rate, seed=args.serve_seed + int(rate))
+        print("serve: rate %g/s, %d requests ..." % (rate, len(reqs)), file=sys.stderr, flush=True)
         got, t, lat = _serve(reqs, arrivals)
+        print("serve: rate %g/s done in %.1f s" % (rate, t), file=sys.stderr, flush=True)
         sweep.append({"rate_per_s": rate, "beams_per_s": len(reqs) / t, "makespan_s": t,
                       "latency_ms": {q: float(np.percentile(lat, float(q[1:]))) for q in ("p50", "p99", "p99.9")},
                       "max_idd_diff_vs_alone_rel_to_peak": _max_rel_diff(got, ref)})

@@ -36,9 +36,9 @@ FLAG_LITE_MEMORY = 1 << 13
 FLAG_STREAMING_FULL = 1 << 14
 # run-time options
 (OPT_TENSOR_CORES, OPT_CUDA_GRAPHS, OPT_PLANE_TRANSPORT, OPT_PAIRED_ANGLES, OPT_CLUSTER_TRANSPORT, OPT_LANE_CHUNK,
- OPT_ENERGY_CHUNK, OPT_STEP_OVERLAP, OPT_STREAM_TRANSPORT) = range(9)
+ OPT_ENERGY_CHUNK, OPT_STEP_OVERLAP, OPT_STREAM_TRANSPORT, OPT_FUSED_ENERGY) = range(10)
 # kernel classes of the profile
-KERNEL_CLASSES = ["energy", "transport", "angle", "source_angular", "source_energy", "idd"]
+KERNEL_CLASSES = ["energy", "transport", "angle", "source_angular", "source_energy", "idd", "energy_fused"]
 # tables
 (TABLE_S_S, TABLE_T_C, TABLE_SIG_TRG, TABLE_SIGMA_C, TABLE_EN, TABLE_OMEND, TABLE_KER_E1, TABLE_KER_E2,
  TABLE_KER_V, TABLE_BAND, TABLE_BEAM_YZA, TABLE_BEAM_E) = range(12)

@@ -210,6 +210,10 @@ void drop_graphs(bfpn_ctx* c) {
         if (g) cudaGraphExecDestroy(g);
         g = nullptr;
     }
+    for (auto& g : c->fus_exec) {
+        if (g) cudaGraphExecDestroy(g);
+        g = nullptr;
+    }
 }
 
 void free_all(bfpn_ctx* c) {
@@ -441,7 +445,8 @@ cudaError_t enq_source_on(bfpn_ctx* c, const void* P1, const void* P2, void* S, 
                                               as<const float>(const_cast<void*>(P2)),
                                               static_cast<uint8_t*>(c->ablob), static_cast<const uint8_t*>(c->bblob),
                                               c->groups, c->n_groups, q, c->Ng, c->dev_err, nyz, c->NA,
-                                              c->umma_nt, c->umma_bk, c->umma_ntiles, c->stream, pread);
+                                              c->umma_nt, c->umma_bk, c->umma_ntiles, c->stream, pread,
+                                              !c->src_prepacked);
         });
         if (e != cudaSuccess) return e;
         return prof(c, BFPN_KERNEL_SOURCE_ENERGY, [&] {
@@ -571,20 +576,17 @@ cudaError_t enq_secondary_half(bfpn_ctx* c, const double* partP, cudaEvent_t pre
     return enq_finalize<T>(c, partP, partS, energy_grid(c->per_e, c->energy_block));
 }
 
+// The IDD of a step without a secondary half (step 0, primary-only and
+// energy-only runs): the secondary state's share, as it stands, unless it is
+// known to be zero.
 template <typename T>
-cudaError_t enq_step(bfpn_ctx* c, bool first, bool secondary_zero) {
-    if (c->lite) return enq_lite_step<T>(c);
+cudaError_t enq_first_finalize(bfpn_ctx* c, const double* partP, bool secondary_zero) {
     const unsigned fl = c->p.flags;
-    double* partP = primary_partials(c, c->steps_done);
     double* partS = c->partials + 2 * static_cast<size_t>(c->n_part);
-    cudaError_t e;
-    if ((e = enq_primary_half<T>(c, partP)) != cudaSuccess) return e;
-    const bool secondary = !(fl & (BFPN_FLAG_ENERGY_ONLY | BFPN_FLAG_PRIMARY_ONLY)) && !first;
-    if (secondary) return enq_secondary_half<T>(c, partP, nullptr);
     int nS = 0;
     if (!secondary_zero) {
         nS = idd_partials_grid(c->per_e);
-        e = prof(c, BFPN_KERNEL_IDD, [&] {
+        cudaError_t e = prof(c, BFPN_KERNEL_IDD, [&] {
             return launch_idd_partials<T>(as<const T>(c->st[1][0]), as<const T>(c->st[1][1]), c->dose_coef, c->Ng,
                                           c->per_e, c->NA, c->Ny, c->Nz, (fl & BFPN_FLAG_TRAPEZOIDAL_YZ) ? 1 : 0, 0,
                                           partS, nS, c->stream);
@@ -592,6 +594,18 @@ cudaError_t enq_step(bfpn_ctx* c, bool first, bool secondary_zero) {
         if (e != cudaSuccess) return e;
     }
     return enq_finalize<T>(c, partP, partS, nS);
+}
+
+template <typename T>
+cudaError_t enq_step(bfpn_ctx* c, bool first, bool secondary_zero) {
+    if (c->lite) return enq_lite_step<T>(c);
+    const unsigned fl = c->p.flags;
+    double* partP = primary_partials(c, c->steps_done);
+    cudaError_t e;
+    if ((e = enq_primary_half<T>(c, partP)) != cudaSuccess) return e;
+    const bool secondary = !(fl & (BFPN_FLAG_ENERGY_ONLY | BFPN_FLAG_PRIMARY_ONLY)) && !first;
+    if (secondary) return enq_secondary_half<T>(c, partP, nullptr);
+    return enq_first_finalize<T>(c, partP, secondary_zero);
 }
 
 // Overlapped form of regular steps (one context stream, the secondary half on
@@ -619,6 +633,109 @@ cudaError_t enq_overlap_body(bfpn_ctx* c, int step) {
     if (e != cudaSuccess) return e;
     if ((e = cudaEventRecord(c->ev_join, c->s_sec)) != cudaSuccess) return e;
     return cudaStreamWaitEvent(c->stream, c->ev_join, 0);
+}
+
+// ---- fused primary energy passes --------------------------------------------
+// With the fused kernel (mixed precision, eq15 modes, transport in place) the
+// steps of one bfpn_step call run as
+//   open(n0) | body(n0+1) ... body(n0+k-1) | close(n0+k-1)
+// where open(n) is the primary's opening energy pass and T-A-T of step n;
+// body(n) = [energy_fused_kernel: the closing pass of step n-1 (its IDD
+// partials and the source's operand) with the opening pass of step n, then
+// the primary's T-A-T of step n] on the context stream, beside [the source of
+// step n-1 from that operand (no pack pass), the secondary half of step n-1
+// and its IDD] on s_sec; close(n) is the closing pass and secondary half of
+// the call's last step.  Step 0 has no secondary half: body(1) finalises its
+// IDD on the context stream.  Each kernel applies the unfused order's
+// arithmetic to the same inputs, so every state and IDD partial is the same;
+// a primary energy pass and the pack pass are saved per step.
+bool fused_ok(const bfpn_ctx* c) {
+    const unsigned fl = c->p.flags;
+    if (!c->fuse_energy || !c->overlap || c->prec != BFPN_PREC_MIXED || c->lite || c->ooc ||
+        !transport_in_place(c) || c->energy_block != 128)
+        return false;
+    if (fl & (BFPN_FLAG_ENERGY_ONLY | BFPN_FLAG_PRIMARY_ONLY | BFPN_FLAG_NO_TRANSPORT | BFPN_FLAG_NO_ANGLE |
+              BFPN_FLAG_LEGACY_ENERGY))
+        return false;
+    const int mode = (fl & BFPN_FLAG_EQ15_STRAGGLING) ? EMODE_EQ15_STRAG : EMODE_EQ15;
+    if (!energy_fused_supported(c->per_e, mode, c->NA)) return false;
+    // the secondary's source must read the operand the fused kernel writes
+    return c->n_groups == 0 || (c->use_umma && c->ablob && c->bblob && c->eblob);
+}
+
+cudaError_t enq_energy_fused(bfpn_ctx* c, double* partP) {
+    EnergyFusedArgs A;
+    EnergyArgs<float>& a = A.e;
+    a.F = as<float>(c->st[0][0]);
+    a.f = as<float>(c->st[0][1]);
+    a.src = nullptr;
+    a.coef = c->ecoef_half;
+    a.Ng = c->Ng;
+    a.lanes = c->per_e;
+    a.mode = (c->p.flags & BFPN_FLAG_EQ15_STRAGGLING) ? EMODE_EQ15_STRAG : EMODE_EQ15;
+    a.partials = partP;
+    a.dose_coef = c->dose_coef;
+    a.NA = c->NA;
+    a.Ny = c->Ny;
+    a.Nz = c->Nz;
+    a.trapezoidal = (c->p.flags & BFPN_FLAG_TRAPEZOIDAL_YZ) ? 1 : 0;
+    A.ablob = c->n_groups > 0 ? static_cast<uint8_t*>(c->ablob) : nullptr;
+    A.gmap = c->gmap;
+    A.n_mt = (c->nyz + 63) / 64;
+    A.nk = (c->NA + c->umma_bk - 1) / c->umma_bk;
+    return prof(c, BFPN_KERNEL_ENERGY_FUSED, [&] { return launch_energy_fused(A, c->stream); });
+}
+
+// The primary's opening energy pass and T-A-T of step steps_done.
+cudaError_t enq_primary_open(bfpn_ctx* c) {
+    cudaError_t e = enq_energy<float>(c, 0, c->ecoef_half, false, nullptr);
+    if (e != cudaSuccess) return e;
+    const bool clip_F = !(c->p.flags & BFPN_FLAG_NO_SPATIAL_CLIPPING);
+    return enq_tat_pair<float>(c, 0, true, true, !clip_F, true);
+}
+
+// body(step): see above; first_prev = step-1 is step 0.
+cudaError_t enq_fused_body(bfpn_ctx* c, int step, bool first_prev) {
+    double* partP = primary_partials(c, step - 1);
+    const bool clip_F = !(c->p.flags & BFPN_FLAG_NO_SPATIAL_CLIPPING);
+    cudaError_t e = enq_energy_fused(c, partP);
+    if (e != cudaSuccess) return e;
+    if (first_prev) {
+        if ((e = enq_first_finalize<float>(c, partP, c->secondary_zero)) != cudaSuccess) return e;
+        c->split_tat = c->split_chains;
+        e = enq_tat_pair<float>(c, 0, true, true, !clip_F, true);
+        c->split_tat = false;
+        return e;
+    }
+    if (c->profiling) {  // per-kernel timing: one kernel after the other
+        c->src_prepacked = true;
+        e = enq_secondary_half<float>(c, partP, nullptr);
+        c->src_prepacked = false;
+        return e == cudaSuccess ? enq_tat_pair<float>(c, 0, true, true, !clip_F, true) : e;
+    }
+    cudaStream_t main = c->stream;
+    if ((e = cudaEventRecord(c->ev_fork, main)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(c->s_sec, c->ev_fork, 0)) != cudaSuccess) return e;
+    c->stream = c->s_sec;
+    c->split_tat = c->split_chains;
+    c->src_prepacked = true;
+    e = enq_secondary_half<float>(c, partP, nullptr);
+    c->src_prepacked = false;
+    c->stream = main;
+    if (e == cudaSuccess) e = enq_tat_pair<float>(c, 0, true, true, !clip_F, true);
+    c->split_tat = false;
+    if (e != cudaSuccess) return e;
+    if ((e = cudaEventRecord(c->ev_join, c->s_sec)) != cudaSuccess) return e;
+    return cudaStreamWaitEvent(c->stream, c->ev_join, 0);
+}
+
+// close: the owed closing pass and secondary half (or step-0 IDD) of step steps_done-1.
+cudaError_t enq_fused_close(bfpn_ctx* c) {
+    double* partP = primary_partials(c, c->steps_done - 1);
+    cudaError_t e = enq_energy<float>(c, 0, c->ecoef_half, false, partP);
+    if (e != cudaSuccess) return e;
+    if (c->pending_first) return enq_first_finalize<float>(c, partP, c->secondary_zero);
+    return enq_secondary_half<float>(c, partP, nullptr);
 }
 
 cudaError_t enq_step_any(bfpn_ctx* c, bool first, bool secondary_zero) {
@@ -923,6 +1040,52 @@ bfpn_status overlap_step(bfpn_ctx* c) {
     return BFPN_OK;
 }
 
+// One step of the fused order (step = steps_done); see enq_fused_body.
+bfpn_status fused_step(bfpn_ctx* c) {
+    const int step = c->steps_done;
+    if (!c->pending_close) {
+        CUDA_TRY(c, enq_primary_open(c));
+        c->pending_close = true;
+        c->pending_first = step == 0;
+        return BFPN_OK;
+    }
+    if (c->pending_first || !c->use_graphs) {  // the body after step 0 runs once: no graph
+        const long long before = c->launches;
+        CUDA_TRY(c, enq_fused_body(c, step, c->pending_first));
+        if (!c->pending_first) c->kernels_per_step = static_cast<int>(c->launches - before);
+        c->pending_first = false;
+        return BFPN_OK;
+    }
+    cudaGraphExec_t& g = c->fus_exec[step & 1];
+    if (!g) {
+        cudaGraph_t graph = nullptr;
+        CUDA_TRY(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        const long long before = c->launches;
+        cudaError_t ce = enq_fused_body(c, step, false);
+        c->kernels_per_step = static_cast<int>(c->launches - before);
+        cudaError_t ee = cudaStreamEndCapture(c->stream, &graph);
+        if (ce != cudaSuccess || ee != cudaSuccess) {
+            if (graph) cudaGraphDestroy(graph);
+            cudaGetLastError();
+            return fail(c, BFPN_CUDA_ERROR,
+                        std::string("step capture failed: ") + cudaGetErrorString(ce != cudaSuccess ? ce : ee));
+        }
+        ce = cudaGraphInstantiate(&g, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ce != cudaSuccess) return fail(c, BFPN_CUDA_ERROR, std::string("graph instantiate: ") + cudaGetErrorString(ce));
+    }
+    CUDA_TRY(c, cudaGraphLaunch(g, c->stream));
+    return BFPN_OK;
+}
+
+bfpn_status flush_close(bfpn_ctx* c) {
+    if (!c->pending_close) return BFPN_OK;
+    c->pending_close = false;
+    CUDA_TRY(c, enq_fused_close(c));
+    c->pending_first = false;
+    return BFPN_OK;
+}
+
 bfpn_status run_steps(bfpn_ctx* c, int nsteps) {
     if (!c->tables_loaded) return fail(c, BFPN_NOT_READY, "tables not loaded (bfpn_load_tables)");
     if (!c->beam_ready) return fail(c, BFPN_NOT_READY, "beam not initialised (bfpn_init_beam)");
@@ -946,13 +1109,16 @@ bfpn_status run_steps(bfpn_ctx* c, int nsteps) {
         }
         return BFPN_OK;
     }
+    const bool fus = fused_ok(c);
     const bool ovl = overlap_ok(c);
-    if (ovl && (s = ensure_overlap_objects(c)) != BFPN_OK) return s;
+    if ((fus || ovl) && (s = ensure_overlap_objects(c)) != BFPN_OK) return s;
     for (int i = 0; i < nsteps; ++i) {
         const bool first = c->steps_done == 0;
         const bool secondary_stepping =
             !first && !(c->p.flags & (BFPN_FLAG_ENERGY_ONLY | BFPN_FLAG_PRIMARY_ONLY));
-        if (ovl && !first) {
+        if (fus) {
+            if ((s = fused_step(c)) != BFPN_OK) return s;
+        } else if (ovl && !first) {
             if ((s = overlap_step(c)) != BFPN_OK) return s;
         } else if (first || !c->use_graphs) {
             const long long before = c->launches;
@@ -987,6 +1153,7 @@ bfpn_status run_steps(bfpn_ctx* c, int nsteps) {
         c->steps_done++;
     }
     // every call leaves whole steps behind it
+    if ((s = flush_close(c)) != BFPN_OK) return s;
     return flush_secondary(c);
 }
 
@@ -1258,6 +1425,7 @@ bfpn_status bfpn_create(const bfpn_grid* grid, const bfpn_phys* phys, int precis
     ALLOC(c->e1, static_cast<size_t>(c->Ng) * c->Ng * sizeof(double));
     ALLOC(c->e2, static_cast<size_t>(c->Ng) * c->Ng * sizeof(double));
     ALLOC(c->groups, static_cast<size_t>(c->Ng) * sizeof(int));
+    ALLOC(c->gmap, static_cast<size_t>(c->Ng) * sizeof(int));
     ALLOC(c->tile_lo, static_cast<size_t>(c->Ng) * sizeof(int));
     ALLOC(c->tile_hi, static_cast<size_t>(c->Ng) * sizeof(int));
     ALLOC(c->beam_yza, static_cast<size_t>(c->per_e) * sizeof(double));
@@ -1357,6 +1525,11 @@ bfpn_status bfpn_load_tables(bfpn_ctx* c, const double* mu, int32_t mu_rows, con
     c->n_groups = static_cast<int>(groups.size());
     if (!groups.empty() && (s = upload_f64(c, c->groups, groups.data(), groups.size() * sizeof(int))) != BFPN_OK)
         return s;
+    {
+        std::vector<int> gmap(c->Ng, -1);
+        for (size_t k = 0; k < groups.size(); ++k) gmap[groups[k]] = static_cast<int>(k);
+        if ((s = upload_f64(c, c->gmap, gmap.data(), gmap.size() * sizeof(int))) != BFPN_OK) return s;
+    }
     // tables of an earlier load (a context reused for another beam): the step
     // graph captured their addresses, so it goes too
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
@@ -1380,7 +1553,12 @@ bfpn_status bfpn_load_tables(bfpn_ctx* c, const double* mu, int32_t mu_rows, con
         size_t free_b = 0, total_b = 0;
         if (!c->ooc && cudaMemGetInfo(&free_b, &total_b) == cudaSuccess && pack + (256u << 20) < free_b) {
             void* ab = nullptr;
-            if (dalloc(c, &ab, pack) == BFPN_OK) c->ablob = ab;
+            if (dalloc(c, &ab, pack) == BFPN_OK) {
+                c->ablob = ab;
+                // the fused energy kernel writes only real (position, angle)
+                // entries; the padding of partial tiles must read as zeros
+                CUDA_TRY(c, cudaMemsetAsync(ab, 0, pack, c->stream));
+            }
         }
         // B tiles from the float ker_v already on the device
         void* d = nullptr;
@@ -1622,6 +1800,9 @@ bfpn_status bfpn_set_option(bfpn_ctx* c, int32_t option, int32_t value) {
         case BFPN_OPT_ENERGY_CHUNK:
             if (value < 1) return fail(c, BFPN_INVALID_ARG, "chunk sizes must be positive");
             (option == BFPN_OPT_LANE_CHUNK ? c->ooc_lane_req : c->ooc_group_req) = value;
+            break;
+        case BFPN_OPT_FUSED_ENERGY:
+            c->fuse_energy = value != 0;
             break;
         case BFPN_OPT_STREAM_TRANSPORT:
             if (value < 0 || value > 2) return fail(c, BFPN_INVALID_ARG, "stream transport: 0, 1 or 2");

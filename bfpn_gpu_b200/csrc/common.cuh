@@ -62,6 +62,31 @@ struct EnergyArgs {
     long long lane0 = 0;   // state lane of lane 0 (a chunk of whole positions; trapezoidal weights)
 };
 
+// Byte offset of element (row, k) in a K-major no-swizzle UMMA tile of
+// `rows` rows: core matrix (row/8, k/8) of 8 x 8 bf16, 16-byte rows.
+__host__ __device__ inline size_t umma_kmajor_offset(int row, int k, int rows) {
+    return (static_cast<size_t>(k >> 3) * (rows >> 3) + (row >> 3)) * 128 + (row & 7) * 16 + (k & 7) * 2;
+}
+
+// The primary's closing energy half-step of one depth step fused with the
+// opening half-step of the next (no source; float state, lanes a multiple of
+// 4, eq15 modes).  e.F / e.f hold the state after the step's transport and
+// angular diffusion and receive the state after the next step's opening
+// half; e.partials receives the closing pass's IDD partials (one pair per
+// block, as energy_ring_kernel).  At the midpoint (after the closing pass)
+// the state of every source group is also written, split into bf16 hi / lo,
+// as the A operand of the source's angular contraction (rows 0..63 of a
+// 64-position tile max(psi^1, 0), rows 64..127 psi^2, K-major core layout,
+// 16-wide k chunks): the operand pack_source_operand_kernel would build.
+struct EnergyFusedArgs {
+    EnergyArgs<float> e;
+    uint8_t* ablob;      // [n_groups][n_mt][nk][hi|lo][128 x 16 bf16], or nullptr
+    const int* gmap;     // [Ng]: index of each group among the source groups, -1 for none
+    int n_mt, nk;
+};
+cudaError_t launch_energy_fused(const EnergyFusedArgs& a, cudaStream_t s);
+bool energy_fused_supported(long long lanes, int mode, int NA);
+
 // Arguments of one transport half-step (Eq. 18) over one array.
 template <typename T>
 struct TransportArgs {
@@ -218,11 +243,12 @@ cudaError_t launch_spot_plane(const T* F, const T* f, const T* F1, const T* f1, 
 // The epilogue writes A1 / A2 split into bf16 hi / lo into q (umma_q_bytes,
 // the energy stage's operand layout); rows of groups it does not write must
 // be zero.  packed (may be null) is recorded on s once the pack, the last
-// reader of P1 and P2, has been enqueued.
+// reader of P1 and P2, has been enqueued.  pack = false: ablob already holds
+// the operand (written by energy_fused_kernel); P1, P2 are not read.
 cudaError_t launch_source_angular_pipe(const float* P1, const float* P2, uint8_t* ablob, const uint8_t* bblob,
                                        const int* groups, int n_groups, uint8_t* q, int Ng, int* err, int nyz,
                                        int NA, int NT, int BK, int n_ntiles, cudaStream_t s,
-                                       cudaEvent_t packed = nullptr);
+                                       cudaEvent_t packed = nullptr, bool pack = true);
 size_t umma_pack_bytes(int n_groups, int nyz, int NA, int BK);
 size_t umma_q_bytes(long long per_e, int Ng);
 // Tensor-core energy stage: S[e][l] from q with the coefficient tiles and

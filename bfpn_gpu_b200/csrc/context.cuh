@@ -133,6 +133,16 @@ struct bfpn_ctx {
     cudaStream_t s_f[2] = {nullptr, nullptr};
     cudaEvent_t ev_ff[2] = {nullptr, nullptr}, ev_fj[2] = {nullptr, nullptr};
     cudaGraphExec_t ovl_exec[2] = {nullptr, nullptr};
+    // fused primary energy passes (mixed precision, overlapped steps): the
+    // closing pass of step n and the opening pass of step n+1 run as one
+    // kernel, which also writes the source's operand.  pending_close: the
+    // closing pass and the secondary half of step steps_done-1 are still owed
+    // (pending_first: that step is step 0, which has no secondary half)
+    bool fuse_energy = true;    // option
+    bool pending_close = false, pending_first = false;
+    bool src_prepacked = false;  // the source's operand is already in ablob
+    int* gmap = nullptr;         // [Ng]: index among the source groups, -1 for none
+    cudaGraphExec_t fus_exec[2] = {nullptr, nullptr};
     bool profiling = false;
     struct Pending {
         int cls;

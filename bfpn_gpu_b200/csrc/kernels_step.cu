@@ -9,6 +9,8 @@
 #include "common.cuh"
 #include "async_copy.cuh"
 
+#include <cuda_bf16.h>
+
 #include <cooperative_groups.h>
 
 #include <algorithm>
@@ -399,6 +401,190 @@ cudaError_t launch_energy_ring(const EnergyArgs<float>& a, cudaStream_t s) {
     const int grid = energy_ring_grid(a.lanes);
     if (a.mode == EMODE_EQ15) energy_ring_kernel<EMODE_EQ15, D, NTH><<<grid, NTH, smem, s>>>(a);
     else energy_ring_kernel<EMODE_EQ15_STRAG, D, NTH><<<grid, NTH, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Fused primary energy half-steps: the closing E1/2 of step n and the opening
+// E1/2 of step n+1 in one sweep over the groups (high -> low).  The opening
+// sweep's update of group g needs the closing result of groups g and g-1
+// (straggling) and its own results for g+1, so it runs one group behind the
+// closing sweep, its carried values in registers: iteration i applies the
+// closing update to group ek = Ng-1-i and the opening update to group ek+1.
+// Each update is energy_ring_kernel's, on the same inputs -- the midpoint
+// value is rounded to float as the separate passes store it -- so the state
+// equals the two passes' bit for bit; the closing pass's IDD partials are
+// those of the closing ring pass.  At the midpoint the source groups' values
+// go to the angular contraction's operand (split bf16), which removes that
+// operand's own pass over the primary.
+// ---------------------------------------------------------------------------
+template <int MODE, int D, int NTH>
+__global__ void __launch_bounds__(NTH) energy_fused_kernel(EnergyFusedArgs A) {
+    const EnergyArgs<float>& a = A.e;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float4* ring = reinterpret_cast<float4*>(smem_raw);  // [D][2][NTH]
+    const long long L = a.lanes;
+    const int Ng = a.Ng, tid = threadIdx.x;
+    const long long bid = blockIdx.x;
+    const long long lane0 = (bid * NTH + tid) * 4;
+    const bool ok = lane0 < L;  // L % 4 == 0: the 4 lanes are all in or all out
+    auto slot = [&](int k, int arr) { return ring + (k * 2 + arr) * NTH + tid; };
+    auto fill = [&](int i) {  // group Ng-1-i into slot i % D, one commit group per call
+        const int e = Ng - 1 - i;
+        if (ok && e >= 0) {
+            const size_t off = static_cast<size_t>(e) * L + lane0;
+            cp_async16(slot(i % D, 0), a.F + off, true);
+            cp_async16(slot(i % D, 1), a.f + off, true);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    for (int i = 0; i < D; ++i) fill(i);
+    // closing sweep: old values and new values of the group above; opening
+    // sweep: midpoint values and new values of the group above its own
+    double cFo[4], cfo[4], cFn[4], cfn[4], oFo[4], ofo[4], oFn[4], ofn[4], w_pos[4], acc = 0.0, accp = 0.0;
+    float mF[4], mf[4];  // midpoint of group ek+1
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        cFo[j] = cfo[j] = cFn[j] = cfn[j] = oFo[j] = ofo[j] = oFn[j] = ofn[j] = 0.0;
+        mF[j] = mf[j] = 0.f;
+        w_pos[j] = 1.0;
+        if (a.partials && a.trapezoidal && ok) {
+            const int pos = static_cast<int>((lane0 + j) / a.NA);
+            const int iy = pos % (a.Ny + 1), iz = pos / (a.Ny + 1);
+            if (iy == 0 || iy == a.Ny) w_pos[j] *= 0.5;
+            if (iz == 0 || iz == a.Nz) w_pos[j] *= 0.5;
+        }
+    }
+    // this thread's place in the source operand: position p, angles k0 .. k0+3 of chunk kc
+    const int p = ok ? static_cast<int>(lane0 / a.NA) : 0, k0 = ok ? static_cast<int>(lane0 % a.NA) : 0;
+    constexpr size_t kPart = 128 * 16 * 2;  // one (hi or lo) 128 x 16 bf16 tile
+    const size_t a_tile = (static_cast<size_t>(p >> 6) * A.nk + (k0 >> 4)) * 2 * kPart;
+    const size_t a_off1 = umma_kmajor_offset(p & 63, k0 & 15, 128), a_off2 = umma_kmajor_offset(64 + (p & 63), k0 & 15, 128);
+    const size_t a_group = static_cast<size_t>(A.n_mt) * A.nk * 2 * kPart;
+    auto put = [&](size_t off, float x0, float x1, float x2, float x3) {  // 4 values: hi, then lo
+        const __nv_bfloat162 h01 = __floats2bfloat162_rn(x0, x1), h23 = __floats2bfloat162_rn(x2, x3);
+        const __nv_bfloat162 l01 = __floats2bfloat162_rn(x0 - __low2float(h01), x1 - __high2float(h01));
+        const __nv_bfloat162 l23 = __floats2bfloat162_rn(x2 - __low2float(h23), x3 - __high2float(h23));
+        uint2 hv, lv;
+        hv.x = *reinterpret_cast<const uint32_t*>(&h01);
+        hv.y = *reinterpret_cast<const uint32_t*>(&h23);
+        lv.x = *reinterpret_cast<const uint32_t*>(&l01);
+        lv.y = *reinterpret_cast<const uint32_t*>(&l23);
+        *reinterpret_cast<uint2*>(A.ablob + off) = hv;
+        *reinterpret_cast<uint2*>(A.ablob + off + kPart) = lv;
+    };
+    constexpr bool kStrag = MODE == EMODE_EQ15_STRAG;
+    const bool dose = a.partials != nullptr;
+    Eq15Coef k_next = load_eq15_coef<MODE>(a.coef + (Ng - 1) * kEnergyCoef, a.dose_coef + 2 * (Ng - 1), dose);
+    Eq15Coef k_up = k_next;  // constants of group ek+1 (the opening update's group)
+    for (int i = 0; i <= Ng; ++i) {
+        const int ek = Ng - 1 - i;
+        float nF[4] = {0.f, 0.f, 0.f, 0.f}, nf[4] = {0.f, 0.f, 0.f, 0.f};  // midpoint of group ek
+        Eq15Coef kc = k_up;
+        if (ek >= 0) {
+            // closing update of group ek
+            kc = k_next;
+            if (ek > 0) k_next = load_eq15_coef<MODE>(a.coef + (ek - 1) * kEnergyCoef, a.dose_coef + 2 * (ek - 1), dose);
+            if (kStrag) asm volatile("cp.async.wait_group %0;" ::"n"(D - 3) : "memory");
+            else asm volatile("cp.async.wait_group %0;" ::"n"(D - 2) : "memory");
+            const float4 vF = *slot(i % D, 0), vf = *slot(i % D, 1);
+            float4 vn = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (kStrag && ek > 0) vn = *slot((i + 1) % D, 0);
+            if (i > 0) fill(i - 1 + D);  // the slot read in the previous iteration
+            const float Fa[4] = {vF.x, vF.y, vF.z, vF.w}, fa[4] = {vf.x, vf.y, vf.z, vf.w};
+            const float na[4] = {vn.x, vn.y, vn.z, vn.w};
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const double Fg = Fa[j], fg = fa[j];
+                double Fv, fv;
+                eq15_update<MODE>(kc, ek, Fg, fg, 0.0, static_cast<double>(na[j]), cFo[j], cfo[j], cFn[j], cfn[j],
+                                  Fv, fv);
+                nF[j] = static_cast<float>(Fv);
+                nf[j] = static_cast<float>(fv);
+                if (dose && ok) {
+                    acc += w_pos[j] * (kc.d0 * static_cast<double>(nF[j]) + kc.d1 * static_cast<double>(nf[j]));
+                    accp += static_cast<double>(nf[j]);
+                }
+                cFo[j] = Fg;
+                cfo[j] = fg;
+                cFn[j] = Fv;
+                cfn[j] = fv;
+            }
+            const int gz = A.ablob ? __ldg(A.gmap + ek) : -1;
+            if (ok && gz >= 0) {
+                const size_t base = static_cast<size_t>(gz) * a_group + a_tile;
+                put(base + a_off1, fmaxf(nF[0], 0.f), fmaxf(nF[1], 0.f), fmaxf(nF[2], 0.f), fmaxf(nF[3], 0.f));
+                put(base + a_off2, nf[0], nf[1], nf[2], nf[3]);
+            }
+        }
+        if (ek + 1 <= Ng - 1) {
+            // opening update of group ek+1 from the midpoint: its value mF/mf,
+            // group ek's (straggling) nF, the group above's oFo/oFn
+            const int eo = ek + 1;
+            float Fo[4], fo[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const double Fg = mF[j], fg = mf[j];
+                double Fv, fv;
+                eq15_update<MODE>(k_up, eo, Fg, fg, 0.0, static_cast<double>(nF[j]), oFo[j], ofo[j], oFn[j], ofn[j],
+                                  Fv, fv);
+                Fo[j] = static_cast<float>(Fv);
+                fo[j] = static_cast<float>(fv);
+                oFo[j] = Fg;
+                ofo[j] = fg;
+                oFn[j] = Fv;
+                ofn[j] = fv;
+            }
+            if (ok) {
+                const size_t off = static_cast<size_t>(eo) * L + lane0;
+                *reinterpret_cast<float4*>(a.F + off) = make_float4(Fo[0], Fo[1], Fo[2], Fo[3]);
+                *reinterpret_cast<float4*>(a.f + off) = make_float4(fo[0], fo[1], fo[2], fo[3]);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            mF[j] = nF[j];
+            mf[j] = nf[j];
+        }
+        k_up = kc;
+    }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    if (a.partials) {
+        __shared__ double red[2][NTH / 32];
+        for (int o = 16; o > 0; o >>= 1) {
+            acc += __shfl_down_sync(0xffffffffu, acc, o);
+            accp += __shfl_down_sync(0xffffffffu, accp, o);
+        }
+        const int w = tid >> 5, l = tid & 31;
+        if (l == 0) {
+            red[0][w] = acc;
+            red[1][w] = accp;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            double s0 = 0.0, s1 = 0.0;
+            for (int k = 0; k < NTH / 32; ++k) {
+                s0 += red[0][k];
+                s1 += red[1][k];
+            }
+            a.partials[2 * bid] = s0;
+            a.partials[2 * bid + 1] = s1;
+        }
+    }
+}
+
+bool energy_fused_supported(long long lanes, int mode, int NA) {
+    return lanes % 4 == 0 && NA % 4 == 0 && mode != EMODE_LEGACY;
+}
+
+cudaError_t launch_energy_fused(const EnergyFusedArgs& A, cudaStream_t s) {
+    const EnergyArgs<float>& a = A.e;
+    if (!energy_fused_supported(a.lanes, a.mode, a.NA) || a.src || a.lane0 != 0) return cudaErrorNotSupported;
+    constexpr int D = kEnergyRing, NTH = kEnergyRingThreads;
+    const size_t smem = static_cast<size_t>(D) * 2 * NTH * sizeof(float4);
+    const int grid = energy_ring_grid(a.lanes);
+    if (a.mode == EMODE_EQ15) energy_fused_kernel<EMODE_EQ15, D, NTH><<<grid, NTH, smem, s>>>(A);
+    else energy_fused_kernel<EMODE_EQ15_STRAG, D, NTH><<<grid, NTH, smem, s>>>(A);
     return cudaGetLastError();
 }
 

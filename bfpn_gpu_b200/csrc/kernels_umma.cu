@@ -71,12 +71,6 @@ __device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
 
 }  // namespace
 
-// Byte offset of element (row, k) in a K-major no-swizzle tile of `rows`
-// rows: core matrix (row/8, k/8) of 8 x 8 bf16.
-__host__ __device__ inline size_t umma_kmajor_offset(int row, int k, int rows) {
-    return (static_cast<size_t>(k >> 3) * (rows >> 3) + (row >> 3)) * 128 + (row & 7) * 16 + (k & 7) * 2;
-}
-
 // Byte offset of element (plane, s, l) in the energy stage's A operand: lanes
 // in tiles of 128, source groups in rows of 8.  One (lane tile, 8 groups)
 // block is 8 KB: 4 planes (A1 hi, A1 lo, A2 hi, A2 lo) x 2 atoms of 64 lanes
@@ -353,16 +347,19 @@ size_t umma_pipe_smem(int NT, int BK) {
 
 cudaError_t launch_source_angular_pipe(const float* P1, const float* P2, uint8_t* ablob, const uint8_t* bblob,
                                        const int* groups, int n_groups, uint8_t* q, int Ng, int* err, int nyz,
-                                       int NA, int NT, int BK, int n_ntiles, cudaStream_t s, cudaEvent_t packed) {
+                                       int NA, int NT, int BK, int n_ntiles, cudaStream_t s, cudaEvent_t packed,
+                                       bool pack) {
     if (n_groups <= 0) return packed ? cudaEventRecord(packed, s) : cudaSuccess;
     if (BK != 16 || NT % 16 != 0 || NT < 16 || NT > 256) return cudaErrorInvalidValue;
     const int n_mt = (nyz + kPos - 1) / kPos, nk = (NA + BK - 1) / BK;
-    UmmaPackArgs p{P1, P2, groups, ablob, nyz, NA, nk, n_mt, BK};
-    const long long per_group = static_cast<long long>(n_mt) * nk * kRows * (BK / 8);
-    if ((per_group + 255) / 256 > 0x7fffffffLL || n_groups > 65535) return cudaErrorInvalidConfiguration;
-    pack_source_operand_kernel<<<dim3(static_cast<unsigned>((per_group + 255) / 256), n_groups), 256, 0, s>>>(p);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
+    cudaError_t e = cudaSuccess;
+    if (pack) {
+        UmmaPackArgs p{P1, P2, groups, ablob, nyz, NA, nk, n_mt, BK};
+        const long long per_group = static_cast<long long>(n_mt) * nk * kRows * (BK / 8);
+        if ((per_group + 255) / 256 > 0x7fffffffLL || n_groups > 65535) return cudaErrorInvalidConfiguration;
+        pack_source_operand_kernel<<<dim3(static_cast<unsigned>((per_group + 255) / 256), n_groups), 256, 0, s>>>(p);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
     if (packed && (e = cudaEventRecord(packed, s)) != cudaSuccess) return e;
     UmmaPipeArgs a{ablob, bblob, groups, q, err, nyz, NA, NT, nk, n_ntiles, n_mt, 2 * ((Ng + 15) / 16)};
     size_t smem = umma_pipe_smem(NT, BK);

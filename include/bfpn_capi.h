@@ -231,7 +231,8 @@ enum {
     BFPN_KERNEL_SOURCE_ANGULAR = 3, /* source: angular contraction */
     BFPN_KERNEL_SOURCE_ENERGY = 4,  /* source: banded energy contraction */
     BFPN_KERNEL_IDD = 5,            /* IDD partials / final sum */
-    BFPN_KERNEL_CLASSES = 6
+    BFPN_KERNEL_ENERGY_FUSED = 6,   /* primary closing + next opening energy pass, source operand */
+    BFPN_KERNEL_CLASSES = 7
 };
 
 /* With profiling on, steps run eagerly (no graph) and every launch is
@@ -290,7 +291,16 @@ int32_t bfpn_source_groups(bfpn_ctx* ctx);
  *   plane walks the z rows, the z-stencil in registers and one row of the
  *   y-stencil in shared memory, in place; 2 also uses it where a whole-plane
  *   kernel exists; 0 leaves those planes to the cluster / tiled kernels.
- *   Same values as the whole-plane kernel. */
+ *   Same values as the whole-plane kernel.
+ * BFPN_OPT_FUSED_ENERGY: 1 (default) runs, in mixed precision with step
+ *   overlap on (eq15 energy, NA a multiple of 4, the tensor-core source), the
+ *   primary's closing energy half-step of each step and the opening half-step
+ *   of the next as one kernel, which also writes the source's split-bf16
+ *   operand: per step one primary energy pass and the operand's pack pass
+ *   fewer.  Within a bfpn_step call the secondary half of step n then runs
+ *   beside the primary's transport and angular passes of step n+1; the call
+ *   still ends on whole steps.  0 keeps the separate passes.  Same states and
+ *   IDD values. */
 enum {
     BFPN_OPT_TENSOR_CORES = 0,
     BFPN_OPT_CUDA_GRAPHS = 1,
@@ -300,7 +310,8 @@ enum {
     BFPN_OPT_LANE_CHUNK = 5,
     BFPN_OPT_ENERGY_CHUNK = 6,
     BFPN_OPT_STEP_OVERLAP = 7,
-    BFPN_OPT_STREAM_TRANSPORT = 8
+    BFPN_OPT_STREAM_TRANSPORT = 8,
+    BFPN_OPT_FUSED_ENERGY = 9
 };
 bfpn_status bfpn_set_option(bfpn_ctx* ctx, int32_t option, int32_t value);
 

@@ -425,9 +425,10 @@ def test_mixed_context_tables_equal_host_tables():
         assert np.array_equal(ctx.table(which, n), capi.host_table(cfg.grid(), cfg.phys(), mu, sig, which))
 
 
-def _stepped(cfg, precision, overlap, calls):
+def _stepped(cfg, precision, overlap, calls, fused=0):
     ctx, ora = build(cfg, precision=precision)
     ctx.set_option(capi.OPT_STEP_OVERLAP, overlap)
+    ctx.set_option(capi.OPT_FUSED_ENERGY, fused)
     idd = np.concatenate([ctx.step(n)[0] for n in calls])
     states = [ctx.get_state(sp, cf) for sp in (0, 1) for cf in (0, 1)]
     return ctx, ora, idd, states
@@ -452,6 +453,39 @@ def test_overlapped_steps_equal_sequential_steps(precision, overlap):
         idd_r, _ = ora.step(sum(calls))
         assert rel_err(idd_o, idd_r) < STEP_TOL
         assert_states(ctx, ora, STEP_TOL)
+
+
+@pytest.mark.parametrize("straggling", [False, True])
+def test_fused_energy_passes_equal_separate_passes(straggling):
+    """The primary's closing energy pass of each step fused with the next
+    step's opening pass (which also writes the source's operand) gives the
+    separate passes' states bit for bit, over calls of 1, 2, 5 and 3 steps
+    (each call opens its first step and closes its last); the IDD history
+    agrees up to the order of the closing pass's partial sums (this plane is
+    swept by the 2-lane register kernel when the passes are separate)."""
+    cfg = small_cfg(ny=8, nz=8, nmu=4, nom=4, ng=40, ly=2.0, lz=2.0, eq15_straggling=straggling)
+    calls = [1, 2, 5, 3]
+    _, _, idd_s, st_s = _stepped(cfg, capi.PREC_MIXED, 0, calls)
+    ctx, _, idd_f, st_f = _stepped(cfg, capi.PREC_MIXED, 2, calls, fused=1)
+    assert ctx.kernels_per_step() > 0 and ctx.source_groups() > 0
+    assert np.abs(idd_s).max() > 0
+    assert np.abs(idd_f - idd_s).max() <= 1e-13 * np.abs(idd_s).max()
+    for a, b in zip(st_s, st_f):
+        assert np.array_equal(a, b)
+
+
+def test_fused_energy_passes_large_plane_bit_identical():
+    """On a plane of more than 2^20 lanes the separate passes use the 4-lane
+    ring kernel, whose partial sums the fused kernel shares: the IDD history
+    is bit-identical too."""
+    cfg = small_cfg(ny=64, nz=64, nmu=16, nom=16, ng=24, ly=8.0, lz=8.0)
+    calls = [3, 4]
+    _, _, idd_s, st_s = _stepped(cfg, capi.PREC_MIXED, 0, calls)
+    _, _, idd_f, st_f = _stepped(cfg, capi.PREC_MIXED, 2, calls, fused=1)
+    assert np.abs(idd_s).max() > 0
+    assert np.array_equal(idd_s, idd_f)
+    for a, b in zip(st_s, st_f):
+        assert np.array_equal(a, b)
 
 
 def test_step_api_pieces_agree():
