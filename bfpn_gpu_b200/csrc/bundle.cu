@@ -226,7 +226,12 @@ bfpn_status build_plan(bfpn_bundle* b, const std::vector<int>& prim, const std::
         BUNDLE_CUDA(b, cudaMalloc(&b->dimg, cap));
         b->dimg_bytes = cap;
     }
-    BUNDLE_CUDA(b, cudaMemcpy(b->dimg, img.bytes.data(), img.bytes.size(), cudaMemcpyHostToDevice));
+    // on the bundle's own stream: a plain cudaMemcpy from pageable memory may
+    // return before its DMA lands and runs on the legacy stream, which the
+    // bundle's non-blocking stream does not wait for -- the next step's
+    // kernels could read the previous slot set's arguments
+    BUNDLE_CUDA(b, cudaMemcpyAsync(b->dimg, img.bytes.data(), img.bytes.size(), cudaMemcpyHostToDevice, b->stream));
+    BUNDLE_CUDA(b, cudaStreamSynchronize(b->stream));
     b->plan = p;
     return BFPN_OK;
 }
@@ -441,7 +446,8 @@ bfpn_status bfpn_bundle_create(int32_t device, int32_t max_slots, bfpn_bundle** 
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming);
     for (int i = 0; e == cudaSuccess && i < 8; ++i) e = cudaEventCreate(&b->ev[i]);
     if (e == cudaSuccess) e = cudaMalloc(&b->err, sizeof(int));
-    if (e == cudaSuccess) e = cudaMemset(b->err, 0, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemsetAsync(b->err, 0, sizeof(int), b->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
     if (e != cudaSuccess) {
         const std::string msg = std::string("bundle: ") + cudaGetErrorString(e);
         bfpn_bundle_destroy(b);
@@ -583,7 +589,8 @@ bfpn_status bfpn_bundle_sync(bfpn_bundle* b) {
     int err = 0;
     BUNDLE_CUDA(b, cudaMemcpy(&err, b->err, sizeof(int), cudaMemcpyDeviceToHost));
     if (err) {
-        cudaMemset(b->err, 0, sizeof(int));
+        cudaMemsetAsync(b->err, 0, sizeof(int), b->stream);
+        cudaStreamSynchronize(b->stream);
         return bfail(b, BFPN_TIMEOUT, "bundle: a kernel's bounded wait ran out (code " + std::to_string(err) + ")");
     }
     // the slots' own error words (the tensor-core source kernels' bounded waits)
@@ -592,7 +599,8 @@ bfpn_status bfpn_bundle_sync(bfpn_bundle* b) {
         if (!c || !c->dev_err) continue;
         BUNDLE_CUDA(b, cudaMemcpy(&err, c->dev_err, sizeof(int), cudaMemcpyDeviceToHost));
         if (err) {
-            cudaMemset(c->dev_err, 0, sizeof(int));
+            cudaMemsetAsync(c->dev_err, 0, sizeof(int), b->stream);
+            cudaStreamSynchronize(b->stream);
             return bfail(b, BFPN_TIMEOUT, "bundle: slot " + std::to_string(i) + ": a source kernel's bounded wait ran out "
                                           "(code " + std::to_string(err) + ")");
         }

@@ -1179,7 +1179,8 @@ bfpn_status check_device_error(bfpn_ctx* c) {
     int h = 0;
     CUDA_TRY(c, cudaMemcpy(&h, c->dev_err, sizeof(int), cudaMemcpyDeviceToHost));
     if (h == 0) return BFPN_OK;
-    CUDA_TRY(c, cudaMemset(c->dev_err, 0, sizeof(int)));
+    CUDA_TRY(c, cudaMemsetAsync(c->dev_err, 0, sizeof(int), c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     return fail(c, BFPN_TIMEOUT, "a bounded device wait ran out (code " + std::to_string(h) + "); results of the step are invalid");
 }
 
