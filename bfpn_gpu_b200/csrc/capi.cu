@@ -445,8 +445,8 @@ cudaError_t enq_source_on(bfpn_ctx* c, const void* P1, const void* P2, void* S, 
                                               as<const float>(const_cast<void*>(P2)),
                                               static_cast<uint8_t*>(c->ablob), static_cast<const uint8_t*>(c->bblob),
                                               c->groups, c->n_groups, q, c->Ng, c->dev_err, nyz, c->NA,
-                                              c->umma_nt, c->umma_bk, c->umma_ntiles, c->stream, pread,
-                                              !c->src_prepacked);
+                                              c->umma_nt, c->umma_bk, c->umma_ntiles, c->ulist, c->ubegin,
+                                              c->stream, pread, !c->src_prepacked);
         });
         if (e != cudaSuccess) return e;
         return prof(c, BFPN_KERNEL_SOURCE_ENERGY, [&] {
@@ -1538,6 +1538,8 @@ bfpn_status bfpn_load_tables(bfpn_ctx* c, const double* mu, int32_t mu_rows, con
     dfree(c, c->ablob);
     dfree(c, c->bblob);
     dfree(c, c->eblob);
+    { void* w = c->ulist; dfree(c, w); c->ulist = nullptr; }
+    { void* w = c->ubegin; dfree(c, w); c->ubegin = nullptr; }
     { void* w = c->ework; dfree(c, w); c->ework = nullptr; }
     { void* w = c->ework_begin; dfree(c, w); c->ework_begin = nullptr; }
     // rows of groups without an angular kernel are read as zeros; an earlier
@@ -1568,6 +1570,22 @@ bfpn_status bfpn_load_tables(bfpn_ctx* c, const double* mu, int32_t mu_rows, con
         CUDA_TRY(c, launch_build_umma_blob(as<const float>(c->ker_v), c->groups, c->n_groups, c->NA, c->umma_nt,
                                            c->umma_bk, static_cast<uint8_t*>(d), c->stream));
         CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+        // the kernel blocks' non-zero k chunks and column ranges (the kernel is
+        // sparse: entries below the threshold were dropped)
+        if (!T.ker_v_f.empty()) {
+            std::vector<int4> ul;
+            std::vector<int> ub;
+            build_umma_ranges(T.ker_v_f.data(), groups.data(), c->n_groups, c->NA, c->umma_nt, c->umma_bk,
+                              c->umma_ntiles, ul, ub);
+            void *dl = nullptr, *dbg = nullptr;
+            if ((s = dalloc(c, &dl, std::max<size_t>(16, ul.size() * sizeof(int4)))) != BFPN_OK) return s;
+            c->ulist = static_cast<int4*>(dl);
+            if (!ul.empty() && (s = upload_f64(c, dl, ul.data(), ul.size() * sizeof(int4))) != BFPN_OK) return s;
+            if ((s = dalloc(c, &dbg, ub.size() * sizeof(int))) != BFPN_OK) return s;
+            c->ubegin = static_cast<int*>(dbg);
+            if ((s = upload_f64(c, dbg, ub.data(), ub.size() * sizeof(int))) != BFPN_OK) return s;
+            CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+        }
         // energy stage: banded coefficient tiles and per-output-tile work lists
         std::vector<uint8_t> eb;
         std::vector<int> work, begin;

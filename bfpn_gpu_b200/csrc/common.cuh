@@ -245,10 +245,20 @@ cudaError_t launch_spot_plane(const T* F, const T* f, const T* F1, const T* f1, 
 // be zero.  packed (may be null) is recorded on s once the pack, the last
 // reader of P1 and P2, has been enqueued.  pack = false: ablob already holds
 // the operand (written by energy_fused_kernel); P1, P2 are not read.
+// ulist / ubegin (may be null: every k chunk, full width): the k chunks of
+// source group gz and output tile nt whose kernel block has a non-zero entry,
+// entries ubegin[gz * n_ntiles + nt] .. ubegin[gz * n_ntiles + nt + 1] - 1 of
+// ulist, each {k chunk, first column, columns} with the column range a
+// multiple of 16 covering the chunk's non-zero columns in the tile
+// (build_umma_ranges); the other chunks add nothing and are skipped.
 cudaError_t launch_source_angular_pipe(const float* P1, const float* P2, uint8_t* ablob, const uint8_t* bblob,
                                        const int* groups, int n_groups, uint8_t* q, int Ng, int* err, int nyz,
-                                       int NA, int NT, int BK, int n_ntiles, cudaStream_t s,
-                                       cudaEvent_t packed = nullptr, bool pack = true);
+                                       int NA, int NT, int BK, int n_ntiles, const int4* ulist, const int* ubegin,
+                                       cudaStream_t s, cudaEvent_t packed = nullptr, bool pack = true);
+// Host: the entries of ulist / ubegin from the float angular kernel kv
+// ([Ng][NA in][NA out]) of the source groups.
+void build_umma_ranges(const float* kv, const int* groups, int n_groups, int NA, int NT, int BK, int n_ntiles,
+                       std::vector<int4>& list, std::vector<int>& begin);
 size_t umma_pack_bytes(int n_groups, int nyz, int NA, int BK);
 size_t umma_q_bytes(long long per_e, int Ng);
 // Tensor-core energy stage: S[e][l] from q with the coefficient tiles and

@@ -69,6 +69,8 @@ struct bfpn_ctx {
     void* bblob = nullptr;          // split-bf16 angular kernel tiles for the tensor-core source
     void* ablob = nullptr;          // packed split-bf16 A operand (pipelined tensor-core source)
     void* eblob = nullptr;          // split-bf16 energy coefficient tiles (tensor-core source)
+    int4* ulist = nullptr;          // non-zero k chunks / column ranges of the angular kernel blocks
+    int* ubegin = nullptr;          // [n_groups * umma_ntiles + 1] offsets into ulist
     int* ework = nullptr;           // energy work items {chunk, column, columns, e group}
     int* ework_begin = nullptr;     // [e tiles + 1]
     int e_et = 0, e_emax = 0;

@@ -23,6 +23,9 @@
 
 namespace bfpn {
 
+template <int V>
+using IntC = std::integral_constant<int, V>;
+
 cudaError_t allow_dynamic_smem(const void* func, size_t need) {
     static std::mutex m;
     static std::map<std::pair<const void*, int>, size_t> limit;  // (function, device) -> bytes allowed
@@ -313,11 +316,17 @@ __device__ __forceinline__ void energy_ring_body(const EnergyArgs<float>& a, lon
     }
     constexpr bool kStrag = MODE == EMODE_EQ15_STRAG;
     const bool dose = a.partials != nullptr;
-    Eq15Coef k_next = load_eq15_coef<MODE>(a.coef + (Ng - 1) * kEnergyCoef, a.dose_coef + 2 * (Ng - 1), dose);
-    for (int i = 0; i < Ng; ++i) {
+    // group Ng-1-i's constants in K[i % 2]; iteration i loads the next
+    // group's into the other slot.  Two iterations per trip keep the slots
+    // fixed registers instead of a copy of the set per group.
+    Eq15Coef K[2];
+    K[0] = load_eq15_coef<MODE>(a.coef + (Ng - 1) * kEnergyCoef, a.dose_coef + 2 * (Ng - 1), dose);
+    auto iter = [&](auto Rc, int i) {
+        constexpr int R = decltype(Rc)::value;
         const int ek = Ng - 1 - i;
-        const Eq15Coef kc = k_next;
-        if (ek > 0) k_next = load_eq15_coef<MODE>(a.coef + (ek - 1) * kEnergyCoef, a.dose_coef + 2 * (ek - 1), dose);
+        if (ek < 0) return;
+        const Eq15Coef& kc = K[R];
+        if (ek > 0) K[R ^ 1] = load_eq15_coef<MODE>(a.coef + (ek - 1) * kEnergyCoef, a.dose_coef + 2 * (ek - 1), dose);
         // groups 0 .. i (and i+1 for straggling) have landed
         if (kStrag) asm volatile("cp.async.wait_group %0;" ::"n"(D - 3) : "memory");
         else asm volatile("cp.async.wait_group %0;" ::"n"(D - 2) : "memory");
@@ -351,6 +360,11 @@ __device__ __forceinline__ void energy_ring_body(const EnergyArgs<float>& a, lon
             *reinterpret_cast<float4*>(a.F + off) = make_float4(Fo[0], Fo[1], Fo[2], Fo[3]);
             *reinterpret_cast<float4*>(a.f + off) = make_float4(fo[0], fo[1], fo[2], fo[3]);
         }
+    };
+#pragma unroll 1
+    for (int i = 0; i < Ng; i += 2) {
+        iter(IntC<0>(), i);
+        iter(IntC<1>(), i + 1);
     }
     asm volatile("cp.async.wait_group 0;" ::: "memory");
     if (a.partials) {
@@ -475,16 +489,19 @@ __global__ void __launch_bounds__(NTH) energy_fused_kernel(EnergyFusedArgs A) {
     };
     constexpr bool kStrag = MODE == EMODE_EQ15_STRAG;
     const bool dose = a.partials != nullptr;
-    Eq15Coef k_next = load_eq15_coef<MODE>(a.coef + (Ng - 1) * kEnergyCoef, a.dose_coef + 2 * (Ng - 1), dose);
-    Eq15Coef k_up = k_next;  // constants of group ek+1 (the opening update's group)
-    for (int i = 0; i <= Ng; ++i) {
+    // group Ng-1-i's constants in K[i % 3]: iteration i reads K[i % 3] (its
+    // closing group) and K[(i+2) % 3] (the opening group above it) and loads
+    // the next closing group's into K[(i+1) % 3]; the loop runs three
+    // iterations per trip so the slots are fixed registers, not copies
+    Eq15Coef K[3];
+    K[0] = load_eq15_coef<MODE>(a.coef + (Ng - 1) * kEnergyCoef, a.dose_coef + 2 * (Ng - 1), dose);
+    auto iter = [&](auto Rc, int i) {
+        constexpr int R = decltype(Rc)::value, R1 = (R + 1) % 3, R2 = (R + 2) % 3;
         const int ek = Ng - 1 - i;
         float nF[4] = {0.f, 0.f, 0.f, 0.f}, nf[4] = {0.f, 0.f, 0.f, 0.f};  // midpoint of group ek
-        Eq15Coef kc = k_up;
         if (ek >= 0) {
             // closing update of group ek
-            kc = k_next;
-            if (ek > 0) k_next = load_eq15_coef<MODE>(a.coef + (ek - 1) * kEnergyCoef, a.dose_coef + 2 * (ek - 1), dose);
+            if (ek > 0) K[R1] = load_eq15_coef<MODE>(a.coef + (ek - 1) * kEnergyCoef, a.dose_coef + 2 * (ek - 1), dose);
             if (kStrag) asm volatile("cp.async.wait_group %0;" ::"n"(D - 3) : "memory");
             else asm volatile("cp.async.wait_group %0;" ::"n"(D - 2) : "memory");
             const float4 vF = *slot(i % D, 0), vf = *slot(i % D, 1);
@@ -497,12 +514,12 @@ __global__ void __launch_bounds__(NTH) energy_fused_kernel(EnergyFusedArgs A) {
             for (int j = 0; j < 4; ++j) {
                 const double Fg = Fa[j], fg = fa[j];
                 double Fv, fv;
-                eq15_update<MODE>(kc, ek, Fg, fg, 0.0, static_cast<double>(na[j]), cFo[j], cfo[j], cFn[j], cfn[j],
+                eq15_update<MODE>(K[R], ek, Fg, fg, 0.0, static_cast<double>(na[j]), cFo[j], cfo[j], cFn[j], cfn[j],
                                   Fv, fv);
                 nF[j] = static_cast<float>(Fv);
                 nf[j] = static_cast<float>(fv);
                 if (dose && ok) {
-                    acc += w_pos[j] * (kc.d0 * static_cast<double>(nF[j]) + kc.d1 * static_cast<double>(nf[j]));
+                    acc += w_pos[j] * (K[R].d0 * static_cast<double>(nF[j]) + K[R].d1 * static_cast<double>(nf[j]));
                     accp += static_cast<double>(nf[j]);
                 }
                 cFo[j] = Fg;
@@ -517,16 +534,16 @@ __global__ void __launch_bounds__(NTH) energy_fused_kernel(EnergyFusedArgs A) {
                 put(base + a_off2, nf[0], nf[1], nf[2], nf[3]);
             }
         }
-        if (ek + 1 <= Ng - 1) {
+        const int eo = ek + 1;
+        if (eo >= 0 && eo <= Ng - 1) {
             // opening update of group ek+1 from the midpoint: its value mF/mf,
             // group ek's (straggling) nF, the group above's oFo/oFn
-            const int eo = ek + 1;
             float Fo[4], fo[4];
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 const double Fg = mF[j], fg = mf[j];
                 double Fv, fv;
-                eq15_update<MODE>(k_up, eo, Fg, fg, 0.0, static_cast<double>(nF[j]), oFo[j], ofo[j], oFn[j], ofn[j],
+                eq15_update<MODE>(K[R2], eo, Fg, fg, 0.0, static_cast<double>(nF[j]), oFo[j], ofo[j], oFn[j], ofn[j],
                                   Fv, fv);
                 Fo[j] = static_cast<float>(Fv);
                 fo[j] = static_cast<float>(fv);
@@ -546,7 +563,14 @@ __global__ void __launch_bounds__(NTH) energy_fused_kernel(EnergyFusedArgs A) {
             mF[j] = nF[j];
             mf[j] = nf[j];
         }
-        k_up = kc;
+    };
+    // iterations 0 .. Ng (the last one only opens group 0); trailing
+    // iterations past Ng do nothing
+#pragma unroll 1
+    for (int i = 0; i <= Ng; i += 3) {
+        iter(IntC<0>(), i);
+        iter(IntC<1>(), i + 1);
+        iter(IntC<2>(), i + 2);
     }
     asm volatile("cp.async.wait_group 0;" ::: "memory");
     if (a.partials) {
@@ -1571,9 +1595,6 @@ struct StreamPair {
     int own, offl, offr, ghi, glo;              // shared-memory offsets (float2) in a row / a face row
     bool ok1, ok_half;                          // both angles of the pair inside NA; only the first
 };
-
-template <int V>
-using IntC = std::integral_constant<int, V>;
 
 __device__ __forceinline__ void transport_stream_body(const TransportArgs<float>& a, int n_chunks, int bid) {
     constexpr int A2 = kStreamPairs, AC = 2 * A2, RF = kStreamRing, PD = kStreamAhead, RP = kStreamPRows;

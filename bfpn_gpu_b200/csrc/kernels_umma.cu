@@ -162,6 +162,8 @@ struct UmmaPipeArgs {
     const int* groups;
     uint8_t* q;              // energy-stage operand (q_offset layout)
     int* err;
+    const int4* ulist;       // non-zero k chunks and column ranges (or null: all, full width)
+    const int* ubegin;
     int nyz, NA, NT, nk, n_ntiles, n_mt, nsg;
 };
 
@@ -182,7 +184,12 @@ __global__ void __launch_bounds__(128, 1) source_angular_umma_pipe_kernel(UmmaPi
     const int m0 = mt * kPos, n0 = nt * NT;
     const int tid = threadIdx.x, warp = tid >> 5;
     const uint32_t ncols = NT <= 32 ? 32 : NT <= 64 ? 64 : NT <= 128 ? 128 : 256;
-    const int nk = a.nk;
+    // the k chunks this tile multiplies: the non-zero ones of its kernel block
+    const int u0 = a.ulist ? __ldg(a.ubegin + gz * a.n_ntiles + nt) : 0;
+    const int nk = a.ulist ? __ldg(a.ubegin + gz * a.n_ntiles + nt + 1) - u0 : a.nk;
+    auto entry = [&](int it) {
+        return a.ulist ? __ldg(a.ulist + u0 + it) : make_int4(it, 0, NT, 0);
+    };
 
     if (tid == 0) {
         for (int s = 0; s < kPipe; ++s) {
@@ -202,21 +209,36 @@ __global__ void __launch_bounds__(128, 1) source_angular_umma_pipe_kernel(UmmaPi
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tmem_base_slot;
+    {
+        // zero the accumulator: the MMAs cover only the columns their chunks reach
+        const uint32_t lane_base = static_cast<uint32_t>(warp * 32) << 16;
+        const uint32_t z = 0;
+        for (uint32_t c0 = 0; c0 < ncols; c0 += 16)
+            asm volatile(
+                "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1};" ::"r"(
+                    tmem + lane_base + c0),
+                "r"(z)
+                : "memory");
+        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 
-    const uint8_t* __restrict__ ablob = a.ablob + (static_cast<size_t>(gz) * a.n_mt + mt) * nk * (2 * a_part);
+    const uint8_t* __restrict__ ablob = a.ablob + (static_cast<size_t>(gz) * a.n_mt + mt) * a.nk * (2 * a_part);
     const uint8_t* __restrict__ bblob =
-        a.bblob + (static_cast<size_t>(gz) * a.n_ntiles + nt) * nk * static_cast<size_t>(2 * b_part);
-    const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(NT >> 3) << 17) |
-                           (static_cast<uint32_t>(kRows >> 4) << 24);
+        a.bblob + (static_cast<size_t>(gz) * a.n_ntiles + nt) * a.nk * static_cast<size_t>(2 * b_part);
+    const uint32_t idesc0 = (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(kRows >> 4) << 24);
 
     if (tid == 0) {
         int issued[kPipe] = {}, landed[kPipe] = {}, committed[kPipe] = {}, drained[kPipe] = {};
         auto issue = [&](int it) {
             const int st = it % kPipe;
+            const int kc = entry(it).x;
             uint8_t* sA = smem + st * stage_bytes;
             mbar_expect_tx(&bar_full[st], 2 * a_part + 2 * b_part);
-            bulk_copy_g2s(sA, ablob + static_cast<size_t>(it) * 2 * a_part, 2 * a_part, &bar_full[st]);
-            bulk_copy_g2s(sA + 2 * a_part, bblob + static_cast<size_t>(it) * 2 * b_part, 2 * b_part, &bar_full[st]);
+            bulk_copy_g2s(sA, ablob + static_cast<size_t>(kc) * 2 * a_part, 2 * a_part, &bar_full[st]);
+            bulk_copy_g2s(sA + 2 * a_part, bblob + static_cast<size_t>(kc) * 2 * b_part, 2 * b_part, &bar_full[st]);
             ++issued[st];
         };
         bool bad = false;
@@ -229,18 +251,21 @@ __global__ void __launch_bounds__(128, 1) source_angular_umma_pipe_kernel(UmmaPi
             }
             ++landed[st];
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t aA = smem_u32(smem + st * stage_bytes), aB = aA + 2 * a_part;
+            const int4 en = entry(it);  // {k chunk, first column, columns}
+            const uint32_t aA = smem_u32(smem + st * stage_bytes), aB = aA + 2 * a_part + (en.y / 8) * 128;
             constexpr uint32_t lboA = (kRows / 8) * 128;
             const uint32_t lboB = (NT / 8) * 128;
+            const uint32_t idesc = idesc0 | (static_cast<uint32_t>(en.z >> 3) << 17);
+            const uint32_t dcol = tmem + static_cast<uint32_t>(en.y);
 #pragma unroll
             for (int j = 0; j < BK / 16; ++j) {
                 const uint64_t ah = umma_desc(aA + j * 2 * lboA, lboA, 128);
                 const uint64_t al = umma_desc(aA + a_part + j * 2 * lboA, lboA, 128);
                 const uint64_t bh = umma_desc(aB + j * 2 * lboB, lboB, 128);
                 const uint64_t bl = umma_desc(aB + b_part + j * 2 * lboB, lboB, 128);
-                umma_bf16(tmem, ah, bh, idesc, (it > 0 || j > 0) ? 1u : 0u);
-                umma_bf16(tmem, ah, bl, idesc, 1u);
-                umma_bf16(tmem, al, bh, idesc, 1u);
+                umma_bf16(dcol, ah, bh, idesc, 1u);
+                umma_bf16(dcol, ah, bl, idesc, 1u);
+                umma_bf16(dcol, al, bh, idesc, 1u);
             }
             umma_commit(&bar_mma[st]);
             ++committed[st];
@@ -347,8 +372,8 @@ size_t umma_pipe_smem(int NT, int BK) {
 
 cudaError_t launch_source_angular_pipe(const float* P1, const float* P2, uint8_t* ablob, const uint8_t* bblob,
                                        const int* groups, int n_groups, uint8_t* q, int Ng, int* err, int nyz,
-                                       int NA, int NT, int BK, int n_ntiles, cudaStream_t s, cudaEvent_t packed,
-                                       bool pack) {
+                                       int NA, int NT, int BK, int n_ntiles, const int4* ulist, const int* ubegin,
+                                       cudaStream_t s, cudaEvent_t packed, bool pack) {
     if (n_groups <= 0) return packed ? cudaEventRecord(packed, s) : cudaSuccess;
     if (BK != 16 || NT % 16 != 0 || NT < 16 || NT > 256) return cudaErrorInvalidValue;
     const int n_mt = (nyz + kPos - 1) / kPos, nk = (NA + BK - 1) / BK;
@@ -361,7 +386,7 @@ cudaError_t launch_source_angular_pipe(const float* P1, const float* P2, uint8_t
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     if (packed && (e = cudaEventRecord(packed, s)) != cudaSuccess) return e;
-    UmmaPipeArgs a{ablob, bblob, groups, q, err, nyz, NA, NT, nk, n_ntiles, n_mt, 2 * ((Ng + 15) / 16)};
+    UmmaPipeArgs a{ablob, bblob, groups, q, err, ulist, ubegin, nyz, NA, NT, nk, n_ntiles, n_mt, 2 * ((Ng + 15) / 16)};
     size_t smem = umma_pipe_smem(NT, BK);
     // at most two CTAs per SM when each holds 256 tensor-memory columns (512 per SM)
     if (NT > 128) smem = std::max<size_t>(smem, 80 * 1024);
@@ -682,6 +707,36 @@ __global__ void build_umma_blob_kernel(const float* __restrict__ ker_v, const in
     const size_t off = umma_kmajor_offset(nn, kh * 8, NT);
     *reinterpret_cast<uint4*>(base + off) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
     *reinterpret_cast<uint4*>(base + part + off) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+}
+
+void build_umma_ranges(const float* kv, const int* groups, int n_groups, int NA, int NT, int BK, int n_ntiles,
+                       std::vector<int4>& list, std::vector<int>& begin) {
+    const int nk = (NA + BK - 1) / BK;
+    list.clear();
+    begin.assign(static_cast<size_t>(n_groups) * n_ntiles + 1, 0);
+    for (int gz = 0; gz < n_groups; ++gz) {
+        const float* K = kv + static_cast<size_t>(groups[gz]) * NA * NA;  // [in][out]
+        for (int nt = 0; nt < n_ntiles; ++nt) {
+            begin[static_cast<size_t>(gz) * n_ntiles + nt] = static_cast<int>(list.size());
+            const int n0 = nt * NT, n1 = std::min(NA, n0 + NT);
+            for (int kc = 0; kc < nk; ++kc) {
+                int lo = NT, hi = 0;
+                for (int in = kc * BK; in < std::min(NA, (kc + 1) * BK); ++in) {
+                    const float* row = K + static_cast<size_t>(in) * NA;
+                    for (int o = n0; o < n1; ++o)
+                        if (row[o] != 0.0f) {
+                            lo = std::min(lo, o - n0);
+                            hi = std::max(hi, o - n0 + 1);
+                        }
+                }
+                if (hi <= lo) continue;
+                lo = lo / 16 * 16;
+                hi = std::min(NT, (hi + 15) / 16 * 16);
+                list.push_back(make_int4(kc, lo, hi - lo, 0));
+            }
+        }
+    }
+    begin.back() = static_cast<int>(list.size());
 }
 
 size_t umma_blob_bytes(int n_groups, int NA, int NT, int BK) {

@@ -604,6 +604,31 @@ def test_tensor_core_source_mixed(shape):
     assert rel_err(s_simt, s_ref) < 2e-6
 
 
+def test_tensor_core_source_sparse_kernel_blocks():
+    """Water's angular scattering kernel on a 20x20 angular grid keeps ~2 %
+    of its entries (the rest fall below the reference's 1e-3 cut): the
+    tensor-core contraction multiplies only the k chunks and column ranges of
+    each 16 x 208 kernel block that hold non-zero entries.  Against the fp32
+    CUDA-core contraction, which multiplies everything."""
+    cfg = small_cfg(ny=6, nz=6, nmu=20, nom=20, ng=120, lg=259.0, beam_energy=230.0, sigma_e=2.3, ly=2.0, lz=2.0,
+                    lu=1.0, lv=1.0)
+    mu, sig = read_tables(table_dir("water"), cfg.ng)
+    ctx = Context(cfg.grid(), cfg.phys(), capi.PREC_MIXED)
+    ctx.load_tables(mu, sig)
+    ctx.init_beam()
+    assert ctx.source_groups() > 0
+    F, f, F1, f1 = seeded_states(ctx, 5)
+    for k, arr in enumerate((F, f, F1, f1)):
+        ctx.set_state(k // 2, k % 2, arr.astype(np.float32).astype(np.float64))
+    ctx.secondary_source()
+    s_tc = ctx.source()
+    ctx.set_option(capi.OPT_TENSOR_CORES, 0)
+    ctx.secondary_source()
+    s_simt = ctx.source()
+    assert np.abs(s_simt).max() > 0
+    assert rel_err(s_tc, s_simt) < 2e-5
+
+
 def test_fp64_100mev_configuration_full_run():
     """The 100 MeV FP64 configuration (16x16 yz, 8x8 angles, 200 groups over
     104 MeV, 10 cm) against the oracle's full-run fixture, 1e-10 relative."""
