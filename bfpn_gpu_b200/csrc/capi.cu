@@ -647,8 +647,9 @@ cudaError_t enq_overlap_body(bfpn_ctx* c, int step) {
 // and its IDD] on s_sec; close(n) is the closing pass and secondary half of
 // the call's last step.  Step 0 has no secondary half: body(1) finalises its
 // IDD on the context stream.  Each kernel applies the unfused order's
-// arithmetic to the same inputs, so every state and IDD partial is the same;
-// a primary energy pass and the pack pass are saved per step.
+// arithmetic to the same inputs, so the states are the same (a few values
+// far below the peak aside, which may round one float step apart); a
+// primary energy pass and the pack pass are saved per step.
 bool fused_ok(const bfpn_ctx* c) {
     const unsigned fl = c->p.flags;
     if (!c->fuse_energy || !c->overlap || c->prec != BFPN_PREC_MIXED || c->lite || c->ooc ||

@@ -427,8 +427,10 @@ cudaError_t launch_energy_ring(const EnergyArgs<float>& a, cudaStream_t s) {
 // closing update to group ek = Ng-1-i and the opening update to group ek+1.
 // Each update is energy_ring_kernel's, on the same inputs -- the midpoint
 // value is rounded to float as the separate passes store it -- so the state
-// equals the two passes' bit for bit; the closing pass's IDD partials are
-// those of the closing ring pass.  At the midpoint the source groups' values
+// equals the two passes' bit for bit on the grids tested, except a few values
+// far below the peak, which may come out one float rounding step apart (on a
+// 35 x 35, 12-group grid: values 1e-8 below the peak, 4.6e-16 of it).  The closing pass's IDD partials are those of the
+// closing ring pass.  At the midpoint the source groups' values
 // go to the angular contraction's operand (split bf16), which removes that
 // operand's own pass over the primary.
 // ---------------------------------------------------------------------------
@@ -1565,18 +1567,16 @@ constexpr int kStreamMaxThreads = 256 * kStreamTPC;   // planes up to 256 points
 constexpr int kStreamMaxReg = kStreamPT == 2 ? 168 : 88;
 
 size_t transport_stream_smem(int NPy) {
-    // rows of F and P: positions -1 .. NPy (halos) and a spare; face rows: NPy + 3 faces x (F, P), double-buffered
-    const size_t row = static_cast<size_t>(NPy + 3) * kStreamPairs * sizeof(float2);
-    const size_t grow = static_cast<size_t>(NPy + 3) * 2 * kStreamPairs * sizeof(float2);
-    return (kStreamRing + kStreamPRows) * row + 2 * grow;
+    const size_t row = static_cast<size_t>(NPy) * kStreamPairs * sizeof(float2);
+    const size_t grow = static_cast<size_t>(NPy + 3) * kStreamPairs * sizeof(float2);
+    return (kStreamRing + kStreamPRows) * row + 4 * grow;  // face rows of F and P, double-buffered
 }
 
 // kStreamTPC threads per column y: thread (y, t) carries angle pairs t,
 // t + kStreamTPC, ... of the block's four; threads t < 2 also copy the row's
-// 16-byte pieces, one each.  The z-stencil of a pair lives in three-slot
-// register rotations indexed by row mod 3; the row loop is unrolled by three
-// so every slot index is a compile-time constant and the rotation costs no
-// moves.
+// 16-byte pieces, one each.  The z-stencil of a pair lives in three-slot register
+// rotations indexed by row mod 3; the row loop is unrolled by three so every
+// slot index is a compile-time constant and the rotation costs no moves.
 struct StreamPair {
     float2 f[3];              // F row r in f[r % 3] (rows i .. i+2 at iteration i)
     float2 p[3], hh[3];       // predictor P and H row r in [r % 3] (rows i-2 .. i)
@@ -1584,8 +1584,8 @@ struct StreamPair {
     float2 pz[3], pf[3], pf2[3];  // z-walk of P: face value of cell c in pz[c % 3]; P(i) - P(i-1) and its double in [i % 3]
     float2 wry, wrz, hy, hz;
     bool dnz;
-    int gr;                   // face-row index of the lower face this cell's y-divergence reads
-    bool ok1, ok_half;        // both angles of the pair inside NA; only the first
+    int own, offl, offr, ghi, glo;              // shared-memory offsets (float2) in a row / a face row
+    bool ok1, ok_half;                          // both angles of the pair inside NA; only the first
 };
 
 __device__ __forceinline__ void transport_stream_body(const TransportArgs<float>& a, int n_chunks, int bid) {
@@ -1593,47 +1593,34 @@ __device__ __forceinline__ void transport_stream_body(const TransportArgs<float>
     static_assert((RF & (RF - 1)) == 0 && (RP & (RP - 1)) == 0 && AC == 8, "ring sizes are powers of two");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int Ny = a.Ny, Nz = a.Nz, NPy = Ny + 1, NA = a.NA;
-    // A row of F or P holds positions -1 .. NPy at index (p + 1) * A2 (the two
-    // halo positions repeat the edge values: the reference's clamped stencil)
-    // and a spare position NPy + 1 for stores that have no halo to fill; so
-    // every row access is the thread's row base plus a constant.  A face row
-    // interleaves F and P per face: face g of F at 2 g A2, of P at (2 g + 1) A2;
-    // faces 0 .. NPy + 1 as the cells' y-walks use them, face NPy + 2 spare.
-    const int RS = (NPy + 3) * A2;       // one row, in float2
-    const int GS = (NPy + 3) * 2 * A2;   // one face row (F and P)
-    float2* Fr = reinterpret_cast<float2*>(smem_raw);  // [RF][NPy + 3][A2]
-    float2* Pr = Fr + RF * RS;                         // [RP][NPy + 3][A2]
-    float2* Gb = Pr + RP * RS;                         // [2][NPy + 3][F, P][A2]: G of the y-walks, by row parity
+    const int RS = NPy * A2;       // one row, in float2
+    const int GS = (NPy + 2) * A2 + A2;  // one face row: faces -1 .. N+1, then a spare row for edge-less threads
+    float2* Fr = reinterpret_cast<float2*>(smem_raw);  // [RF][NPy][A2]
+    float2* Pr = Fr + RF * RS;                         // [RP][NPy][A2]
+    float2* Gb = Pr + RP * RS;                         // [2][F, P][GS]: G of the y-walks, by row parity
     const int chunk = bid % n_chunks, ek = bid / n_chunks, a0 = chunk * AC;
     const size_t zs = static_cast<size_t>(NPy) * NA;  // one z row in the state
     const size_t base = static_cast<size_t>(ek) * (Nz + 1) * zs + a0;
     constexpr int PT = kStreamPT, TPC = kStreamTPC;
     const int tid = threadIdx.x, h = tid % TPC, y = tid / TPC;
 
-    // this thread's 16-byte piece of every row (threads h < 2): position y, angles a0 + 4h .. a0 + 4h + 3;
-    // the edge columns' threads also copy it into the halo
+    // this thread's 16-byte piece of every row (threads h < 2): position y, angles a0 + 4h .. a0 + 4h + 3
     const bool vec = NA % 4 == 0;
     const bool lcp = h < 2;
     const bool lok = vec && lcp && a0 + 4 * h < NA;
     const float* in0 = a.in;
     const float* lsrc = in0 + base + static_cast<size_t>(y) * NA + 4 * (h & 1);
-    float* ldst = reinterpret_cast<float*>(Fr) + (y + 1) * AC + 4 * (h & 1);
+    float* ldst = reinterpret_cast<float*>(Fr) + y * AC + 4 * (h & 1);
     auto fill = [&](int r) {  // row r of F into slot r % RF; one commit group per call, empty past the plane
         if (r <= Nz) {
             if (vec) {
-                if (lcp) {
-                    float* d = ldst + (r & (RF - 1)) * (2 * RS);
-                    const float* src = lok ? lsrc + static_cast<size_t>(r) * zs : in0;
-                    cp_async16(d, src, lok);
-                    if (y == 0) cp_async16(d - AC, src, lok);
-                    if (y == Ny) cp_async16(d + AC, src, lok);
-                }
+                if (lcp) cp_async16(ldst + (r & (RF - 1)) * (2 * RS), lok ? lsrc + static_cast<size_t>(r) * zs : in0, lok);
             } else {
                 float* row = reinterpret_cast<float*>(Fr + (r & (RF - 1)) * RS);
                 const float* src = in0 + base + static_cast<size_t>(r) * zs;
-                for (int v = tid; v < (NPy + 2) * AC; v += blockDim.x) {
-                    const int e = v % AC, ps = v / AC, p = min(max(ps - 1, 0), Ny);
-                    row[ps * AC + e] = (a0 + e < NA) ? src[static_cast<size_t>(p) * NA + e] : 0.f;
+                for (int v = tid; v < NPy * AC; v += blockDim.x) {
+                    const int e = v % AC, p = v / AC;
+                    row[p * AC + e] = (a0 + e < NA) ? src[static_cast<size_t>(p) * NA + e] : 0.f;
                 }
             }
         }
@@ -1642,12 +1629,8 @@ __device__ __forceinline__ void transport_stream_body(const TransportArgs<float>
 
     const float2 ndt = make_float2(-a.dt, -a.dt), nhdt = make_float2(-0.5f * a.dt, -0.5f * a.dt);
     const float lo = a.preserve_sign ? -INFINITY : 0.f;
-    const int own = (y + 1) * A2 + h;  // pair k at own + TPC k, in every row
-    // face of the cell beyond the plane (edge threads) or the spare face; the
-    // P halo (edge threads) or the spare position: every thread stores one of each
-    const int gw = (y + 1) * 2 * A2 + h;
-    const int gedge = (y == 0 ? 0 : (y == Ny ? NPy + 1 : NPy + 2)) * 2 * A2 + h;
-    const int phalo = y == 0 ? own - A2 : (y == Ny ? own + A2 : (NPy + 2) * A2 + h);
+    // the face beyond the plane (edge threads) or a spare slot (the others): every thread stores one
+    const int gedge_row = y == 0 ? 0 : (y == Ny ? (NPy + 1) * A2 : (NPy + 2) * A2);
     StreamPair S[PT];
 #pragma unroll
     for (int k = 0; k < PT; ++k) {
@@ -1664,50 +1647,53 @@ __device__ __forceinline__ void transport_stream_body(const TransportArgs<float>
         P.dnz = wz0 < 0.f;
         P.hy = dny ? make_float2(-0.5f, -0.5f) : make_float2(0.5f, 0.5f);
         P.hz = P.dnz ? make_float2(-0.5f, -0.5f) : make_float2(0.5f, 0.5f);
-        // the cell's y-divergence: faces y+1 and y (upwind y+), y+2 and y+1 (upwind y-)
-        P.gr = (y + (dny ? 1 : 0)) * 2 * A2 + q;
+        P.own = y * A2 + q;
+        P.offl = max(y - 1, 0) * A2 + q;
+        P.offr = min(y + 1, Ny) * A2 + q;
+        // G index of the two faces of this cell's y-divergence (G is stored one face up)
+        P.ghi = P.own + (dny ? 2 * A2 : A2);
+        P.glo = P.own + (dny ? A2 : 0);
 #pragma unroll
         for (int r = 0; r < 3; ++r) P.p[r] = P.hh[r] = make_float2(0.f, 0.f);
     }
     float* orow = a.out + base + static_cast<size_t>(y) * NA;  // this position's angles a0 .. a0+7, row 0
 
-    // y face value of this thread's cell (pair k, value x, row base rb) into face row G
-    auto y_face = [&](float2* G, const float2* rb, int k, const StreamPair& P, float2 x) {
-        const float2 back = sub2(x, rb[TPC * k - A2]), fwd = sub2(rb[TPC * k + A2], x);
-        G[gw + TPC * k] = __ffma2_rn(P.hy, superbee_diff2(back, __fadd2_rn(back, back), fwd, __fadd2_rn(fwd, fwd)), x);
-        G[gedge + TPC * k] = x;  // faces beyond the plane equal the edge value
+    auto y_face = [&](float2* G, const float2* row, const StreamPair& P, float2 x) {
+        const float2 back = sub2(x, row[P.offl]), fwd = sub2(row[P.offr], x);
+        G[P.own + A2] = __ffma2_rn(P.hy, superbee_diff2(back, __fadd2_rn(back, back), fwd, __fadd2_rn(fwd, fwd)), x);
+        G[gedge_row + (P.own - y * A2)] = x;  // faces beyond the plane equal the edge value
     };
-
     // Iteration i (R = i mod 3).  Phase A: y faces of F row i (stage 1) and of
-    // P row j = i-2 (stage 2) into the face row of parity i, and F row
+    // P row j = i-2 (stage 2) into the face rows of parity i, and F row
     // min(i+2, Nz) into the rotation (row Nz stays in its ring slot: nothing is
     // copied past the plane).  Then this thread's copy of row i+3 is waited
     // for and the block meets once: faces published, F row i+3 and P row i-1
     // visible.  Phase B: stage 1 on row i (z face of cell i+1, P(i) -- also
-    // to shared memory, with its halo -- and H(i)), stage 2 on row j (z face
-    // of cell j+1 from P rows j .. i, the output row).  One barrier per row
-    // suffices: a face row of parity i is rewritten only at iteration i+2,
-    // after every thread has passed barrier i+1 and so finished iteration i;
-    // the F slot refilled at iteration i held row i+PD+2-RF, the P slot written
-    // held row i-4, both last read before barrier i-1.  A row of F past the
-    // plane is not walked: P(i) repeats the last predictor row.  FILL: issue
-    // the copy of row i+PD+2 (every iteration that walks F).
+    // to shared memory -- and H(i)), stage 2 on row j (z face of cell j+1 from
+    // P rows j .. i, the output row).  One barrier per row suffices: a face
+    // row of parity i is rewritten only at iteration i+2, after every thread
+    // has passed barrier i+1 and so finished iteration i; the F slot refilled
+    // at iteration i held row i-2 and the P slot written held row i-4, both
+    // last read before barrier i-1.  A row of F past the plane is not walked:
+    // P(i) repeats the last predictor row.  FILL: issue the copy of row
+    // i+PD+2 (every iteration that walks F).
     auto iter = [&](auto Rc, auto S1c, auto S2c, auto FILLc, int i) {
         constexpr int R = decltype(Rc)::value, R1 = (R + 1) % 3, R2 = (R + 2) % 3;
         constexpr bool st1 = decltype(S1c)::value != 0, st2 = decltype(S2c)::value != 0;
         constexpr bool do_fill = decltype(FILLc)::value != 0;
-        float2* G = Gb + (i & 1) * GS;  // F faces at G[2 g A2 + q], P faces A2 further
-        const float2* Fi = Fr + (i & (RF - 1)) * RS + own;
-        const float2* f2row = Fr + ((i + min(2, Nz - i)) & (RF - 1)) * RS + own;
-        const float2* Pj = Pr + ((i - 2) & (RP - 1)) * RS + own;
+        float2* GF = Gb + (i & 1) * (2 * GS);
+        float2* GP = GF + GS;
+        const float2* Fi = Fr + (i & (RF - 1)) * RS;
+        const float2* f2row = Fr + ((i + min(2, Nz - i)) & (RF - 1)) * RS;
+        const float2* Pj = Pr + ((i - 2) & (RP - 1)) * RS;
 #pragma unroll
         for (int k = 0; k < PT; ++k) {
             StreamPair& P = S[k];
             if (st1) {
-                P.f[R2] = f2row[TPC * k];
-                y_face(G, Fi, k, P, P.f[R]);
+                P.f[R2] = f2row[P.own];
+                y_face(GF, Fi, P, P.f[R]);
             }
-            if (st2) y_face(G + A2, Pj, k, P, P.p[R1]);
+            if (st2) y_face(GP, Pj, P, P.p[R1]);
         }
         asm volatile("cp.async.wait_group %0;" ::"n"(PD - 2) : "memory");  // row i+3 of F landed
         __syncthreads();
@@ -1723,13 +1709,10 @@ __device__ __forceinline__ void transport_stream_body(const TransportArgs<float>
                 const float2 gz_p = __ffma2_rn(P.hz, superbee_diff2(back, back2, P.zf[R], P.zf2[R]), P.f[R1]);
                 const float2 dz = __fmul2_rn(P.wrz, P.dnz ? sub2(gz_p, P.gz[R]) : sub2(P.gz[R], P.gz[R2]));
                 P.gz[R1] = gz_p;
-                const float2* gr = G + P.gr;
-                const float2 d = __fadd2_rn(__fmul2_rn(P.wry, sub2(gr[2 * A2], gr[0])), dz);
+                const float2 d = __fadd2_rn(__fmul2_rn(P.wry, sub2(GF[P.ghi], GF[P.glo])), dz);
                 P.p[R] = max_lo2(__ffma2_rn(ndt, d, P.f[R]), lo);
                 P.hh[R] = __ffma2_rn(nhdt, d, P.f[R]);
-                Pw[own + TPC * k] = P.p[R];
-                Pw[phalo + TPC * k] = P.p[R];
-                if (Ny == 0) Pw[own + TPC * k + A2] = P.p[R];  // a one-point row: both halos
+                Pw[P.own] = P.p[R];
             } else {
                 P.p[R] = P.p[R2];
             }
@@ -1744,8 +1727,7 @@ __device__ __forceinline__ void transport_stream_body(const TransportArgs<float>
                 const float2 gp_p = __ffma2_rn(P.hz, superbee_diff2(back, back2, P.pf[R], P.pf2[R]), P.p[R2]);
                 const float2 dzp = __fmul2_rn(P.wrz, P.dnz ? sub2(gp_p, P.pz[R1]) : sub2(P.pz[R1], P.pz[R]));
                 P.pz[R2] = gp_p;
-                const float2* gr = G + A2 + P.gr;
-                const float2 t = __ffma2_rn(nhdt, __fmul2_rn(P.wry, sub2(gr[2 * A2], gr[0])), P.hh[R1]);
+                const float2 t = __ffma2_rn(nhdt, __fmul2_rn(P.wry, sub2(GP[P.ghi], GP[P.glo])), P.hh[R1]);
                 const float2 v = max_lo2(__ffma2_rn(nhdt, dzp, t), lo);
                 float* o = orow + 2 * (h + TPC * k);  // pair h + TPC k
                 if (P.ok1) *reinterpret_cast<float2*>(o) = v;
@@ -1762,8 +1744,8 @@ __device__ __forceinline__ void transport_stream_body(const TransportArgs<float>
 #pragma unroll
     for (int k = 0; k < PT; ++k) {
         StreamPair& P = S[k];
-        P.f[0] = Fr[own + TPC * k];
-        P.f[1] = Fr[(min(1, Nz) & (RF - 1)) * RS + own + TPC * k];
+        P.f[0] = Fr[P.own];
+        P.f[1] = Fr[(min(1, Nz) & (RF - 1)) * RS + P.own];
         P.gz[2] = P.gz[0] = P.f[0];  // faces of cells -1 and 0 of a clamped column: the edge value
         P.zf[2] = sub2(P.f[1], P.f[0]);
         P.zf2[2] = __fadd2_rn(P.zf[2], P.zf[2]);

@@ -299,8 +299,10 @@ int32_t bfpn_source_groups(bfpn_ctx* ctx);
  *   operand: per step one primary energy pass and the operand's pack pass
  *   fewer.  Within a bfpn_step call the secondary half of step n then runs
  *   beside the primary's transport and angular passes of step n+1; the call
- *   still ends on whole steps.  0 keeps the separate passes.  Same states and
- *   IDD values. */
+ *   still ends on whole steps.  0 keeps the separate passes.  The states
+ *   are the separate passes' bit for bit except a few values far below the
+ *   peak, which may round one float step apart (within 1e-12 of the peak);
+ *   the IDD agrees to the order of the closing pass's partial sums. */
 enum {
     BFPN_OPT_TENSOR_CORES = 0,
     BFPN_OPT_CUDA_GRAPHS = 1,

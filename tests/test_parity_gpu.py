@@ -474,6 +474,23 @@ def test_fused_energy_passes_equal_separate_passes(straggling):
         assert np.array_equal(a, b)
 
 
+def test_fused_energy_passes_tiny_values():
+    """A 35 x 35 plane with 12 groups: a few psi^1 values about 1e-8 below
+    the array's peak come out one float rounding step apart between the fused
+    and the separate passes (4.6e-16 of the peak seen), so the states are
+    compared to 1e-12 of their peak and bit for bit from 1e-6 of the peak up.
+    The IDD agrees to the order of its partial sums."""
+    cfg = small_cfg(nx=160, ny=34, nz=34, nmu=4, nom=4, ng=12, ly=8.0, lz=8.0, t_final=0.5)
+    _, _, idd_s, st_s = _stepped(cfg, capi.PREC_MIXED, 0, [8])
+    _, _, idd_f, st_f = _stepped(cfg, capi.PREC_MIXED, 2, [8], fused=1)
+    assert np.abs(idd_f - idd_s).max() <= 1e-13 * np.abs(idd_s).max()
+    for a, b in zip(st_s, st_f):
+        peak = np.abs(a).max()
+        assert np.abs(a - b).max() <= 1e-12 * peak
+        big = np.abs(a) >= 1e-6 * peak
+        assert np.array_equal(a[big], b[big])
+
+
 def test_fused_energy_passes_large_plane_bit_identical():
     """On a plane of more than 2^20 lanes the separate passes use the 4-lane
     ring kernel, whose partial sums the fused kernel shares: the IDD history
