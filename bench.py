@@ -244,7 +244,7 @@ NCU_DRAM_BYTES_PER_CELL = {
         "source_energy": (249.24e6 + 132.63e6) / 44.1e6,
     },
     "water230_80": {
-        "transport": (420.1e6 + 366.1e6) / 104.976e6,  # transport_cluster_kernel, 81x81x400x40
+        "transport": (420.0e6 + 366.8e6) / 104.976e6,  # transport_stream_kernel, 81x81x400x40
     },
 }
 NCU_DRAM_BYTES_PER_CELL["bone230_80"] = NCU_DRAM_BYTES_PER_CELL["water230_80"]
